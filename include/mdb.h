@@ -1,0 +1,326 @@
+/*
+ * mdb.h -- the C ABI of the B200 molecular-dynamics step engine.
+ *
+ * This is the drop-in boundary for the step loop of making-it-rain-webgpu:
+ * every entry point below replaces one public member of `StepLoop`
+ * (src/gpu/loop.ts) or of the single-configuration evaluators it is tested
+ * through, and the comment on each names the reference interface it stands in
+ * for (paths relative to the reference project root).
+ *
+ * Conventions, all of them fixed:
+ *   - Plain C types only: pointers, sizes, doubles.  No torch, no CUDA types.
+ *   - Units are OpenMM's: nm, ps, amu, kJ/mol, e, K, bar (src/engine/units.ts).
+ *   - Positions, velocities and forces are xyz-interleaved double arrays of
+ *     3*N entries, as `StepLoop.positions()` returns them (loop.ts:900).
+ *   - Box vectors are row-major a, b, c (9 doubles) in OpenMM's reduced form.
+ *   - Every function returns an `int` status (`mdb_status`); nothing is
+ *     thrown across the ABI.  The message for the last failure on an engine
+ *     is `mdb_last_error(engine)`.  The reference throws named Error subclasses
+ *     instead (src/engine/system.ts:178, src/gpu/nonbonded.ts:54,
+ *     src/engine/constraint-clusters.ts:71, src/reference/triclinic.ts:179);
+ *     each has a status code here.
+ *   - Calls on one engine are not thread-safe: one host thread per engine, as
+ *     the reference's single JS thread (src/gpu/loop.ts:208).
+ *   - Input arrays are copied; nothing is aliased after a call returns
+ *     (src/gpu/allocator.ts:69 ownership rule).
+ */
+#ifndef MDB_H
+#define MDB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDB_ABI_VERSION 1
+
+typedef enum mdb_status {
+  MDB_OK = 0,
+  MDB_ERR_INVALID_ARGUMENT = 1,
+  /* UnsupportedForce, src/engine/system.ts:178 */
+  MDB_ERR_UNSUPPORTED_FORCE = 2,
+  /* CutoffTooLargeForBox, src/reference/triclinic.ts:179 */
+  MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX = 3,
+  /* ClusterTooLarge, src/engine/constraint-clusters.ts:71 */
+  MDB_ERR_CLUSTER_TOO_LARGE = 4,
+  /* SHAKE/RATTLE gave up after the iteration cap, src/reference/constraints.ts:34 */
+  MDB_ERR_NOT_CONVERGED = 5,
+  /* a device-side table (tile list, cell list) ran out of room */
+  MDB_ERR_CAPACITY = 6,
+  /* fixed-point range exceeded: a diverged run, src/reference/fixed-point.ts:56 */
+  MDB_ERR_RANGE = 7,
+  MDB_ERR_DEVICE = 8,
+  /* a bounded device-side wait gave up */
+  MDB_ERR_TIMEOUT = 9,
+  MDB_ERR_NO_DEVICE = 10,
+  /* NotSmooth, src/reference/fft.ts:24 */
+  MDB_ERR_NOT_SMOOTH = 11,
+  MDB_ERR_DEVICE_LOST = 12
+} mdb_status;
+
+enum { MDB_INTEGRATOR_LFMIDDLE = 0, MDB_INTEGRATOR_VERLET = 1 };
+
+/* Run-option flags. */
+enum {
+  /* Launch every kernel directly instead of replaying captured CUDA graphs. */
+  MDB_FLAG_NO_GRAPH = 1,
+  /* Rebuild the tile list every step, whatever the displacement. */
+  MDB_FLAG_ALWAYS_REBUILD = 2
+};
+
+/*
+ * An OpenMM System, as flat arrays.  Mirrors `OpenMMSystem` and the force
+ * interfaces of src/engine/system.ts:41-173.  A force that is absent has its
+ * count set to zero (or `has_nonbonded` = 0).  Bonded forces never use
+ * periodic boundary conditions (src/reference/forces/bonded.ts:14-18).
+ */
+typedef struct mdb_system_desc {
+  int32_t n_particles;
+  const double* masses; /* amu; 0 = frozen particle */
+  double box[9];        /* default periodic box vectors */
+
+  int32_t n_constraints;
+  const int32_t* constraint_p1;
+  const int32_t* constraint_p2;
+  const double* constraint_distance; /* nm */
+
+  /* NonbondedForce with method PME (system.ts:88-121) */
+  int32_t has_nonbonded;
+  double cutoff;          /* nm */
+  double ewald_tolerance;
+  double alpha;           /* nm^-1; 0 = derive from cutoff and tolerance */
+  int32_t grid[3];        /* 0 = derive from box and tolerance */
+  int32_t use_dispersion_correction;
+  const double* charge;   /* e */
+  const double* sigma;    /* nm */
+  const double* epsilon;  /* kJ/mol */
+  int32_t n_exceptions;
+  const int32_t* exception_p1;
+  const int32_t* exception_p2;
+  const double* exception_charge_prod; /* e^2 */
+  const double* exception_sigma;
+  const double* exception_epsilon;
+
+  /* HarmonicBondForce: E = k/2 (r - length)^2 */
+  int32_t n_bonds;
+  const int32_t* bond_p1;
+  const int32_t* bond_p2;
+  const double* bond_length;
+  const double* bond_k;
+
+  /* HarmonicAngleForce: E = k/2 (theta - angle)^2 */
+  int32_t n_angles;
+  const int32_t* angle_p1;
+  const int32_t* angle_p2;
+  const int32_t* angle_p3;
+  const double* angle_theta;
+  const double* angle_k;
+
+  /* PeriodicTorsionForce: E = k (1 + cos(n phi - phase)) */
+  int32_t n_torsions;
+  const int32_t* torsion_p1;
+  const int32_t* torsion_p2;
+  const int32_t* torsion_p3;
+  const int32_t* torsion_p4;
+  const int32_t* torsion_periodicity;
+  const double* torsion_phase;
+  const double* torsion_k;
+
+  /* CMMotionRemover; 0 = absent (com-motion.ts:38) */
+  int32_t com_frequency;
+
+  /* MonteCarloBarostat; frequency 0 = absent (system.ts:128) */
+  int32_t barostat_frequency;
+  double barostat_pressure;    /* bar */
+  double barostat_temperature; /* K */
+
+  /* PositionRestraint, k*periodicdistance(x,y,z,x0,y0,z0)^2 (system.ts:139) */
+  int32_t n_restraints;
+  const int32_t* restraint_particle;
+  const double* restraint_k;
+  const double* restraint_x0;
+  const double* restraint_y0;
+  const double* restraint_z0;
+} mdb_system_desc;
+
+/* An OpenMM State: mirrors `OpenMMState`, src/engine/state.ts:18-39. */
+typedef struct mdb_state_desc {
+  const double* positions;  /* 3N, nm */
+  const double* velocities; /* 3N, nm/ps; NULL = all zero */
+  double box[9];
+  int64_t step;
+} mdb_state_desc;
+
+/* Mirrors `RunOptions`, src/gpu/loop.ts:117-168. */
+typedef struct mdb_run_options {
+  double time_step;            /* ps */
+  double temperature;          /* K */
+  double friction;             /* ps^-1; 0 = deterministic without a seed */
+  double constraint_tolerance; /* relative */
+  uint32_t seed;
+  int32_t integrator;          /* MDB_INTEGRATOR_* */
+  double verlet_skin;          /* nm; negative = the default 0.15 (nonbonded.ts:227) */
+  int32_t max_batch;           /* steps per captured graph; 0 = 100 (loop.ts:171) */
+  int32_t mesh[3];             /* PME mesh override; 0 = from the box */
+  int32_t device;              /* CUDA device ordinal */
+  int32_t flags;               /* MDB_FLAG_* */
+} mdb_run_options;
+
+/*
+ * Energies by OpenMM force group, kJ/mol.  `direct_group` and
+ * `reciprocal_group` are what OpenMM reports for "NonbondedForce[direct]" and
+ * "NonbondedForce[reciprocal]" (src/reference/potential.ts:122-141); the parts
+ * they sum are given separately (src/reference/forces/nonbonded.ts:79-96).
+ */
+typedef struct mdb_energies {
+  double bond;
+  double angle;
+  double torsion;
+  double restraint;
+  double direct_coulomb;       /* erfc Coulomb over non-excluded pairs */
+  double direct_lj;            /* LJ over non-excluded pairs */
+  double exclusion_correction; /* minus the reciprocal part of excluded pairs */
+  double exceptions;           /* the exceptions' own Coulomb + LJ */
+  double dispersion;           /* analytic long-range correction */
+  double reciprocal_mesh;      /* the mesh sum alone */
+  double self_energy;
+  double net_charge;
+  double direct_group;
+  double reciprocal_group;
+  double potential;
+  double kinetic;              /* from the velocities as they are (kinetic.ts:31) */
+  double temperature;          /* K, from `kinetic` and the constrained DoF */
+  double degrees_of_freedom;
+  double virial[9];            /* sum of r (x) F over pairs, lattice-resolved; kJ/mol */
+} mdb_energies;
+
+/* Mirrors `StepLoop.barostatStatistics`, src/gpu/loop.ts:572. */
+typedef struct mdb_barostat_stats {
+  int64_t attempts;
+  int64_t accepted;
+  double volume_scale;     /* nm^3 */
+  /* delayed-acceptance screening (no reference counterpart) */
+  int64_t screened;        /* proposals decided by the surrogate stage alone */
+  int64_t exact_evaluations;
+} mdb_barostat_stats;
+
+/* Mirrors `StepLoop.verletFlags`, src/gpu/loop.ts:941. */
+typedef struct mdb_neighbour_stats {
+  int64_t rebuilds;
+  int64_t tiles;          /* cluster-pair tiles in the current list */
+  int64_t tile_capacity;
+  int64_t blocks;         /* 32-atom clusters */
+  int32_t overflowed;     /* a table ran out of room since creation */
+  double skin;            /* nm */
+} mdb_neighbour_stats;
+
+typedef struct mdb_engine mdb_engine;
+
+/* ---- lifetime --------------------------------------------------------- */
+
+int mdb_abi_version(void);
+const char* mdb_status_string(int status);
+
+/* Number of CUDA devices visible; 0 with MDB_ERR_NO_DEVICE when there are none. */
+int mdb_device_count(int32_t* out);
+
+/*
+ * One system.  Replaces `StepLoop.fromParsed(device, system, state, options)`,
+ * src/gpu/loop.ts:278.  Validates, splits the constraints
+ * (constraint-clusters.ts:93), derives alpha and the mesh (loop.ts:298-306),
+ * uploads, and builds the first neighbour list.
+ */
+int mdb_create(const mdb_system_desc* system, const mdb_state_desc* state,
+               const mdb_run_options* options, mdb_engine** out);
+
+/*
+ * Many independent systems advanced together, one launch per stage for all of
+ * them.  No reference counterpart: the reference runs one system per device.
+ * `systems` and `states` are arrays of `n` descriptors.
+ */
+int mdb_batch_create(int32_t n, const mdb_system_desc* systems,
+                     const mdb_state_desc* states, const mdb_run_options* options,
+                     mdb_engine** out);
+
+/* Replaces `StepLoop.destroy()`, loop.ts:1113.  `leaked_bytes` may be NULL. */
+int mdb_destroy(mdb_engine* engine, int64_t* leaked_bytes);
+
+const char* mdb_last_error(const mdb_engine* engine);
+int mdb_system_count(const mdb_engine* engine, int32_t* out);
+
+/* ---- stepping ----------------------------------------------------------- */
+
+/*
+ * Advance every system by `steps` steps.  Replaces `StepLoop.run(n)`,
+ * loop.ts:651, including the barostat attempts it makes between batches
+ * (loop.ts:662-685).
+ */
+int mdb_run(mdb_engine* engine, int64_t steps);
+
+/*
+ * `mdb_run` timed on the device with CUDA events recorded on the engine's own
+ * stream; `*device_ms` is the elapsed device time.  No reference counterpart
+ * (the reference times passes with timestamp queries, src/gpu/profile.ts:68).
+ */
+int mdb_run_timed(mdb_engine* engine, int64_t steps, double* device_ms);
+
+/* Replaces `StepLoop.advanceStepCount`, loop.ts:564. */
+int mdb_set_step(mdb_engine* engine, int64_t step);
+int mdb_get_step(const mdb_engine* engine, int64_t* step);
+
+/* ---- state in and out --------------------------------------------------- */
+
+/* Replace `StepLoop.positions()` / `velocities()`, loop.ts:900/909. */
+int mdb_get_positions(mdb_engine* engine, int32_t system, double* out);
+int mdb_get_velocities(mdb_engine* engine, int32_t system, double* out);
+
+/* Replace `StepLoop.setPositions` / `setVelocities`, loop.ts:819/842.
+ * setPositions clears the integrator's residual, as the reference does. */
+int mdb_set_positions(mdb_engine* engine, int32_t system, const double* positions);
+int mdb_set_velocities(mdb_engine* engine, int32_t system, const double* velocities);
+
+/* Replaces `StepLoop.setBox(vectors)`, loop.ts:1031; the mesh is kept. */
+int mdb_set_box(mdb_engine* engine, int32_t system, const double box[9]);
+int mdb_get_box(const mdb_engine* engine, int32_t system, double box[9]);
+int mdb_get_mesh(const mdb_engine* engine, int32_t system, int32_t mesh[3]);
+
+/* ---- evaluation ---------------------------------------------------------- */
+
+/*
+ * Forces and energies by group at the current configuration.  Replaces
+ * `StepLoop.evaluateForces()` + `report()` (loop.ts:924, 761) and the
+ * per-group evaluators `evaluateDirectSpace` (nonbonded.ts:1000),
+ * `evaluateReciprocalSpace` (pme.ts:454) and `evaluateBondedForce`
+ * (forces.ts:189).  `forces` (3N, kJ/mol/nm) and `energies` may be NULL.
+ */
+int mdb_evaluate(mdb_engine* engine, int32_t system, double* forces,
+                 mdb_energies* energies);
+
+/*
+ * Energy and forces at the given positions, leaving the engine's own state
+ * unchanged.  Replaces `StepLoop.potential(positions)`, loop.ts:870.
+ */
+int mdb_potential(mdb_engine* engine, int32_t system, const double* positions,
+                  double* forces, mdb_energies* energies);
+
+/* ---- statistics ------------------------------------------------------------ */
+
+int mdb_get_barostat_stats(const mdb_engine* engine, int32_t system,
+                           mdb_barostat_stats* out);
+int mdb_get_neighbour_stats(mdb_engine* engine, int32_t system,
+                            mdb_neighbour_stats* out);
+
+/*
+ * Device memory the engine holds, by owner label, as "label=bytes;" pairs in
+ * `buffer` (NUL-terminated, truncated to `capacity`).  Replaces
+ * `BufferPool.report()`, src/gpu/allocator.ts:69.
+ */
+int mdb_memory_report(const mdb_engine* engine, char* buffer, int64_t capacity,
+                      int64_t* total_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDB_H */
