@@ -1,0 +1,119 @@
+// device_state.h -- the device tables of one engine, passed by value to every
+// kernel, and the host-side launchers each kernel file provides.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mdb {
+
+struct BondDev { int a, b, sys; float r0, k; };
+struct AngleDev { int a, b, c, sys; float theta0, k; };
+struct TorsionDev { int a, b, c, d, sys, periodicity; float phase, k; };
+// qq values already carry ONE_4PI_EPS0 (kJ/mol nm).
+struct ExceptionDev { int a, b, sys; float qq_particles, qq_own, sigma, eps4; };
+struct RestraintDev { int p, sys; float k; long long x0, y0, z0; };
+
+// One CTA of an FFT pass: system, first line (or x / y), kz start, count.
+struct FftWork { int sys, a, b, n; };
+
+struct Dev {
+  int S;
+  const SysDev* sys;
+  RunDev run;
+  int n_atoms, n_slots, n_blocks, n_cells, n_units, n_iblk;
+
+  // atoms, original order
+  long long *px, *py, *pz;
+  float *vx, *vy, *vz;
+  float *rx, *ry, *rz;
+  float* invm;
+  int* atom_sys;
+  int* rank;      // slot of an atom within its system's sorted order
+  int* cell_of;   // global cell
+  long long *refx, *refy, *refz;
+  const float4* prm_atom;  // q*sqrt(ONE_4PI_EPS0), sigma/2, sqrt(eps), q
+
+  // slots, sorted order
+  int* order;     // global atom or -1
+  int* tmp_order;
+  int4* pc;
+  float4* prm;
+  unsigned long long *fx, *fy, *fz;
+  const int* slot_sys;
+
+  // blocks
+  float4 *bb_lo, *bb_hi;
+  int* tile_cnt;
+  int* tile_start;
+  const int* block_sys;
+
+  // cells
+  int *cell_cnt, *cell_start, *cell_cur;
+  const int* cell_sys;
+  const int* cell_map;
+
+  // tiles
+  int2* tiles;
+  unsigned int* masks;
+  int* tile_count;   // per system
+  int* tile_prefix;  // S+1
+
+  // flags and status
+  int* rebuild_flag;  // set by the integrator: some atom moved skin/2
+  int* rebuild_now;   // snapshot the rebuild kernels act on
+  int* any_rebuild;
+  int* err;           // per system ErrorBit
+  long long* rebuild_count;
+  int* global_ticket;
+
+  // exclusions (every exception pair)
+  const int2* excl;
+  const int* excl_sys;
+  int n_excl;
+
+  // listed interactions
+  const BondDev* bonds; int n_bonds;
+  const AngleDev* angles; int n_angles;
+  const TorsionDev* torsions; int n_torsions;
+  const ExceptionDev* exceptions; int n_exceptions;
+  const RestraintDev* restraints; int n_restraints;
+
+  // PME
+  unsigned long long* qgrid;
+  float2* cgrid;
+  float* phi;
+  const float* moduli;
+  const float2* twiddles;
+  double* mesh_partial;  // one per x-pass work item
+  const FftWork* fft_z; int n_fft_z;
+  const FftWork* fft_y; int n_fft_y;
+  const FftWork* fft_x; int n_fft_x;
+
+  // energies, int64 2^32 fixed, [S][kECount]
+  unsigned long long* energy;
+
+  // integrator
+  const UnitDev* units;
+  const int* iblk_sys;
+  const int* iblk_unit0;
+  const int* iblk_nunit;
+  double* mom_partial;  // 3 per integrate block
+  float4* vcom;         // per system, for the next step's COM removal
+  long long* step;      // per system
+  int* done_count;      // per system
+  int* shake_failures;
+};
+
+// ---- launchers (one per kernel file) ----
+void launch_rebuild_decide(const Dev& d, cudaStream_t s);
+void launch_rebuild_sort(const Dev& d, cudaStream_t s);     // phases 0-4
+void launch_wrap(const Dev& d, cudaStream_t s);
+void launch_rebuild_tiles(const Dev& d, cudaStream_t s);    // phases 5-9
+void launch_nonbonded(const Dev& d, bool energy, cudaStream_t s);
+void launch_listed(const Dev& d, bool energy, cudaStream_t s);
+void launch_pme(const Dev& d, bool energy, cudaStream_t s);
+void launch_integrate(const Dev& d, cudaStream_t s);
+void launch_momentum(const Dev& d, cudaStream_t s);
+
+}  // namespace mdb

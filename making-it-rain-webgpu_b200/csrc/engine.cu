@@ -1,0 +1,1065 @@
+// engine.cu -- the host runtime behind include/mdb.h.
+//
+// Owns every device table (labelled, so destroy() can report what it frees,
+// src/gpu/allocator.ts:69), three streams, and the captured CUDA graphs that
+// replace the reference's per-step command-buffer encoding
+// (src/gpu/loop.ts:715-751).  One step is
+//
+//   list kernels (return at once unless a rebuild was asked for)
+//   wrap
+//   fork:  nonbonded tiles (s0) | listed terms (s2) | PME chain (s1)
+//   join:  fused integrator (s0)
+//
+// and `max_batch` such steps are captured once and replayed.  Nothing on this
+// path runs on the CPU: the host only uploads inputs, replays graphs, and
+// reads results back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mdb.h"
+#include "device_state.h"
+#include "prep.h"
+
+namespace mdb {
+void set_pme_smem(int z, int y, int x);
+}
+
+using namespace mdb;
+
+namespace {
+
+constexpr double kCellWidth = 0.3;  // nm, fractional cells of the spatial sort
+constexpr int kIntegrateBlock = 128;
+constexpr int kFftTile = 16;
+
+struct Allocation {
+  std::string label;
+  void* ptr;
+  size_t bytes;
+};
+
+struct BarostatState {
+  double volume_scale = 0;
+  int64_t attempts = 0, accepted = 0, step = 0, draw = 0;
+  int window_attempts = 0, window_accepted = 0;
+};
+
+}  // namespace
+
+struct mdb_engine {
+  int device = 0;
+  mdb_run_options opt{};
+  RunDev run{};
+  std::vector<HostSystem> hs;
+  std::vector<SysDev> sd;
+  std::vector<BarostatState> baro;
+  Dev d{};
+  std::vector<Allocation> allocs;
+  cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
+  cudaEvent_t fork = nullptr, join1 = nullptr, join2 = nullptr, t0 = nullptr, t1 = nullptr;
+  std::map<int64_t, cudaGraphExec_t> graphs;
+  int64_t step = 0;
+  std::string error;
+  int n_mesh_items = 0;
+  std::vector<int> fft_x_sys;  // system of each x-pass work item
+};
+
+namespace {
+
+int fail(mdb_engine* e, int status, const std::string& message) {
+  if (e) e->error = message;
+  return status;
+}
+
+#define CUDA_TRY(e, call)                                                                        \
+  do {                                                                                           \
+    cudaError_t err_ = (call);                                                                   \
+    if (err_ != cudaSuccess) {                                                                   \
+      return fail(e, MDB_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(err_));      \
+    }                                                                                            \
+  } while (0)
+
+template <typename T>
+int alloc(mdb_engine* e, const char* label, T*& out, size_t count) {
+  out = nullptr;
+  const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+  void* p = nullptr;
+  cudaError_t err = cudaMalloc(&p, bytes);
+  if (err != cudaSuccess) return fail(e, MDB_ERR_DEVICE, std::string("cudaMalloc ") + label + ": " + cudaGetErrorString(err));
+  cudaMemset(p, 0, bytes);
+  e->allocs.push_back({label, p, bytes});
+  out = static_cast<T*>(p);
+  return MDB_OK;
+}
+
+template <typename T>
+int upload(mdb_engine* e, const char* label, T*& out, const std::vector<T>& host) {
+  int st = alloc(e, label, out, host.size());
+  if (st) return st;
+  if (!host.empty()) CUDA_TRY(e, cudaMemcpy(out, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return MDB_OK;
+}
+
+long long to_fixed_host(double x) { return std::llround(x * 4294967296.0); }
+
+// Morton order of the fractional cells, so consecutive slots stay compact.
+std::vector<int> morton_map(const int* dim) {
+  const int n = dim[0] * dim[1] * dim[2];
+  std::vector<std::pair<uint64_t, int>> keys(n);
+  auto spread = [](uint64_t v) {
+    uint64_t r = 0;
+    for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
+    return r;
+  };
+  for (int x = 0; x < dim[0]; ++x)
+    for (int y = 0; y < dim[1]; ++y)
+      for (int z = 0; z < dim[2]; ++z) {
+        const int id = (x * dim[1] + y) * dim[2] + z;
+        keys[id] = {spread(x) | (spread(y) << 1) | (spread(z) << 2), id};
+      }
+  std::sort(keys.begin(), keys.end());
+  std::vector<int> map(n);
+  for (int r = 0; r < n; ++r) map[keys[r].second] = r;
+  return map;
+}
+
+// Every box-dependent field of one system's device constants.
+void fill_box(const HostSystem& h, SysDev& S, bool keep_shift) {
+  const double* B = h.box.data();
+  double M[9];
+  inverse_box(B, M);
+  for (int i = 0; i < 9; ++i) {
+    S.box_f[i] = float(B[i]);
+    S.inv_f[i] = float(M[i]);
+    S.box_fx[i] = to_fixed_host(B[i]);
+    S.inv_fx[i] = to_fixed_host(M[i]);
+  }
+  S.triclinic = (B[3] != 0 || B[6] != 0 || B[7] != 0) ? 1 : 0;
+  // Pair coordinates: the folded extent plus one box stays below 2^31.
+  const double ext = std::max({B[0] + std::fabs(B[3]) + std::fabs(B[6]), B[4] + std::fabs(B[7]), B[8]});
+  int shift = int(std::floor(std::log2(std::ldexp(1.0, 30) / ext)));
+  shift = std::min(shift, 30);
+  if (!keep_shift || shift < S.pc_shift) S.pc_shift = shift;
+  const double sc = std::ldexp(1.0, S.pc_shift);
+  S.pc_inv = float(1.0 / sc);
+  for (int i = 0; i < 9; ++i) S.pc_box[i] = int(std::llround(B[i] * sc));
+  for (int k = 0; k < 3; ++k) {
+    S.pc_half[k] = S.pc_box[k * 4] / 2;
+    S.pc_inv_diag[k] = float(1.0 / S.pc_box[k * 4]);
+  }
+  // PME: u = r . (K o M)
+  const int* K = h.grid.data();
+  const double um[6] = {K[0] * M[0], K[0] * M[3], K[0] * M[6], K[1] * M[4], K[1] * M[7], K[2] * M[8]};
+  for (int i = 0; i < 6; ++i) S.umat[i] = to_fixed_host(um[i]);
+  for (int v = 0; v < 3; ++v)
+    for (int u = 0; u < 3; ++u) S.umat_f[v * 3 + u] = float(K[u] * M[v * 3 + u]);
+  const double vol = box_volume(B);
+  S.pme_pref = float(kOne4PiEps0 * 2 * 3.14159265358979323846 / vol);
+}
+
+int check_device_status(mdb_engine* e) {
+  cudaError_t err = cudaStreamSynchronize(e->s0);
+  if (err != cudaSuccess) return fail(e, MDB_ERR_DEVICE, std::string("device: ") + cudaGetErrorString(err));
+  std::vector<int> flags(e->d.S), shake(e->d.S);
+  cudaMemcpy(flags.data(), e->d.err, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost);
+  int any = 0;
+  for (int f : flags) any |= f;
+  if (any & kErrTileCapacity) return fail(e, MDB_ERR_CAPACITY, "the cluster-pair tile list ran out of room");
+  if (any & kErrTimeout) return fail(e, MDB_ERR_TIMEOUT, "a bounded device wait gave up");
+  if (any & kErrRange) return fail(e, MDB_ERR_RANGE, "a value left the fixed-point range: the run diverged");
+  return MDB_OK;
+}
+
+void launch_step(mdb_engine* e) {
+  const Dev& d = e->d;
+  launch_rebuild_sort(d, e->s0);
+  launch_wrap(d, e->s0);
+  launch_rebuild_tiles(d, e->s0);
+  cudaEventRecord(e->fork, e->s0);
+  cudaStreamWaitEvent(e->s1, e->fork, 0);
+  cudaStreamWaitEvent(e->s2, e->fork, 0);
+  launch_pme(d, false, e->s1);
+  launch_listed(d, false, e->s2);
+  launch_nonbonded(d, false, e->s0);
+  cudaEventRecord(e->join1, e->s1);
+  cudaEventRecord(e->join2, e->s2);
+  cudaStreamWaitEvent(e->s0, e->join1, 0);
+  cudaStreamWaitEvent(e->s0, e->join2, 0);
+  launch_integrate(d, e->s0);
+}
+
+int run_steps(mdb_engine* e, int64_t steps) {
+  if (steps <= 0) return MDB_OK;
+  if (e->opt.flags & MDB_FLAG_NO_GRAPH) {
+    for (int64_t k = 0; k < steps; ++k) launch_step(e);
+    CUDA_TRY(e, cudaGetLastError());
+  } else {
+    auto it = e->graphs.find(steps);
+    if (it == e->graphs.end()) {
+      cudaGraph_t g = nullptr;
+      CUDA_TRY(e, cudaStreamBeginCapture(e->s0, cudaStreamCaptureModeThreadLocal));
+      for (int64_t k = 0; k < steps; ++k) launch_step(e);
+      CUDA_TRY(e, cudaStreamEndCapture(e->s0, &g));
+      cudaGraphExec_t exec = nullptr;
+      CUDA_TRY(e, cudaGraphInstantiate(&exec, g, 0));
+      cudaGraphDestroy(g);
+      it = e->graphs.emplace(steps, exec).first;
+    }
+    CUDA_TRY(e, cudaGraphLaunch(it->second, e->s0));
+  }
+  e->step += steps;
+  return MDB_OK;
+}
+
+void request_rebuild(mdb_engine* e, int s) {
+  std::vector<int> now(e->d.S, 0);
+  cudaMemcpy(now.data(), e->d.rebuild_now, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost);
+  if (s < 0) std::fill(now.begin(), now.end(), 1);
+  else now[s] = 1;
+  const int one = 1;
+  cudaMemcpy(e->d.rebuild_now, now.data(), sizeof(int) * e->d.S, cudaMemcpyHostToDevice);
+  cudaMemcpy(e->d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice);
+}
+
+int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb_state_desc* states,
+                 const mdb_run_options* options) {
+  e->opt = *options;
+  if (e->opt.max_batch <= 0) e->opt.max_batch = 100;
+  if (!(e->opt.time_step > 0)) return fail(e, MDB_ERR_INVALID_ARGUMENT, "time_step must be positive");
+  const double skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(e, MDB_ERR_NO_DEVICE, "no CUDA device is visible");
+  e->device = e->opt.device;
+  CUDA_TRY(e, cudaSetDevice(e->device));
+
+  e->hs.resize(n);
+  for (int s = 0; s < n; ++s) {
+    std::string msg;
+    const int st = prepare_system(systems[s], states[s], e->opt, e->hs[s], msg);
+    if (st) return fail(e, st, n > 1 ? "system " + std::to_string(s) + ": " + msg : msg);
+  }
+  // run options (integrate.ts:170 packStepParams)
+  RunDev& R = e->run;
+  R.dt = float(e->opt.time_step);
+  R.velocity_scale = float(std::exp(-e->opt.time_step * e->opt.friction));
+  R.noise_scale = float(std::sqrt(1.0 - std::exp(-2.0 * e->opt.time_step * e->opt.friction)));
+  R.kt = float(kBoltzmann * e->opt.temperature);
+  R.tolerance = float(e->opt.constraint_tolerance > 0 ? e->opt.constraint_tolerance : 1e-6);
+  R.seed = e->opt.seed;
+  R.integrator = e->opt.integrator;
+  R.draw_noise = (R.noise_scale > 0 && e->opt.integrator == MDB_INTEGRATOR_LFMIDDLE) ? 1 : 0;
+  R.always_rebuild = (e->opt.flags & MDB_FLAG_ALWAYS_REBUILD) ? 1 : 0;
+
+  // ---- layout ----
+  e->sd.resize(n);
+  e->baro.resize(n);
+  std::vector<long long> px, py, pz;
+  std::vector<float> vx, vy, vz, invm;
+  std::vector<int> atom_sys, slot_sys, block_sys, cell_sys, cell_map;
+  std::vector<float4> prm_atom;
+  std::vector<int2> excl;
+  std::vector<int> excl_sys;
+  std::vector<BondDev> bonds;
+  std::vector<AngleDev> angles;
+  std::vector<TorsionDev> torsions;
+  std::vector<ExceptionDev> exceptions;
+  std::vector<RestraintDev> restraints;
+  std::vector<float> moduli;
+  std::vector<float2> twiddles;
+  std::vector<FftWork> wz, wy, wx;
+  std::vector<UnitDev> units;
+  std::vector<int> iblk_sys, iblk_unit0, iblk_nunit;
+  int atoms = 0, slots = 0, blocks = 0, cells = 0, tiles = 0, units_n = 0, iblk = 0;
+  long long grid_pts = 0, cgrid_pts = 0;
+  int smem_z = 0, smem_y = 0, smem_x = 0;
+  const float sq = float(std::sqrt(kOne4PiEps0));
+  for (int s = 0; s < n; ++s) {
+    HostSystem& h = e->hs[s];
+    SysDev& S = e->sd[s];
+    std::memset(&S, 0, sizeof(S));
+    S.n_atoms = h.n;
+    S.atom_off = atoms;
+    S.n_blocks = (h.n + 31) / 32;
+    S.n_slots = S.n_blocks * 32;
+    S.slot_off = slots;
+    S.block_off = blocks;
+    double widths[3];
+    perpendicular_widths(h.box.data(), widths);
+    for (int k = 0; k < 3; ++k) S.cdim[k] = std::max(1, int(std::floor(widths[k] / kCellWidth)));
+    S.n_cells = S.cdim[0] * S.cdim[1] * S.cdim[2];
+    S.cell_off = cells;
+    const long long all_pairs = (long long)S.n_blocks * (S.n_blocks + 1) / 2;
+    S.tile_cap = int(std::min<long long>(all_pairs, (long long)S.n_blocks * 192));
+    S.tile_off = tiles;
+    S.energy_base = s * kECount;
+    S.cut2 = float(h.cutoff * h.cutoff);
+    S.list2 = float((h.cutoff + skin) * (h.cutoff + skin));
+    S.half_skin2 = float(0.25 * skin * skin);
+    S.alpha = float(h.alpha);
+    S.alpha_2_sqrtpi = float(h.alpha * 2.0 / std::sqrt(3.14159265358979323846));
+    S.exp_scale = float(-1.0 / (4 * h.alpha * h.alpha));
+    S.com_freq = h.com_frequency;
+    S.total_mass = h.total_mass;
+    for (int k = 0; k < 3; ++k) S.grid[k] = h.grid[k];
+    S.kzh = h.grid[2] / 2 + 1;
+    S.grid_off = grid_pts;
+    S.cgrid_off = cgrid_pts;
+    S.pc_shift = 0;
+    fill_box(h, S, false);
+    grid_pts += (long long)h.grid[0] * h.grid[1] * h.grid[2];
+    cgrid_pts += (long long)h.grid[0] * h.grid[1] * S.kzh;
+    S.mod_off = int(moduli.size());
+    for (int k = 0; k < 3; ++k)
+      for (double m : bspline_moduli(h.grid[k])) moduli.push_back(float(m));
+    for (int k = 0; k < 3; ++k) {
+      plan_radices(h.grid[k], S.radices[k], &S.nradix[k]);
+      S.tw_off[k] = int(twiddles.size());
+      for (int j = 0; j < h.grid[k]; ++j) {
+        const double a = -2 * 3.14159265358979323846 * j / h.grid[k];
+        twiddles.push_back(make_float2(float(std::cos(a)), float(std::sin(a))));
+      }
+    }
+    // FFT work items
+    const int Kx = h.grid[0], Ky = h.grid[1], Kz = h.grid[2];
+    const int lines = std::max(1, 2048 / Kz);
+    for (int l = 0; l < Kx * Ky; l += lines) wz.push_back({s, l, 0, std::min(lines, Kx * Ky - l)});
+    smem_z = std::max(smem_z, 2 * lines * Kz * int(sizeof(float2)));
+    for (int x = 0; x < Kx; ++x)
+      for (int k = 0; k < S.kzh; k += kFftTile) wy.push_back({s, x, k, std::min(kFftTile, S.kzh - k)});
+    smem_y = std::max(smem_y, 2 * kFftTile * Ky * int(sizeof(float2)));
+    for (int y = 0; y < Ky; ++y)
+      for (int k = 0; k < S.kzh; k += kFftTile) {
+        wx.push_back({s, y, k, std::min(kFftTile, S.kzh - k)});
+        e->fft_x_sys.push_back(s);
+      }
+    smem_x = std::max(smem_x, 2 * kFftTile * Kx * int(sizeof(float2)));
+
+    // atoms
+    const double* pos = states[s].positions;
+    const double* vel = states[s].velocities;
+    for (int a = 0; a < h.n; ++a) {
+      px.push_back(to_fixed_host(pos[3 * a]));
+      py.push_back(to_fixed_host(pos[3 * a + 1]));
+      pz.push_back(to_fixed_host(pos[3 * a + 2]));
+      vx.push_back(vel ? float(vel[3 * a]) : 0.f);
+      vy.push_back(vel ? float(vel[3 * a + 1]) : 0.f);
+      vz.push_back(vel ? float(vel[3 * a + 2]) : 0.f);
+      invm.push_back(h.mass[a] == 0 ? 0.f : float(1.0 / h.mass[a]));
+      atom_sys.push_back(s);
+      prm_atom.push_back(make_float4(float(h.charge[a]) * sq, float(0.5 * h.sigma[a]),
+                                     float(std::sqrt(h.epsilon[a])), float(h.charge[a])));
+    }
+    for (int k = 0; k < S.n_slots; ++k) slot_sys.push_back(s);
+    for (int k = 0; k < S.n_blocks; ++k) block_sys.push_back(s);
+    for (int k = 0; k < S.n_cells; ++k) cell_sys.push_back(s);
+    const std::vector<int> mm = morton_map(S.cdim);
+    cell_map.insert(cell_map.end(), mm.begin(), mm.end());
+
+    // listed terms, global indices
+    const int off = atoms;
+    for (auto b : h.bonds) { b.a += off; b.b += off; b.sys = s; bonds.push_back(b); }
+    for (auto a : h.angles) { a.a += off; a.b += off; a.c += off; a.sys = s; angles.push_back(a); }
+    for (auto t : h.torsions) { t.a += off; t.b += off; t.c += off; t.d += off; t.sys = s; torsions.push_back(t); }
+    for (size_t k = 0; k < h.ep1.size(); ++k) {
+      ExceptionDev x;
+      x.a = h.ep1[k] + off;
+      x.b = h.ep2[k] + off;
+      x.sys = s;
+      x.qq_particles = float(kOne4PiEps0 * h.charge[h.ep1[k]] * h.charge[h.ep2[k]]);
+      x.qq_own = float(kOne4PiEps0 * h.eqq[k]);
+      x.sigma = float(h.esig[k]);
+      x.eps4 = float(4 * h.eeps[k]);
+      exceptions.push_back(x);
+      excl.push_back(make_int2(h.ep1[k] + off, h.ep2[k] + off));
+      excl_sys.push_back(s);
+    }
+    for (size_t k = 0; k < h.rparticle.size(); ++k)
+      restraints.push_back({h.rparticle[k] + off, s, float(h.rk[k]), to_fixed_host(h.rx0[k]),
+                            to_fixed_host(h.ry0[k]), to_fixed_host(h.rz0[k])});
+
+    // integration units: SETTLE waters, SHAKE clusters, free atoms
+    std::vector<UnitDev> su;
+    for (const auto& w : h.settle) {
+      UnitDev u{};
+      u.kind = kUnitSettle;
+      u.sys = s;
+      u.na = 3;
+      u.nc = 0;
+      u.atom[0] = w.central + off;
+      u.atom[1] = w.first + off;
+      u.atom[2] = w.second + off;
+      u.dist[0] = w.d1;
+      u.dist[1] = w.d2;
+      su.push_back(u);
+    }
+    for (const auto& cl : h.shake) {
+      UnitDev u{};
+      u.kind = kUnitShake;
+      u.sys = s;
+      u.na = int(cl.atoms.size());
+      u.nc = int(cl.constraints.size());
+      for (int k = 0; k < u.na; ++k) u.atom[k] = cl.atoms[k] + off;
+      for (int k = 0; k < u.nc; ++k) {
+        const int c = cl.constraints[k];
+        u.ci[k] = (unsigned char)(std::find(cl.atoms.begin(), cl.atoms.end(), h.cp1[c]) - cl.atoms.begin());
+        u.cj[k] = (unsigned char)(std::find(cl.atoms.begin(), cl.atoms.end(), h.cp2[c]) - cl.atoms.begin());
+        u.dist[k] = float(h.cdist[c]);
+      }
+      su.push_back(u);
+    }
+    for (int a : h.free_atoms) {
+      UnitDev u{};
+      u.kind = kUnitFree;
+      u.sys = s;
+      u.na = 1;
+      u.atom[0] = a + off;
+      su.push_back(u);
+    }
+    S.unit_off = units_n;
+    S.n_units = int(su.size());
+    S.iblk_off = iblk;
+    for (int u0 = 0; u0 < S.n_units; u0 += kIntegrateBlock) {
+      iblk_sys.push_back(s);
+      iblk_unit0.push_back(units_n + u0);
+      iblk_nunit.push_back(std::min(kIntegrateBlock, S.n_units - u0));
+      ++iblk;
+    }
+    S.n_iblk = iblk - S.iblk_off;
+    units.insert(units.end(), su.begin(), su.end());
+    units_n += S.n_units;
+
+    atoms += h.n;
+    slots += S.n_slots;
+    blocks += S.n_blocks;
+    cells += S.n_cells;
+    tiles += S.tile_cap;
+    e->baro[s].volume_scale = 0.01 * box_volume(h.box.data());
+    e->baro[s].step = 0;
+  }
+
+  // ---- device tables ----
+  Dev& d = e->d;
+  d.S = n;
+  d.run = e->run;
+  d.n_atoms = atoms;
+  d.n_slots = slots;
+  d.n_blocks = blocks;
+  d.n_cells = cells;
+  d.n_units = units_n;
+  d.n_iblk = iblk;
+  int st = MDB_OK;
+  SysDev* sys_dev = nullptr;
+#define TRY(x) do { st = (x); if (st) return st; } while (0)
+  TRY(upload(e, "system constants", sys_dev, e->sd));
+  d.sys = sys_dev;
+  TRY(upload(e, "positions.x", d.px, px));
+  TRY(upload(e, "positions.y", d.py, py));
+  TRY(upload(e, "positions.z", d.pz, pz));
+  TRY(upload(e, "velocities.x", d.vx, vx));
+  TRY(upload(e, "velocities.y", d.vy, vy));
+  TRY(upload(e, "velocities.z", d.vz, vz));
+  TRY(alloc(e, "residual.x", d.rx, atoms));
+  TRY(alloc(e, "residual.y", d.ry, atoms));
+  TRY(alloc(e, "residual.z", d.rz, atoms));
+  TRY(upload(e, "inverse masses", d.invm, invm));
+  TRY(upload(e, "atom system", d.atom_sys, atom_sys));
+  TRY(alloc(e, "rank", d.rank, atoms));
+  TRY(alloc(e, "cell of atom", d.cell_of, atoms));
+  TRY(alloc(e, "list reference.x", d.refx, atoms));
+  TRY(alloc(e, "list reference.y", d.refy, atoms));
+  TRY(alloc(e, "list reference.z", d.refz, atoms));
+  float4* prm_atom_dev = nullptr;
+  TRY(upload(e, "pair parameters by atom", prm_atom_dev, prm_atom));
+  d.prm_atom = prm_atom_dev;
+  TRY(alloc(e, "order", d.order, slots));
+  TRY(alloc(e, "scatter order", d.tmp_order, slots));
+  TRY(alloc(e, "pair coordinates", d.pc, slots));
+  TRY(alloc(e, "pair parameters", d.prm, slots));
+  TRY(alloc(e, "forces.x", d.fx, slots));
+  TRY(alloc(e, "forces.y", d.fy, slots));
+  TRY(alloc(e, "forces.z", d.fz, slots));
+  int* tmp_i = nullptr;
+  TRY(upload(e, "slot system", tmp_i, slot_sys));
+  d.slot_sys = tmp_i;
+  TRY(alloc(e, "block bounds lo", d.bb_lo, blocks));
+  TRY(alloc(e, "block bounds hi", d.bb_hi, blocks));
+  TRY(alloc(e, "tile row count", d.tile_cnt, blocks));
+  TRY(alloc(e, "tile row start", d.tile_start, blocks));
+  TRY(upload(e, "block system", tmp_i, block_sys));
+  d.block_sys = tmp_i;
+  TRY(alloc(e, "cell count", d.cell_cnt, cells));
+  TRY(alloc(e, "cell start", d.cell_start, cells));
+  TRY(alloc(e, "cell cursor", d.cell_cur, cells));
+  TRY(upload(e, "cell system", tmp_i, cell_sys));
+  d.cell_sys = tmp_i;
+  TRY(upload(e, "cell morton map", tmp_i, cell_map));
+  d.cell_map = tmp_i;
+  TRY(alloc(e, "tiles", d.tiles, tiles));
+  TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * 32));
+  TRY(alloc(e, "tile count", d.tile_count, n));
+  TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
+  TRY(alloc(e, "rebuild flag", d.rebuild_flag, n));
+  TRY(alloc(e, "rebuild now", d.rebuild_now, n));
+  TRY(alloc(e, "any rebuild", d.any_rebuild, 1));
+  TRY(alloc(e, "status", d.err, n));
+  TRY(alloc(e, "rebuild count", d.rebuild_count, n));
+  TRY(alloc(e, "launch ticket", d.global_ticket, 1));
+  int2* ex_dev = nullptr;
+  TRY(upload(e, "exclusions", ex_dev, excl));
+  d.excl = ex_dev;
+  TRY(upload(e, "exclusion system", tmp_i, excl_sys));
+  d.excl_sys = tmp_i;
+  d.n_excl = int(excl.size());
+  BondDev* b_dev = nullptr;
+  AngleDev* a_dev = nullptr;
+  TorsionDev* t_dev = nullptr;
+  ExceptionDev* x_dev = nullptr;
+  RestraintDev* r_dev = nullptr;
+  TRY(upload(e, "bonds", b_dev, bonds));
+  TRY(upload(e, "angles", a_dev, angles));
+  TRY(upload(e, "torsions", t_dev, torsions));
+  TRY(upload(e, "exceptions", x_dev, exceptions));
+  TRY(upload(e, "restraints", r_dev, restraints));
+  d.bonds = b_dev; d.n_bonds = int(bonds.size());
+  d.angles = a_dev; d.n_angles = int(angles.size());
+  d.torsions = t_dev; d.n_torsions = int(torsions.size());
+  d.exceptions = x_dev; d.n_exceptions = int(exceptions.size());
+  d.restraints = r_dev; d.n_restraints = int(restraints.size());
+  TRY(alloc(e, "pme charge grid", d.qgrid, size_t(grid_pts)));
+  TRY(alloc(e, "pme spectrum", d.cgrid, size_t(cgrid_pts)));
+  TRY(alloc(e, "pme potential", d.phi, size_t(grid_pts)));
+  float* mod_dev = nullptr;
+  float2* tw_dev = nullptr;
+  TRY(upload(e, "pme moduli", mod_dev, moduli));
+  TRY(upload(e, "fft twiddles", tw_dev, twiddles));
+  d.moduli = mod_dev;
+  d.twiddles = tw_dev;
+  TRY(alloc(e, "pme energy partials", d.mesh_partial, wx.size()));
+  FftWork* w_dev = nullptr;
+  TRY(upload(e, "fft z work", w_dev, wz));
+  d.fft_z = w_dev; d.n_fft_z = int(wz.size());
+  TRY(upload(e, "fft y work", w_dev, wy));
+  d.fft_y = w_dev; d.n_fft_y = int(wy.size());
+  TRY(upload(e, "fft x work", w_dev, wx));
+  d.fft_x = w_dev; d.n_fft_x = int(wx.size());
+  e->n_mesh_items = int(wx.size());
+  TRY(alloc(e, "energies", d.energy, size_t(n) * kECount));
+  UnitDev* u_dev = nullptr;
+  TRY(upload(e, "integration units", u_dev, units));
+  d.units = u_dev;
+  TRY(upload(e, "integrate block system", tmp_i, iblk_sys));
+  d.iblk_sys = tmp_i;
+  TRY(upload(e, "integrate block unit", tmp_i, iblk_unit0));
+  d.iblk_unit0 = tmp_i;
+  TRY(upload(e, "integrate block count", tmp_i, iblk_nunit));
+  d.iblk_nunit = tmp_i;
+  TRY(alloc(e, "momentum partials", d.mom_partial, size_t(iblk) * 3));
+  TRY(alloc(e, "com velocity", d.vcom, n));
+  std::vector<long long> steps(n);
+  for (int s = 0; s < n; ++s) steps[s] = states[s].step;
+  TRY(upload(e, "step", d.step, steps));
+  TRY(alloc(e, "done count", d.done_count, n));
+  TRY(alloc(e, "constraint failures", d.shake_failures, n));
+#undef TRY
+  e->step = states[0].step;
+  set_pme_smem(smem_z, smem_y, smem_x);
+
+  CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking));
+  CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s1, cudaStreamNonBlocking));
+  CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s2, cudaStreamNonBlocking));
+  CUDA_TRY(e, cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+  CUDA_TRY(e, cudaEventCreateWithFlags(&e->join1, cudaEventDisableTiming));
+  CUDA_TRY(e, cudaEventCreateWithFlags(&e->join2, cudaEventDisableTiming));
+  CUDA_TRY(e, cudaEventCreate(&e->t0));
+  CUDA_TRY(e, cudaEventCreate(&e->t1));
+  CUDA_TRY(e, cudaDeviceSynchronize());
+
+  // first list and the first COM velocity
+  request_rebuild(e, -1);
+  launch_rebuild_sort(d, e->s0);
+  launch_wrap(d, e->s0);
+  launch_rebuild_tiles(d, e->s0);
+  launch_momentum(d, e->s0);
+  CUDA_TRY(e, cudaGetLastError());
+  return check_device_status(e);
+}
+
+int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
+  const Dev& d = e->d;
+  const HostSystem& h = e->hs[s];
+  const SysDev& S = e->sd[s];
+  CUDA_TRY(e, cudaMemsetAsync(d.energy, 0, sizeof(unsigned long long) * d.S * kECount, e->s0));
+  launch_rebuild_sort(d, e->s0);
+  launch_wrap(d, e->s0);
+  launch_rebuild_tiles(d, e->s0);
+  launch_pme(d, true, e->s0);
+  launch_listed(d, true, e->s0);
+  launch_nonbonded(d, true, e->s0);
+  CUDA_TRY(e, cudaGetLastError());
+  int st = check_device_status(e);
+  if (st) return st;
+  if (forces) {
+    std::vector<unsigned long long> f[3];
+    std::vector<int> order(S.n_slots);
+    for (auto& v : f) v.resize(S.n_slots);
+    cudaMemcpy(f[0].data(), d.fx + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost);
+    cudaMemcpy(f[1].data(), d.fy + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost);
+    cudaMemcpy(f[2].data(), d.fz + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost);
+    cudaMemcpy(order.data(), d.order + S.slot_off, sizeof(int) * S.n_slots, cudaMemcpyDeviceToHost);
+    for (int k = 0; k < S.n_slots; ++k) {
+      const int a = order[k];
+      if (a < 0) continue;
+      const int local = a - S.atom_off;
+      for (int ax = 0; ax < 3; ++ax) forces[3 * local + ax] = double((long long)f[ax][k]) / 4294967296.0;
+    }
+  }
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    std::vector<unsigned long long> en(kECount);
+    cudaMemcpy(en.data(), d.energy + S.energy_base, sizeof(long long) * kECount, cudaMemcpyDeviceToHost);
+    auto val = [&](int k) { return double((long long)en[k]) / 4294967296.0; };
+    std::vector<double> mesh(e->n_mesh_items);
+    cudaMemcpy(mesh.data(), d.mesh_partial, sizeof(double) * e->n_mesh_items, cudaMemcpyDeviceToHost);
+    double em = 0;
+    for (int k = 0; k < e->n_mesh_items; ++k)
+      if (e->fft_x_sys[k] == s) em += mesh[k];
+    out->bond = val(kEBond);
+    out->angle = val(kEAngle);
+    out->torsion = val(kETorsion);
+    out->restraint = val(kERestraint);
+    out->direct_coulomb = val(kECoulomb);
+    out->direct_lj = val(kELj);
+    out->exclusion_correction = val(kEExclusion);
+    out->exceptions = val(kEException);
+    out->dispersion = h.dispersion_energy;
+    out->reciprocal_mesh = em;
+    out->self_energy = h.self_energy;
+    out->net_charge = h.net_charge_energy;
+    out->direct_group = out->direct_coulomb + out->direct_lj + out->exclusion_correction + out->exceptions +
+                        out->dispersion;
+    out->reciprocal_group = out->reciprocal_mesh + out->self_energy + out->net_charge;
+    out->potential = out->bond + out->angle + out->torsion + out->restraint + out->direct_group +
+                     out->reciprocal_group;
+    // kinetic energy from the velocities as they are (kinetic.ts:31)
+    std::vector<float> v[3];
+    for (auto& x : v) x.resize(h.n);
+    cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+    double ke = 0;
+    for (int a = 0; a < h.n; ++a)
+      if (h.mass[a] > 0)
+        ke += h.mass[a] * (double(v[0][a]) * v[0][a] + double(v[1][a]) * v[1][a] + double(v[2][a]) * v[2][a]);
+    out->kinetic = 0.5 * ke;
+    out->degrees_of_freedom = h.dof;
+    out->temperature = h.dof > 0 ? 2 * out->kinetic / (h.dof * kBoltzmann) : 0;
+  }
+  // the step loop expects cleared accumulators
+  CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, e->s0));
+  CUDA_TRY(e, cudaMemsetAsync(d.fy, 0, sizeof(long long) * d.n_slots, e->s0));
+  CUDA_TRY(e, cudaMemsetAsync(d.fz, 0, sizeof(long long) * d.n_slots, e->s0));
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  return MDB_OK;
+}
+
+int get_positions(mdb_engine* e, int s, double* out) {
+  const SysDev& S = e->sd[s];
+  const int n = S.n_atoms;
+  std::vector<long long> p[3];
+  for (auto& v : p) v.resize(n);
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  cudaMemcpy(p[0].data(), e->d.px + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(p[1].data(), e->d.py + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(p[2].data(), e->d.pz + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+  for (int a = 0; a < n; ++a)
+    for (int k = 0; k < 3; ++k) out[3 * a + k] = double(p[k][a]) / 4294967296.0;
+  return MDB_OK;
+}
+
+int set_positions(mdb_engine* e, int s, const double* in, bool clear_residual) {
+  const SysDev& S = e->sd[s];
+  const int n = S.n_atoms;
+  std::vector<long long> p[3];
+  for (auto& v : p) v.resize(n);
+  for (int a = 0; a < n; ++a)
+    for (int k = 0; k < 3; ++k) {
+      if (!std::isfinite(in[3 * a + k]) || std::fabs(in[3 * a + k]) > 1.0e6)
+        return fail(e, MDB_ERR_RANGE, "positions must be finite and inside the fixed-point range");
+      p[k][a] = to_fixed_host(in[3 * a + k]);
+    }
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  cudaMemcpy(e->d.px + S.atom_off, p[0].data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(e->d.py + S.atom_off, p[1].data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(e->d.pz + S.atom_off, p[2].data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
+  if (clear_residual) {
+    cudaMemset(e->d.rx + S.atom_off, 0, sizeof(float) * n);
+    cudaMemset(e->d.ry + S.atom_off, 0, sizeof(float) * n);
+    cudaMemset(e->d.rz + S.atom_off, 0, sizeof(float) * n);
+  }
+  request_rebuild(e, s);
+  return MDB_OK;
+}
+
+int set_box(mdb_engine* e, int s, const double* box) {
+  HostSystem& h = e->hs[s];
+  double reduced[9];
+  if (!reduce_box(box, reduced)) return fail(e, MDB_ERR_INVALID_ARGUMENT, "degenerate box");
+  double widths[3];
+  perpendicular_widths(reduced, widths);
+  if (h.cutoff > 0.5 * std::min({widths[0], widths[1], widths[2]}))
+    return fail(e, MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX, "the cutoff does not fit the new box");
+  std::copy(reduced, reduced + 9, h.box.begin());
+  update_box_constants(h);
+  fill_box(h, e->sd[s], true);
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys) + s, &e->sd[s], sizeof(SysDev), cudaMemcpyHostToDevice));
+  request_rebuild(e, s);
+  return MDB_OK;
+}
+
+// One Monte Carlo volume move (src/gpu/loop.ts:602-641, src/reference/barostat.ts:210-274).
+int barostat_attempt(mdb_engine* e, int s) {
+  HostSystem& h = e->hs[s];
+  BarostatState& b = e->baro[s];
+  const int n = h.n;
+  std::vector<double> pos(3 * n);
+  int st = get_positions(e, s, pos.data());
+  if (st) return st;
+  mdb_energies e0{};
+  if ((st = evaluate(e, s, nullptr, &e0))) return st;
+  auto uniform = [&]() {
+    // threefry2x32([draw, seed], [BAROSTAT_DOMAIN, 0]) (loop.ts:614-622)
+    uint32_t c0 = uint32_t(b.draw++), c1 = e->opt.seed, k0 = 0x6a09e667u, k1 = 0;
+    static const int rot[8] = {13, 15, 26, 6, 17, 29, 16, 24};
+    const uint32_t ks[3] = {k0, k1, 0x1bd11bdau ^ k0 ^ k1};
+    uint32_t x0 = c0 + ks[0], x1 = c1 + ks[1];
+    for (int r = 0; r < 20; ++r) {
+      x0 += x1;
+      x1 = ((x1 << rot[r % 8]) | (x1 >> (32 - rot[r % 8]))) ^ x0;
+      if ((r + 1) % 4 == 0) {
+        const uint32_t inj = uint32_t((r + 1) / 4);
+        x0 += ks[inj % 3];
+        x1 += ks[(inj + 1) % 3] + inj;
+      }
+    }
+    return (double(x0 >> 9) + 0.5) * std::ldexp(1.0, -23);
+  };
+  const double volume = box_volume(h.box.data());
+  const double dv = b.volume_scale * 2 * (uniform() - 0.5);
+  const double nv = volume + dv;
+  const double scale = std::cbrt(nv / volume);
+  std::vector<double> trial(pos);
+  for (const auto& mol : h.molecules) {
+    double c[3] = {0, 0, 0};
+    for (int a : mol)
+      for (int k = 0; k < 3; ++k) c[k] += pos[3 * a + k];
+    for (int k = 0; k < 3; ++k) {
+      const double mean = c[k] / double(mol.size());
+      const double off = scale * mean - mean;
+      for (int a : mol) trial[3 * a + k] += off;
+    }
+  }
+  const std::array<double, 9> old_box = h.box;
+  double new_box[9];
+  for (int i = 0; i < 9; ++i) new_box[i] = old_box[i] * scale;
+  if ((st = set_box(e, s, new_box))) return st;
+  if ((st = set_positions(e, s, trial.data(), false))) return st;
+  mdb_energies e1{};
+  if ((st = evaluate(e, s, nullptr, &e1))) return st;
+  const double pressure = h.barostat_pressure * 0.06022140762081242;
+  const double kT = kBoltzmann * h.barostat_temperature;
+  const double w = e1.potential - e0.potential + pressure * dv - double(h.molecules.size()) * kT * std::log(nv / volume);
+  const bool accepted = !(w > 0 && uniform() > std::exp(-w / kT));
+  b.attempts++;
+  b.window_attempts++;
+  if (accepted) {
+    b.accepted++;
+    b.window_accepted++;
+  } else {
+    if ((st = set_box(e, s, old_box.data()))) return st;
+    if ((st = set_positions(e, s, pos.data(), false))) return st;
+  }
+  if (b.window_attempts >= 10) {
+    if (b.window_accepted < 0.25 * b.window_attempts) {
+      b.volume_scale /= 1.1;
+      b.window_attempts = b.window_accepted = 0;
+    } else if (b.window_accepted > 0.75 * b.window_attempts) {
+      b.volume_scale = std::min(b.volume_scale * 1.1, volume * 0.3);
+      b.window_attempts = b.window_accepted = 0;
+    }
+  }
+  return MDB_OK;
+}
+
+int run(mdb_engine* e, int64_t steps) {
+  int freq = 0;
+  for (const auto& h : e->hs)
+    if (h.barostat_frequency > 0) freq = freq == 0 ? h.barostat_frequency : std::min(freq, h.barostat_frequency);
+  int64_t remaining = steps;
+  while (remaining > 0) {
+    int64_t chunk = std::min<int64_t>(remaining, e->opt.max_batch);
+    if (freq > 0) {
+      int64_t until = chunk;
+      for (size_t s = 0; s < e->hs.size(); ++s)
+        if (e->hs[s].barostat_frequency > 0)
+          until = std::min<int64_t>(until, std::max<int64_t>(1, e->hs[s].barostat_frequency - e->baro[s].step));
+      chunk = until;
+    }
+    int st = run_steps(e, chunk);
+    if (st) return st;
+    remaining -= chunk;
+    if (freq > 0) {
+      for (size_t s = 0; s < e->hs.size(); ++s) {
+        auto& h = e->hs[s];
+        auto& b = e->baro[s];
+        if (h.barostat_frequency <= 0) continue;
+        b.step += chunk;  // barostat.ts:129 barostatActsAfterSteps
+        if (b.step < h.barostat_frequency) continue;
+        b.step -= h.barostat_frequency;
+        if ((st = barostat_attempt(e, int(s)))) return st;
+      }
+    }
+  }
+  return check_device_status(e);
+}
+
+bool bad_system(const mdb_engine* e, int32_t s) { return !e || s < 0 || s >= int32_t(e->hs.size()); }
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+int mdb_abi_version(void) { return MDB_ABI_VERSION; }
+
+const char* mdb_status_string(int status) {
+  switch (status) {
+    case MDB_OK: return "ok";
+    case MDB_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case MDB_ERR_UNSUPPORTED_FORCE: return "unsupported force";
+    case MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX: return "cutoff too large for box";
+    case MDB_ERR_CLUSTER_TOO_LARGE: return "constraint cluster too large";
+    case MDB_ERR_NOT_CONVERGED: return "constraints did not converge";
+    case MDB_ERR_CAPACITY: return "device table capacity exceeded";
+    case MDB_ERR_RANGE: return "fixed-point range exceeded";
+    case MDB_ERR_DEVICE: return "device error";
+    case MDB_ERR_TIMEOUT: return "device wait timed out";
+    case MDB_ERR_NO_DEVICE: return "no CUDA device";
+    case MDB_ERR_NOT_SMOOTH: return "mesh size not 2/3/5/7-smooth";
+    case MDB_ERR_DEVICE_LOST: return "device lost";
+    default: return "unknown status";
+  }
+}
+
+int mdb_device_count(int32_t* out) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+  if (out) *out = n;
+  return n > 0 ? MDB_OK : MDB_ERR_NO_DEVICE;
+}
+
+int mdb_batch_create(int32_t n, const mdb_system_desc* systems, const mdb_state_desc* states,
+                     const mdb_run_options* options, mdb_engine** out) {
+  if (!out || n <= 0 || !systems || !states || !options) return MDB_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  auto* e = new mdb_engine();
+  const int st = build_engine(e, n, systems, states, options);
+  *out = e;  // returned even on failure so mdb_last_error can explain; caller destroys
+  return st;
+}
+
+int mdb_create(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
+               mdb_engine** out) {
+  return mdb_batch_create(1, system, state, options, out);
+}
+
+int mdb_destroy(mdb_engine* e, int64_t* leaked_bytes) {
+  if (!e) return MDB_ERR_INVALID_ARGUMENT;
+  if (e->s0) cudaStreamSynchronize(e->s0);
+  for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+  int64_t leaked = 0;
+  for (auto& a : e->allocs)
+    if (cudaFree(a.ptr) != cudaSuccess) leaked += int64_t(a.bytes);
+  for (cudaEvent_t ev : {e->fork, e->join1, e->join2, e->t0, e->t1})
+    if (ev) cudaEventDestroy(ev);
+  for (cudaStream_t s : {e->s0, e->s1, e->s2})
+    if (s) cudaStreamDestroy(s);
+  if (leaked_bytes) *leaked_bytes = leaked;
+  delete e;
+  return MDB_OK;
+}
+
+const char* mdb_last_error(const mdb_engine* e) { return e ? e->error.c_str() : "no engine"; }
+
+int mdb_system_count(const mdb_engine* e, int32_t* out) {
+  if (!e || !out) return MDB_ERR_INVALID_ARGUMENT;
+  *out = int32_t(e->hs.size());
+  return MDB_OK;
+}
+
+int mdb_run(mdb_engine* e, int64_t steps) {
+  if (!e || steps < 0) return MDB_ERR_INVALID_ARGUMENT;
+  return run(e, steps);
+}
+
+int mdb_run_timed(mdb_engine* e, int64_t steps, double* device_ms) {
+  if (!e || steps < 0 || !device_ms) return MDB_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  CUDA_TRY(e, cudaEventRecord(e->t0, e->s0));
+  int st = run(e, steps);
+  if (st) return st;
+  CUDA_TRY(e, cudaEventRecord(e->t1, e->s0));
+  CUDA_TRY(e, cudaEventSynchronize(e->t1));
+  float ms = 0;
+  CUDA_TRY(e, cudaEventElapsedTime(&ms, e->t0, e->t1));
+  *device_ms = ms;
+  return MDB_OK;
+}
+
+int mdb_set_step(mdb_engine* e, int64_t step) {
+  if (!e || step < 0) return MDB_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  std::vector<long long> v(e->d.S, step);
+  CUDA_TRY(e, cudaMemcpy(e->d.step, v.data(), sizeof(long long) * e->d.S, cudaMemcpyHostToDevice));
+  e->step = step;
+  return MDB_OK;
+}
+
+int mdb_get_step(const mdb_engine* e, int64_t* step) {
+  if (!e || !step) return MDB_ERR_INVALID_ARGUMENT;
+  *step = e->step;
+  return MDB_OK;
+}
+
+int mdb_get_positions(mdb_engine* e, int32_t s, double* out) {
+  if (bad_system(e, s) || !out) return MDB_ERR_INVALID_ARGUMENT;
+  return get_positions(e, s, out);
+}
+
+int mdb_get_velocities(mdb_engine* e, int32_t s, double* out) {
+  if (bad_system(e, s) || !out) return MDB_ERR_INVALID_ARGUMENT;
+  const SysDev& S = e->sd[s];
+  const int n = S.n_atoms;
+  std::vector<float> v[3];
+  for (auto& x : v) x.resize(n);
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  cudaMemcpy(v[0].data(), e->d.vx + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(v[1].data(), e->d.vy + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(v[2].data(), e->d.vz + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  for (int a = 0; a < n; ++a)
+    for (int k = 0; k < 3; ++k) out[3 * a + k] = v[k][a];
+  return MDB_OK;
+}
+
+int mdb_set_positions(mdb_engine* e, int32_t s, const double* positions) {
+  if (bad_system(e, s) || !positions) return MDB_ERR_INVALID_ARGUMENT;
+  return set_positions(e, s, positions, true);
+}
+
+int mdb_set_velocities(mdb_engine* e, int32_t s, const double* velocities) {
+  if (bad_system(e, s) || !velocities) return MDB_ERR_INVALID_ARGUMENT;
+  const SysDev& S = e->sd[s];
+  const int n = S.n_atoms;
+  std::vector<float> v[3];
+  for (auto& x : v) x.resize(n);
+  for (int a = 0; a < n; ++a)
+    for (int k = 0; k < 3; ++k) v[k][a] = float(velocities[3 * a + k]);
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  cudaMemcpy(e->d.vx + S.atom_off, v[0].data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(e->d.vy + S.atom_off, v[1].data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(e->d.vz + S.atom_off, v[2].data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  launch_momentum(e->d, e->s0);
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  return MDB_OK;
+}
+
+int mdb_set_box(mdb_engine* e, int32_t s, const double box[9]) {
+  if (bad_system(e, s) || !box) return MDB_ERR_INVALID_ARGUMENT;
+  return set_box(e, s, box);
+}
+
+int mdb_get_box(const mdb_engine* e, int32_t s, double box[9]) {
+  if (bad_system(e, s) || !box) return MDB_ERR_INVALID_ARGUMENT;
+  std::copy(e->hs[s].box.begin(), e->hs[s].box.end(), box);
+  return MDB_OK;
+}
+
+int mdb_get_mesh(const mdb_engine* e, int32_t s, int32_t mesh[3]) {
+  if (bad_system(e, s) || !mesh) return MDB_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 3; ++k) mesh[k] = e->hs[s].grid[k];
+  return MDB_OK;
+}
+
+int mdb_evaluate(mdb_engine* e, int32_t s, double* forces, mdb_energies* energies) {
+  if (bad_system(e, s)) return MDB_ERR_INVALID_ARGUMENT;
+  return evaluate(e, s, forces, energies);
+}
+
+int mdb_potential(mdb_engine* e, int32_t s, const double* positions, double* forces, mdb_energies* energies) {
+  if (bad_system(e, s) || !positions) return MDB_ERR_INVALID_ARGUMENT;
+  const int n = e->hs[s].n;
+  std::vector<double> saved(3 * n);
+  int st = get_positions(e, s, saved.data());
+  if (st) return st;
+  if ((st = set_positions(e, s, positions, false))) return st;
+  st = evaluate(e, s, forces, energies);
+  const int restore = set_positions(e, s, saved.data(), false);
+  return st ? st : restore;
+}
+
+int mdb_get_barostat_stats(const mdb_engine* e, int32_t s, mdb_barostat_stats* out) {
+  if (bad_system(e, s) || !out) return MDB_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  out->attempts = e->baro[s].attempts;
+  out->accepted = e->baro[s].accepted;
+  out->volume_scale = e->baro[s].volume_scale;
+  out->exact_evaluations = 2 * e->baro[s].attempts;
+  return MDB_OK;
+}
+
+int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) {
+  if (bad_system(e, s) || !out) return MDB_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  long long rebuilds = 0;
+  int tiles = 0, err = 0;
+  cudaMemcpy(&rebuilds, e->d.rebuild_count + s, sizeof(long long), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&tiles, e->d.tile_count + s, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&err, e->d.err + s, sizeof(int), cudaMemcpyDeviceToHost);
+  out->rebuilds = rebuilds;
+  out->tiles = tiles;
+  out->tile_capacity = e->sd[s].tile_cap;
+  out->blocks = e->sd[s].n_blocks;
+  out->overflowed = (err & kErrTileCapacity) ? 1 : 0;
+  out->skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
+  return MDB_OK;
+}
+
+int mdb_memory_report(const mdb_engine* e, char* buffer, int64_t capacity, int64_t* total_bytes) {
+  if (!e) return MDB_ERR_INVALID_ARGUMENT;
+  std::ostringstream os;
+  int64_t total = 0;
+  for (const auto& a : e->allocs) {
+    os << a.label << "=" << a.bytes << ";";
+    total += int64_t(a.bytes);
+  }
+  if (total_bytes) *total_bytes = total;
+  if (buffer && capacity > 0) {
+    const std::string s = os.str();
+    const size_t n = std::min<size_t>(s.size(), size_t(capacity - 1));
+    std::memcpy(buffer, s.data(), n);
+    buffer[n] = '\0';
+  }
+  return MDB_OK;
+}
+
+}  // extern "C"

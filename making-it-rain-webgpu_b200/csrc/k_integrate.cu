@@ -1,0 +1,425 @@
+// k_integrate.cu -- one fused launch for the whole integrator step.
+//
+// The reference splits LFMiddle into kick -> RATTLE/SETTLE-v -> drift ->
+// SHAKE/SETTLE -> finish, one dispatch each, because its constraint solvers
+// are separate passes (src/gpu/kernels/integrate.wgsl:140-203, settle.wgsl,
+// shake.wgsl; oracle src/reference/integrator.ts:140-220).  Constraints never
+// couple two clusters, so here one thread owns one *integration unit* -- a
+// SETTLE water, a SHAKE cluster (<= 8 atoms, <= 8 constraints), or a free atom
+// -- and carries it through every phase in registers:
+//
+//   COM removal (com-motion.ts:48, on removesOnStep)
+//   kick          v += dt F / m
+//   SETTLE-v / RATTLE
+//   drift         x' = x + v dt/2 (+ residual); v = e^{-g dt} v + noise; x' += v dt/2
+//   SETTLE / SHAKE (Jacobi, reference bond vectors, FP64 convergence test)
+//   finish        v += (x'' - x')/dt; x = x''
+//
+// and then the things the next step needs: the displacement test that asks for
+// a neighbour-list rebuild (verlet.wgsl:57), the momentum for the next COM
+// removal (a fixed-order FP64 reduction, so it is deterministic), the step
+// counter, and the rebuild decision, all by the last block to finish.
+// Positions are int64 fixed point with residual feedback (integrate.wgsl:40),
+// velocities f32, thermostat noise Threefry-2x32-20 (random.wgsl:78).
+#include "device_state.h"
+
+namespace mdb {
+namespace {
+
+constexpr int kThreads = 128;
+
+struct Atom {
+  long long x, y, z;  // start-of-step position (reference for the constraints)
+  float vx, vy, vz;
+  float im;
+  float rx, ry, rz;
+  float fx, fy, fz;
+};
+
+__device__ __forceinline__ float3 rel(const Atom& a, const Atom& o) {
+  return make_float3(from_fixed(a.x - o.x), from_fixed(a.y - o.y), from_fixed(a.z - o.z));
+}
+
+// src/reference/settle.ts:198 -- exact 3x3 impulse solve for the velocities.
+__device__ void settle_velocities(Atom* at) {
+  const float mA = at[0].im > 0 ? 1.f / at[0].im : 0.f, mB = at[1].im > 0 ? 1.f / at[1].im : 0.f,
+              mC = at[2].im > 0 ? 1.f / at[2].im : 0.f;
+  const float3 pB = rel(at[1], at[0]), pC = rel(at[2], at[0]);
+  auto unit = [](float3 v) {
+    const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+    return make_float3(v.x * inv, v.y * inv, v.z * inv);
+  };
+  const float3 eAB = unit(pB);
+  const float3 eBC = unit(make_float3(pC.x - pB.x, pC.y - pB.y, pC.z - pB.z));
+  const float3 eCA = unit(make_float3(-pC.x, -pC.y, -pC.z));
+  auto relv = [&](int from, int to, float3 e) {
+    return (at[to].vx - at[from].vx) * e.x + (at[to].vy - at[from].vy) * e.y + (at[to].vz - at[from].vz) * e.z;
+  };
+  const float vAB = relv(0, 1, eAB), vBC = relv(1, 2, eBC), vCA = relv(2, 0, eCA);
+  auto dot = [](float3 p, float3 q) { return p.x * q.x + p.y * q.y + p.z * q.z; };
+  const float cA = -dot(eAB, eCA), cB = -dot(eAB, eBC), cC = -dot(eBC, eCA);
+  const float s2A = 1.f - cA * cA, s2B = 1.f - cB * cB, s2C = 1.f - cC * cC;
+  const float mi = 1.f / (mA * mB * mC);
+  const float den = (((s2A * mB + s2B * mA) * mC + (s2A * mB * mB + 2.f * (cA * cB * cC + 1.f) * mA * mB + s2B * mA * mA)) * mC +
+                     s2C * mA * mB * (mA + mB)) * mi;
+  const float tab = ((cB * cC * mA - cA * mB - cA * mC) * vCA + (cA * cC * mB - cB * mC - cB * mA) * vBC +
+                     (s2C * mA * mA * mB * mB * mi + (mA + mB + mC)) * vAB) / den;
+  const float tbc = ((cA * cB * mC - cC * mB - cC * mA) * vCA + (s2A * mB * mB * mC * mC * mi + (mA + mB + mC)) * vBC +
+                     (cA * cC * mB - cB * mA - cB * mC) * vAB) / den;
+  const float tca = ((s2B * mA * mA * mC * mC * mi + (mA + mB + mC)) * vCA + (cA * cB * mC - cC * mB - cC * mA) * vBC +
+                     (cB * cC * mA - cA * mB - cA * mC) * vAB) / den;
+  at[0].vx += (eAB.x * tab - eCA.x * tca) * at[0].im;
+  at[0].vy += (eAB.y * tab - eCA.y * tca) * at[0].im;
+  at[0].vz += (eAB.z * tab - eCA.z * tca) * at[0].im;
+  at[1].vx += (eBC.x * tbc - eAB.x * tab) * at[1].im;
+  at[1].vy += (eBC.y * tbc - eAB.y * tab) * at[1].im;
+  at[1].vz += (eBC.z * tbc - eAB.z * tab) * at[1].im;
+  at[2].vx += (eCA.x * tca - eBC.x * tbc) * at[2].im;
+  at[2].vy += (eCA.y * tca - eBC.y * tbc) * at[2].im;
+  at[2].vz += (eCA.z * tca - eBC.z * tbc) * at[2].im;
+}
+
+// src/reference/settle.ts:31 -- Miyamoto & Kollman in the reference frame.
+// `dp` holds each atom's trial displacement from its start position on input
+// and its constrained displacement on output.
+__device__ void settle_positions(const Atom* at, float3* dp, float d1, float d2) {
+  const float m0 = 1.f / at[0].im, m1 = 1.f / at[1].im, m2 = 1.f / at[2].im;
+  const float3 b0 = rel(at[1], at[0]), c0 = rel(at[2], at[0]);
+  const float xb0 = b0.x, yb0 = b0.y, zb0 = b0.z, xc0 = c0.x, yc0 = c0.y, zc0 = c0.z;
+  const float itm = 1.f / (m0 + m1 + m2);
+  const float xcom = (dp[0].x * m0 + (xb0 + dp[1].x) * m1 + (xc0 + dp[2].x) * m2) * itm;
+  const float ycom = (dp[0].y * m0 + (yb0 + dp[1].y) * m1 + (yc0 + dp[2].y) * m2) * itm;
+  const float zcom = (dp[0].z * m0 + (zb0 + dp[1].z) * m1 + (zc0 + dp[2].z) * m2) * itm;
+  const float xa1 = dp[0].x - xcom, ya1 = dp[0].y - ycom, za1 = dp[0].z - zcom;
+  const float xb1 = xb0 + dp[1].x - xcom, yb1 = yb0 + dp[1].y - ycom, zb1 = zb0 + dp[1].z - zcom;
+  const float xc1 = xc0 + dp[2].x - xcom, yc1 = yc0 + dp[2].y - ycom, zc1 = zc0 + dp[2].z - zcom;
+  const float xZ = yb0 * zc0 - zb0 * yc0, yZ = zb0 * xc0 - xb0 * zc0, zZ = xb0 * yc0 - yb0 * xc0;
+  const float xX = ya1 * zZ - za1 * yZ, yX = za1 * xZ - xa1 * zZ, zX = xa1 * yZ - ya1 * xZ;
+  const float xY = yZ * zX - zZ * yX, yY = zZ * xX - xZ * zX, zY = xZ * yX - yZ * xX;
+  const float ilx = rsqrtf(xX * xX + yX * yX + zX * zX);
+  const float ily = rsqrtf(xY * xY + yY * yY + zY * zY);
+  const float ilz = rsqrtf(xZ * xZ + yZ * yZ + zZ * zZ);
+  const float t11 = xX * ilx, t21 = yX * ilx, t31 = zX * ilx;
+  const float t12 = xY * ily, t22 = yY * ily, t32 = zY * ily;
+  const float t13 = xZ * ilz, t23 = yZ * ilz, t33 = zZ * ilz;
+  const float xb0d = t11 * xb0 + t21 * yb0 + t31 * zb0, yb0d = t12 * xb0 + t22 * yb0 + t32 * zb0;
+  const float xc0d = t11 * xc0 + t21 * yc0 + t31 * zc0, yc0d = t12 * xc0 + t22 * yc0 + t32 * zc0;
+  const float za1d = t13 * xa1 + t23 * ya1 + t33 * za1;
+  const float xb1d = t11 * xb1 + t21 * yb1 + t31 * zb1, yb1d = t12 * xb1 + t22 * yb1 + t32 * zb1;
+  const float zb1d = t13 * xb1 + t23 * yb1 + t33 * zb1;
+  const float xc1d = t11 * xc1 + t21 * yc1 + t31 * zc1, yc1d = t12 * xc1 + t22 * yc1 + t32 * zc1;
+  const float zc1d = t13 * xc1 + t23 * yc1 + t33 * zc1;
+  const float rc = 0.5f * d2;
+  float rb = sqrtf(d1 * d1 - rc * rc);
+  const float ra = rb * (m1 + m2) * itm;
+  rb -= ra;
+  const float sinphi = za1d / ra, cosphi = sqrtf(fmaxf(0.f, 1.f - sinphi * sinphi));
+  const float sinpsi = (zb1d - zc1d) / (2.f * rc * cosphi), cospsi = sqrtf(fmaxf(0.f, 1.f - sinpsi * sinpsi));
+  const float ya2d = ra * cosphi;
+  float xb2d = -rc * cospsi;
+  const float yb2d = -rb * cosphi - rc * sinpsi * sinphi, yc2d = -rb * cosphi + rc * sinpsi * sinphi;
+  const float xb2d2 = xb2d * xb2d;
+  const float hh2 = 4.f * xb2d2 + (yb2d - yc2d) * (yb2d - yc2d) + (zb1d - zc1d) * (zb1d - zc1d);
+  const float deltx = 2.f * xb2d + sqrtf(fmaxf(0.f, 4.f * xb2d2 - hh2 + d2 * d2));
+  xb2d -= deltx * 0.5f;
+  const float al = xb2d * (xb0d - xc0d) + yb0d * yb2d + yc0d * yc2d;
+  const float be = xb2d * (yc0d - yb0d) + xb0d * yb2d + xc0d * yc2d;
+  const float ga = xb0d * yb1d - xb1d * yb0d + xc0d * yc1d - xc1d * yc0d;
+  const float a2b2 = al * al + be * be;
+  const float sinth = (al * ga - be * sqrtf(fmaxf(0.f, a2b2 - ga * ga))) / a2b2;
+  const float costh = sqrtf(fmaxf(0.f, 1.f - sinth * sinth));
+  const float xa3d = -ya2d * sinth, ya3d = ya2d * costh, za3d = za1d;
+  const float xb3d = xb2d * costh - yb2d * sinth, yb3d = xb2d * sinth + yb2d * costh, zb3d = zb1d;
+  const float xc3d = -xb2d * costh - yc2d * sinth, yc3d = -xb2d * sinth + yc2d * costh, zc3d = zc1d;
+  dp[0] = make_float3(xcom + t11 * xa3d + t12 * ya3d + t13 * za3d, ycom + t21 * xa3d + t22 * ya3d + t23 * za3d,
+                      zcom + t31 * xa3d + t32 * ya3d + t33 * za3d);
+  dp[1] = make_float3(xcom + t11 * xb3d + t12 * yb3d + t13 * zb3d - xb0, ycom + t21 * xb3d + t22 * yb3d + t23 * zb3d - yb0,
+                      zcom + t31 * xb3d + t32 * yb3d + t33 * zb3d - zb0);
+  dp[2] = make_float3(xcom + t11 * xc3d + t12 * yc3d + t13 * zc3d - xc0, ycom + t21 * xc3d + t22 * yc3d + t23 * zc3d - yc0,
+                      zcom + t31 * xc3d + t32 * yc3d + t33 * zc3d - zc0);
+}
+
+// src/reference/constraints.ts:195 -- RATTLE, Jacobi, over one cluster.
+__device__ bool rattle(Atom* at, const UnitDev& u, float tol) {
+  float3 rv[kMaxClusterConstraints];
+  float rl[kMaxClusterConstraints], rm[kMaxClusterConstraints], delta[kMaxClusterConstraints];
+  for (int c = 0; c < u.nc; ++c) {
+    rv[c] = rel(at[u.ci[c]], at[u.cj[c]]);
+    rl[c] = rv[c].x * rv[c].x + rv[c].y * rv[c].y + rv[c].z * rv[c].z;
+    const float sum = at[u.ci[c]].im + at[u.cj[c]].im;
+    rm[c] = sum == 0.f ? 0.f : 0.5f / sum;
+  }
+  for (int it = 0; it < kMaxShakeIterations; ++it) {
+    int conv = 0;
+    for (int c = 0; c < u.nc; ++c) {
+      const Atom &i = at[u.ci[c]], &j = at[u.cj[c]];
+      const float proj = (i.vx - j.vx) * rv[c].x + (i.vy - j.vy) * rv[c].y + (i.vz - j.vz) * rv[c].z;
+      delta[c] = rl[c] == 0.f ? 0.f : (-2.f * rm[c] * proj) / rl[c];
+      conv += fabsf(delta[c]) <= tol;
+    }
+    if (conv == u.nc) return true;
+    for (int c = 0; c < u.nc; ++c) {
+      Atom &i = at[u.ci[c]], &j = at[u.cj[c]];
+      const float dx = rv[c].x * delta[c], dy = rv[c].y * delta[c], dz = rv[c].z * delta[c];
+      i.vx += dx * i.im; i.vy += dy * i.im; i.vz += dz * i.im;
+      j.vx -= dx * j.im; j.vy -= dy * j.im; j.vz -= dz * j.im;
+    }
+  }
+  return false;
+}
+
+// src/reference/constraints.ts:130 -- SHAKE, Jacobi along the reference bond
+// vectors, over one cluster.  The trial bond vector is the exact reference
+// vector plus the difference of the two displacements, and the convergence
+// window is tested in FP64.
+__device__ bool shake(const Atom* at, float3* dp, const UnitDev& u, float tol) {
+  float3 rv[kMaxClusterConstraints];
+  float rm[kMaxClusterConstraints], delta[kMaxClusterConstraints];
+  for (int c = 0; c < u.nc; ++c) {
+    rv[c] = rel(at[u.ci[c]], at[u.cj[c]]);
+    const float sum = at[u.ci[c]].im + at[u.cj[c]].im;
+    rm[c] = sum == 0.f ? 0.f : 0.5f / sum;
+  }
+  const double lo = 1.0 - 2.0 * tol + double(tol) * tol, hi = 1.0 + 2.0 * tol + double(tol) * tol;
+  for (int it = 0; it < kMaxShakeIterations; ++it) {
+    int conv = 0;
+    for (int c = 0; c < u.nc; ++c) {
+      const int i = u.ci[c], j = u.cj[c];
+      const float x = rv[c].x + dp[i].x - dp[j].x, y = rv[c].y + dp[i].y - dp[j].y, z = rv[c].z + dp[i].z - dp[j].z;
+      const double l2 = double(x) * x + double(y) * y + double(z) * z;
+      const double d2 = double(u.dist[c]) * u.dist[c];
+      const float proj = x * rv[c].x + y * rv[c].y + z * rv[c].z;
+      delta[c] = proj == 0.f ? 0.f : rm[c] * float(d2 - l2) / proj;
+      conv += (l2 >= lo * d2 && l2 <= hi * d2);
+    }
+    if (conv == u.nc) return true;
+    for (int c = 0; c < u.nc; ++c) {
+      const int i = u.ci[c], j = u.cj[c];
+      const float dx = rv[c].x * delta[c], dy = rv[c].y * delta[c], dz = rv[c].z * delta[c];
+      dp[i].x += dx * at[i].im; dp[i].y += dy * at[i].im; dp[i].z += dz * at[i].im;
+      dp[j].x -= dx * at[j].im; dp[j].y -= dy * at[j].im; dp[j].z -= dz * at[j].im;
+    }
+  }
+  return false;
+}
+
+__device__ __forceinline__ long long displace(float wanted, float& left_over) {
+  const long long taken = to_fixed(wanted);
+  left_over = wanted - from_fixed(taken);
+  return taken;
+}
+
+__device__ void block_sum3(double* v, double (*red)[kThreads / 32]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; ++k) red[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) {
+      double t = 0;
+      for (int w = 0; w < kThreads / 32; ++w) t += red[k][w];
+      v[k] = t;
+    }
+}
+
+// The last block of a system turns the block momenta into the next step's
+// COM velocity and advances the step; the last block of the launch snapshots
+// the rebuild requests for the next step's list kernels.
+__device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance) {
+  __shared__ int last_of_system, last_of_launch;
+  __threadfence();
+  if (threadIdx.x == 0) last_of_system = atomicAdd(&d.done_count[s], 1) == S.n_iblk - 1;
+  __syncthreads();
+  if (last_of_system && threadIdx.x == 0) {
+    __threadfence();
+    double p[3] = {0, 0, 0};
+    for (int b = S.iblk_off; b < S.iblk_off + S.n_iblk; ++b)
+      for (int k = 0; k < 3; ++k) p[k] += d.mom_partial[b * 3 + k];
+    const double m = S.total_mass > 0 ? S.total_mass : 1.0;
+    d.vcom[s] = make_float4(float(p[0] / m), float(p[1] / m), float(p[2] / m), 0.f);
+    if (advance) d.step[s] += 1;
+    d.done_count[s] = 0;
+  }
+  if (!advance) return;
+  __threadfence();
+  if (threadIdx.x == 0) last_of_launch = atomicAdd(d.global_ticket, 1) == int(gridDim.x) - 1;
+  __syncthreads();
+  if (last_of_launch && threadIdx.x == 0) {
+    __threadfence();
+    int any = 0;
+    for (int k = 0; k < d.S; ++k) {
+      const int f = d.rebuild_flag[k] | d.run.always_rebuild;
+      d.rebuild_now[k] = f;
+      d.rebuild_flag[k] = 0;
+      any |= f;
+    }
+    *d.any_rebuild = any;
+    *d.global_ticket = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
+  __shared__ double red[3][kThreads / 32];
+  const int b = blockIdx.x;
+  const int s = d.iblk_sys[b];
+  const SysDev& S = d.sys[s];
+  const RunDev& R = d.run;
+  const long long step = d.step[s];
+  const bool com = S.com_freq > 0 && (step % S.com_freq) == 0;
+  const float4 vc = com ? d.vcom[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double mom[3] = {0, 0, 0};
+  bool moved = false, bad = false;
+
+  if (threadIdx.x < d.iblk_nunit[b]) {
+    const UnitDev u = d.units[d.iblk_unit0[b] + threadIdx.x];
+    Atom at[kMaxClusterAtoms];
+    for (int k = 0; k < u.na; ++k) {
+      const int a = u.atom[k];
+      Atom& A = at[k];
+      A.x = d.px[a]; A.y = d.py[a]; A.z = d.pz[a];
+      A.vx = d.vx[a]; A.vy = d.vy[a]; A.vz = d.vz[a];
+      A.rx = d.rx[a]; A.ry = d.ry[a]; A.rz = d.rz[a];
+      A.im = d.invm[a];
+      const int gs = S.slot_off + d.rank[a];
+      A.fx = from_fixed(static_cast<long long>(d.fx[gs]));
+      A.fy = from_fixed(static_cast<long long>(d.fy[gs]));
+      A.fz = from_fixed(static_cast<long long>(d.fz[gs]));
+      d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;  // consumer clears
+      if (com && A.im > 0.f) { A.vx -= vc.x; A.vy -= vc.y; A.vz -= vc.z; }
+    }
+    const float dt = R.dt;
+    long long tx[kMaxClusterAtoms], ty[kMaxClusterAtoms], tz[kMaxClusterAtoms];  // drift, fixed
+    float3 dp[kMaxClusterAtoms];
+    if (R.integrator == 0) {
+      // ---- LFMiddle ----
+      for (int k = 0; k < u.na; ++k) {
+        Atom& A = at[k];
+        if (A.im == 0.f) continue;
+        A.vx += dt * A.im * A.fx; A.vy += dt * A.im * A.fy; A.vz += dt * A.im * A.fz;
+      }
+      if (u.kind == kUnitSettle) settle_velocities(at);
+      else if (u.kind == kUnitShake) bad |= !rattle(at, u, R.tolerance);
+      const float half = 0.5f * dt;
+      for (int k = 0; k < u.na; ++k) {
+        Atom& A = at[k];
+        tx[k] = ty[k] = tz[k] = 0;
+        if (A.im == 0.f) continue;
+        float n0 = 0.f, n1 = 0.f, n2 = 0.f;
+        if (R.draw_noise) {
+          const unsigned p = static_cast<unsigned>(u.atom[k] - S.atom_off);
+          const uint2 key = make_uint2(R.seed, kThermostatDomain);
+          const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
+          const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
+          n0 = g0.x; n1 = g0.y; n2 = g1.x;
+        }
+        const float noise = R.noise_scale * sqrtf(R.kt * A.im);
+        float lo;
+        tx[k] = displace(A.vx * half + A.rx, lo);
+        A.vx = R.velocity_scale * A.vx + noise * n0;
+        tx[k] += displace(A.vx * half + lo, A.rx);
+        ty[k] = displace(A.vy * half + A.ry, lo);
+        A.vy = R.velocity_scale * A.vy + noise * n1;
+        ty[k] += displace(A.vy * half + lo, A.ry);
+        tz[k] = displace(A.vz * half + A.rz, lo);
+        A.vz = R.velocity_scale * A.vz + noise * n2;
+        tz[k] += displace(A.vz * half + lo, A.rz);
+      }
+    } else {
+      // ---- velocity Verlet (integrate.wgsl:91-132) ----
+      for (int k = 0; k < u.na; ++k) {
+        Atom& A = at[k];
+        tx[k] = ty[k] = tz[k] = 0;
+        if (A.im == 0.f) continue;
+        A.vx += A.im * A.fx * dt; A.vy += A.im * A.fy * dt; A.vz += A.im * A.fz * dt;
+        tx[k] = displace(A.vx * dt + A.rx, A.rx);
+        ty[k] = displace(A.vy * dt + A.ry, A.ry);
+        tz[k] = displace(A.vz * dt + A.rz, A.rz);
+      }
+    }
+    // position constraints, relative to the start-of-step positions
+    for (int k = 0; k < u.na; ++k) dp[k] = make_float3(from_fixed(tx[k]), from_fixed(ty[k]), from_fixed(tz[k]));
+    long long cx[kMaxClusterAtoms], cy[kMaxClusterAtoms], cz[kMaxClusterAtoms];
+    if (u.kind == kUnitFree) {
+      cx[0] = tx[0]; cy[0] = ty[0]; cz[0] = tz[0];
+    } else {
+      if (u.kind == kUnitSettle) settle_positions(at, dp, u.dist[0], u.dist[1]);
+      else bad |= !shake(at, dp, u, R.tolerance);
+      for (int k = 0; k < u.na; ++k) {
+        if (at[k].im == 0.f) { cx[k] = tx[k]; cy[k] = ty[k]; cz[k] = tz[k]; continue; }
+        cx[k] = to_fixed(dp[k].x); cy[k] = to_fixed(dp[k].y); cz[k] = to_fixed(dp[k].z);
+      }
+    }
+    const float idt = 1.f / dt;
+    for (int k = 0; k < u.na; ++k) {
+      Atom& A = at[k];
+      const int a = u.atom[k];
+      if (A.im != 0.f) {
+        if (R.integrator == 0) {
+          A.vx += idt * from_fixed(cx[k] - tx[k]);
+          A.vy += idt * from_fixed(cy[k] - ty[k]);
+          A.vz += idt * from_fixed(cz[k] - tz[k]);
+        } else {
+          A.vx = idt * from_fixed(cx[k]);
+          A.vy = idt * from_fixed(cy[k]);
+          A.vz = idt * from_fixed(cz[k]);
+        }
+        A.x += cx[k]; A.y += cy[k]; A.z += cz[k];
+        d.px[a] = A.x; d.py[a] = A.y; d.pz[a] = A.z;
+        d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
+        d.rx[a] = A.rx; d.ry[a] = A.ry; d.rz[a] = A.rz;
+        const double m = 1.0 / A.im;
+        mom[0] += m * A.vx; mom[1] += m * A.vy; mom[2] += m * A.vz;
+        bad |= !isfinite(A.vx + A.vy + A.vz);
+      } else if (com) {
+        d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
+      }
+      const float ex = from_fixed(A.x - d.refx[a]), ey = from_fixed(A.y - d.refy[a]), ez = from_fixed(A.z - d.refz[a]);
+      moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
+    }
+  }
+  if (moved) atomicOr(&d.rebuild_flag[s], 1);
+  if (bad) atomicAdd(&d.shake_failures[s], 1);
+  block_sum3(mom, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) d.mom_partial[b * 3 + k] = mom[k];
+  finish_block(d, s, S, true);
+}
+
+// The momentum of the current velocities, for the first COM removal after the
+// host set them.
+__global__ void __launch_bounds__(kThreads) k_momentum(Dev d) {
+  __shared__ double red[3][kThreads / 32];
+  const int b = blockIdx.x;
+  const int s = d.iblk_sys[b];
+  const SysDev& S = d.sys[s];
+  double mom[3] = {0, 0, 0};
+  if (threadIdx.x < d.iblk_nunit[b]) {
+    const UnitDev u = d.units[d.iblk_unit0[b] + threadIdx.x];
+    for (int k = 0; k < u.na; ++k) {
+      const int a = u.atom[k];
+      const float im = d.invm[a];
+      if (im == 0.f) continue;
+      const double m = 1.0 / im;
+      mom[0] += m * d.vx[a]; mom[1] += m * d.vy[a]; mom[2] += m * d.vz[a];
+    }
+  }
+  block_sum3(mom, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) d.mom_partial[b * 3 + k] = mom[k];
+  finish_block(d, s, S, false);
+}
+
+}  // namespace
+
+void launch_integrate(const Dev& d, cudaStream_t st) {
+  k_integrate<<<d.n_iblk, kThreads, 0, st>>>(d);
+}
+
+void launch_momentum(const Dev& d, cudaStream_t st) {
+  k_momentum<<<d.n_iblk, kThreads, 0, st>>>(d);
+}
+
+}  // namespace mdb

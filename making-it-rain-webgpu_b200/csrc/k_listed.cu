@@ -1,0 +1,188 @@
+// k_listed.cu -- every listed interaction in one launch: harmonic bonds,
+// harmonic angles, periodic torsions (src/gpu/kernels/bonded.wgsl:31/51/86;
+// oracle src/reference/forces/bonded.ts:39/71/133), the nonbonded exceptions
+// (nonbonded-exceptions.wgsl:74; oracle nonbonded.ts:330) and position
+// restraints (restraint.wgsl:81; oracle forces/restraint.ts:38).
+//
+// One thread per term over the concatenation [bonds | angles | torsions |
+// exceptions | restraints] of all systems.  Vectors are differenced exactly in
+// 64-bit fixed point and only then converted, so nothing is rounded while it
+// is still box-sized (fixed64.wgsl:166-233).  Bonded terms take no minimum
+// image, as in OpenMM; exceptions and restraints do.  Forces are scattered as
+// int64 fixed-point atomics into the slot-ordered force arrays.
+#include "device_state.h"
+
+namespace mdb {
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Ctx {
+  const Dev& d;
+};
+
+__device__ __forceinline__ float3 diff(const Dev& d, int a, int b) {
+  return make_float3(from_fixed(d.px[b] - d.px[a]), from_fixed(d.py[b] - d.py[a]),
+                     from_fixed(d.pz[b] - d.pz[a]));
+}
+
+// Minimum image of an exact fixed-point difference: the box count is estimated
+// in f32 and removed in integers, c then b then a (nonbonded.ts:241).
+__device__ __forceinline__ float3 min_image_fixed(const SysDev& S, long long dx, long long dy, long long dz) {
+  const long long kc = __float2ll_rn(from_fixed(dz) * S.inv_f[8]);
+  dz -= kc * S.box_fx[8];
+  dy -= kc * S.box_fx[7];
+  dx -= kc * S.box_fx[6];
+  const long long kb = __float2ll_rn(from_fixed(dy) * S.inv_f[4]);
+  dy -= kb * S.box_fx[4];
+  dx -= kb * S.box_fx[3];
+  const long long ka = __float2ll_rn(from_fixed(dx) * S.inv_f[0]);
+  dx -= ka * S.box_fx[0];
+  return make_float3(from_fixed(dx), from_fixed(dy), from_fixed(dz));
+}
+
+__device__ __forceinline__ void add_force(const Dev& d, const SysDev& S, int atom, float x, float y, float z) {
+  const int gs = S.slot_off + d.rank[atom];
+  add_fixed(&d.fx[gs], x);
+  add_fixed(&d.fy[gs], y);
+  add_fixed(&d.fz[gs], z);
+}
+
+template <bool ENERGY>
+__device__ __forceinline__ void add_energy(const Dev& d, const SysDev& S, int slot, float e) {
+  if (ENERGY) add_fixed(&d.energy[S.energy_base + slot], e);
+}
+
+template <bool ENERGY>
+__device__ void bond(const Dev& d, const BondDev& t) {
+  const SysDev& S = d.sys[t.sys];
+  const float3 v = diff(d, t.a, t.b);
+  const float r = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+  const float dr = r - t.r0;
+  add_energy<ENERGY>(d, S, kEBond, 0.5f * t.k * dr * dr);
+  const float sc = t.k * dr / r;
+  add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);
+  add_force(d, S, t.b, -sc * v.x, -sc * v.y, -sc * v.z);
+}
+
+template <bool ENERGY>
+__device__ void angle(const Dev& d, const AngleDev& t) {
+  const SysDev& S = d.sys[t.sys];
+  const float3 v1 = diff(d, t.b, t.a), v2 = diff(d, t.b, t.c);
+  const float r1 = v1.x * v1.x + v1.y * v1.y + v1.z * v1.z;
+  const float r2 = v2.x * v2.x + v2.y * v2.y + v2.z * v2.z;
+  const float dot = v1.x * v2.x + v1.y * v2.y + v1.z * v2.z;
+  const float cs = fminf(1.f, fmaxf(-1.f, dot * rsqrtf(r1 * r2)));
+  const float nx = v1.y * v2.z - v1.z * v2.y, ny = v1.z * v2.x - v1.x * v2.z, nz = v1.x * v2.y - v1.y * v2.x;
+  const float nn = fmaxf(sqrtf(nx * nx + ny * ny + nz * nz), 1e-6f);
+  // theta from atan2(|n|, dot) keeps its precision near 0 and pi, where acos does not.
+  const float theta = atan2f(sqrtf(nx * nx + ny * ny + nz * nz), dot);
+  (void)cs;
+  const float dth = theta - t.theta0;
+  add_energy<ENERGY>(d, S, kEAngle, 0.5f * t.k * dth * dth);
+  const float dE = t.k * dth;
+  const float tA = dE / (r1 * nn), tC = -dE / (r2 * nn);
+  const float f1x = -tA * (v1.y * nz - v1.z * ny), f1y = -tA * (v1.z * nx - v1.x * nz),
+              f1z = -tA * (v1.x * ny - v1.y * nx);
+  const float f3x = -tC * (v2.y * nz - v2.z * ny), f3y = -tC * (v2.z * nx - v2.x * nz),
+              f3z = -tC * (v2.x * ny - v2.y * nx);
+  add_force(d, S, t.a, f1x, f1y, f1z);
+  add_force(d, S, t.c, f3x, f3y, f3z);
+  add_force(d, S, t.b, -f1x - f3x, -f1y - f3y, -f1z - f3z);
+}
+
+template <bool ENERGY>
+__device__ void torsion(const Dev& d, const TorsionDev& t) {
+  const SysDev& S = d.sys[t.sys];
+  const float3 b1 = diff(d, t.a, t.b), b2 = diff(d, t.b, t.c), b3 = diff(d, t.c, t.d);
+  const float n1x = b1.y * b2.z - b1.z * b2.y, n1y = b1.z * b2.x - b1.x * b2.z, n1z = b1.x * b2.y - b1.y * b2.x;
+  const float n2x = b2.y * b3.z - b2.z * b3.y, n2y = b2.z * b3.x - b2.x * b3.z, n2z = b2.x * b3.y - b2.y * b3.x;
+  const float n1 = n1x * n1x + n1y * n1y + n1z * n1z, n2 = n2x * n2x + n2y * n2y + n2z * n2z;
+  const float b2n = sqrtf(b2.x * b2.x + b2.y * b2.y + b2.z * b2.z);
+  const float X = n1x * n2x + n1y * n2y + n1z * n2z;
+  const float Y = b2n * (b1.x * n2x + b1.y * n2y + b1.z * n2z);
+  const float phi = atan2f(Y, X);
+  const float arg = t.periodicity * phi - t.phase;
+  float sn, cn;
+  sincosf(arg, &sn, &cn);
+  add_energy<ENERGY>(d, S, kETorsion, t.k * (1.f + cn));
+  if (n1 == 0.f || n2 == 0.f) return;
+  const float dEdPhi = -t.k * t.periodicity * sn;
+  const float s1 = dEdPhi * b2n / n1, s4 = -dEdPhi * b2n / n2;
+  const float f1x = s1 * n1x, f1y = s1 * n1y, f1z = s1 * n1z;
+  const float f4x = s4 * n2x, f4y = s4 * n2y, f4z = s4 * n2z;
+  const float b2sq = b2n * b2n;
+  const float ss = (b1.x * b2.x + b1.y * b2.y + b1.z * b2.z) / b2sq;
+  const float tt = (b3.x * b2.x + b3.y * b2.y + b3.z * b2.z) / b2sq;
+  add_force(d, S, t.a, f1x, f1y, f1z);
+  add_force(d, S, t.b, -(1.f + ss) * f1x + tt * f4x, -(1.f + ss) * f1y + tt * f4y, -(1.f + ss) * f1z + tt * f4z);
+  add_force(d, S, t.c, ss * f1x - (1.f + tt) * f4x, ss * f1y - (1.f + tt) * f4y, ss * f1z - (1.f + tt) * f4z);
+  add_force(d, S, t.d, f4x, f4y, f4z);
+}
+
+template <bool ENERGY>
+__device__ void exception(const Dev& d, const ExceptionDev& t) {
+  const SysDev& S = d.sys[t.sys];
+  const float3 v = min_image_fixed(S, d.px[t.b] - d.px[t.a], d.py[t.b] - d.py[t.a], d.pz[t.b] - d.pz[t.a]);
+  const float r2 = v.x * v.x + v.y * v.y + v.z * v.z;
+  const float rinv = rsqrtf(r2);
+  const float r = r2 * rinv;
+  float dEdR = 0.f, correction = 0.f, own = 0.f;
+  if (t.qq_particles != 0.f) {
+    const float x = S.alpha * r;
+    const float ef = erff(x);
+    correction = -t.qq_particles * ef * rinv;
+    dEdR += t.qq_particles * (ef * rinv * rinv - S.alpha_2_sqrtpi * __expf(-x * x) * rinv);
+  }
+  if (t.qq_own != 0.f) {
+    own += t.qq_own * rinv;
+    dEdR -= t.qq_own * rinv * rinv;
+  }
+  if (t.eps4 != 0.f) {
+    const float s2 = t.sigma * t.sigma * rinv * rinv;
+    const float s6 = s2 * s2 * s2, s12 = s6 * s6;
+    own += t.eps4 * (s12 - s6);
+    dEdR += t.eps4 * rinv * (6.f * s6 - 12.f * s12);
+  }
+  add_energy<ENERGY>(d, S, kEExclusion, correction);
+  add_energy<ENERGY>(d, S, kEException, own);
+  if (dEdR != 0.f) {
+    const float sc = dEdR * rinv;
+    add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);
+    add_force(d, S, t.b, -sc * v.x, -sc * v.y, -sc * v.z);
+  }
+}
+
+template <bool ENERGY>
+__device__ void restraint(const Dev& d, const RestraintDev& t) {
+  const SysDev& S = d.sys[t.sys];
+  const float3 v = min_image_fixed(S, d.px[t.p] - t.x0, d.py[t.p] - t.y0, d.pz[t.p] - t.z0);
+  add_energy<ENERGY>(d, S, kERestraint, t.k * (v.x * v.x + v.y * v.y + v.z * v.z));
+  add_force(d, S, t.p, -2.f * t.k * v.x, -2.f * t.k * v.y, -2.f * t.k * v.z);
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(kThreads) k_listed(Dev d) {
+  const int n0 = d.n_bonds, n1 = n0 + d.n_angles, n2 = n1 + d.n_torsions, n3 = n2 + d.n_exceptions,
+            n4 = n3 + d.n_restraints;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
+    if (i < n0) bond<ENERGY>(d, d.bonds[i]);
+    else if (i < n1) angle<ENERGY>(d, d.angles[i - n0]);
+    else if (i < n2) torsion<ENERGY>(d, d.torsions[i - n1]);
+    else if (i < n3) exception<ENERGY>(d, d.exceptions[i - n2]);
+    else restraint<ENERGY>(d, d.restraints[i - n3]);
+  }
+}
+
+}  // namespace
+
+void launch_listed(const Dev& d, bool energy, cudaStream_t st) {
+  const int n = d.n_bonds + d.n_angles + d.n_torsions + d.n_exceptions + d.n_restraints;
+  if (n == 0) return;
+  int blocks = (n + kThreads - 1) / kThreads;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (energy) k_listed<true><<<blocks, kThreads, 0, st>>>(d);
+  else k_listed<false><<<blocks, kThreads, 0, st>>>(d);
+}
+
+}  // namespace mdb

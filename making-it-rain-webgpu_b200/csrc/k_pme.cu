@@ -1,0 +1,450 @@
+// k_pme.cu -- reciprocal-space PME: B-spline spread, 3D real-to-complex FFT
+// with the Ewald convolution fused into the x pass, complex-to-real FFT, and
+// the force gather.
+//
+// Physics follows src/gpu/kernels/pme.wgsl:124 (spread), fft.wgsl:60,
+// pme-convolve.wgsl:34, pme-interpolate.wgsl:105 and the f64 oracle
+// src/reference/forces/pme.ts:93-263: order-5 cardinal B-splines on a mesh
+// laid out in fractional coordinates, E = sum_k f(k) |Q(k)|^2 with
+// f = (2 pi / V) ONE_4PI_EPS0 exp(-k^2/4a^2) / (k^2 |b(m)|^2), and the grid
+// multiplied by 2 f before the inverse transform.
+//
+// B200 shape:
+//   * the spline argument u = r . (K o B^-1) is formed exactly in 2^32 fixed
+//     point from the int64 positions (a 64x64->128-bit product), so the grid
+//     index and the weight fraction carry no f32 coordinate rounding;
+//   * the charge grid is int64 fixed point filled with atomics, so the spread
+//     is order independent and runs are bit-identical;
+//   * the transform is five passes, each a CTA loading whole lines into shared
+//     memory and running a Stockham mixed-radix (2, 3, 4, 5, 7) FFT there: z
+//     (int64 -> complex, real-to-complex, clearing the grid it read), y, then
+//     x forward + convolution + x inverse in one pass, y inverse, z
+//     complex-to-real.  The reference's 7-13 global passes per direction and
+//     its separate load/convolve passes disappear.
+#include "device_state.h"
+
+namespace mdb {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// exp(-2 pi i t / R) for the small DFTs.
+__constant__ float2 kRoot3[3] = {{1.f, 0.f}, {-0.500000000f, -0.866025404f}, {-0.500000000f, 0.866025404f}};
+__constant__ float2 kRoot5[5] = {{1.f, 0.f},
+                                 {0.309016994f, -0.951056516f},
+                                 {-0.809016994f, -0.587785252f},
+                                 {-0.809016994f, 0.587785252f},
+                                 {0.309016994f, 0.951056516f}};
+__constant__ float2 kRoot7[7] = {{1.f, 0.f},
+                                 {0.623489802f, -0.781831482f},
+                                 {-0.222520934f, -0.974927912f},
+                                 {-0.900968868f, -0.433883739f},
+                                 {-0.900968868f, 0.433883739f},
+                                 {-0.222520934f, 0.974927912f},
+                                 {0.623489802f, 0.781831482f}};
+
+template <int R>
+__device__ __forceinline__ float2 root(int t, int sign) {
+  float2 w;
+  if (R == 3) w = kRoot3[t];
+  else if (R == 5) w = kRoot5[t];
+  else w = kRoot7[t];
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+template <int R>
+__device__ __forceinline__ void small_dft(float2* v, int sign) {
+  if (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = make_float2(a.x + b.x, a.y + b.y);
+    v[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else if (R == 4) {
+    const float2 a0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+    const float2 a1 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const float2 b0 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+    float2 b1 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+    // multiply by -i (forward) or +i (inverse)
+    b1 = sign < 0 ? make_float2(b1.y, -b1.x) : make_float2(-b1.y, b1.x);
+    v[0] = make_float2(a0.x + b0.x, a0.y + b0.y);
+    v[2] = make_float2(a0.x - b0.x, a0.y - b0.y);
+    v[1] = make_float2(a1.x + b1.x, a1.y + b1.y);
+    v[3] = make_float2(a1.x - b1.x, a1.y - b1.y);
+  } else {
+    float2 out[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      float2 s = v[0];
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        const float2 w = root<R>((m * q) % R, sign);
+        s.x += v[q].x * w.x - v[q].y * w.y;
+        s.y += v[q].x * w.y + v[q].y * w.x;
+      }
+      out[m] = s;
+    }
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[m] = out[m];
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void stage_butterfly(const float2* src, float2* dst, int n, int j, int ns,
+                                                const float2* tw, int sign) {
+  const int bf = n / R;
+  const int k = j % ns;
+  const int step = n / (ns * R);
+  float2 v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    float2 x = src[j + q * bf];
+    if (q > 0 && k > 0) {
+      float2 w = tw[(k * q * step) % n];
+      if (sign > 0) w.y = -w.y;
+      x = cmul(x, w);
+    }
+    v[q] = x;
+  }
+  small_dft<R>(v, sign);
+  const int dest = (j / ns) * ns * R + k;
+#pragma unroll
+  for (int q = 0; q < R; ++q) dst[dest + q * ns] = v[q];
+}
+
+// Stockham autosort over `nl` lines of length n in shared memory
+// (src/reference/fft.ts:128 is the f64 restatement of the same recursion).
+// Returns the buffer holding the result.
+__device__ float2* fft_lines(float2* a, float2* b, int n, int nl, const int* radices, int nrad,
+                             const float2* tw, int sign) {
+  int ns = 1;
+  for (int st = 0; st < nrad; ++st) {
+    const int r = radices[st];
+    const int bf = n / r;
+    for (int idx = threadIdx.x; idx < nl * bf; idx += blockDim.x) {
+      const int line = idx / bf, j = idx - line * bf;
+      const float2* src = a + line * n;
+      float2* dst = b + line * n;
+      switch (r) {
+        case 2: stage_butterfly<2>(src, dst, n, j, ns, tw, sign); break;
+        case 3: stage_butterfly<3>(src, dst, n, j, ns, tw, sign); break;
+        case 4: stage_butterfly<4>(src, dst, n, j, ns, tw, sign); break;
+        case 5: stage_butterfly<5>(src, dst, n, j, ns, tw, sign); break;
+        default: stage_butterfly<7>(src, dst, n, j, ns, tw, sign); break;
+      }
+    }
+    __syncthreads();
+    float2* t = a;
+    a = b;
+    b = t;
+    ns *= r;
+  }
+  return a;
+}
+
+// ------------------------------------------------------------- splines ----
+// Order-5 cardinal B-spline weights and derivatives at fraction w
+// (src/reference/forces/bspline.ts:55, the same recursion in f32).
+__device__ __forceinline__ void bspline5(float w, float* th, float* dth) {
+  float lo[5];
+  lo[0] = 1.f - w;
+  lo[1] = w;
+  lo[2] = 0.f;
+  lo[3] = 0.f;
+  lo[4] = 0.f;
+#pragma unroll
+  for (int k = 3; k <= 4; ++k) {
+    const float dv = 1.f / (k - 1);
+    lo[k - 1] = dv * w * lo[k - 2];
+#pragma unroll
+    for (int j = 1; j < k - 1; ++j) lo[k - j - 1] = dv * ((w + j) * lo[k - j - 2] + (k - j - w) * lo[k - j - 1]);
+    lo[0] = dv * (1.f - w) * lo[0];
+  }
+  if (dth) {
+    dth[0] = -lo[0];
+#pragma unroll
+    for (int j = 1; j < 5; ++j) dth[j] = lo[j - 1] - lo[j];
+  }
+#pragma unroll
+  for (int j = 0; j < 5; ++j) th[j] = lo[j];
+  const float dv = 0.25f;
+  th[4] = dv * w * th[3];
+#pragma unroll
+  for (int j = 1; j < 4; ++j) th[4 - j] = dv * ((w + j) * th[3 - j] + (5 - j - w) * th[4 - j]);
+  th[0] = dv * (1.f - w) * th[0];
+}
+
+struct Spline {
+  int base[3];
+  float th[3][5], dth[3][5];
+};
+
+__device__ __forceinline__ void spline_for(const SysDev& S, long long x, long long y, long long z,
+                                           Spline& sp, bool derivatives) {
+  const long long u[3] = {fixed_mul(x, S.umat[0]) + fixed_mul(y, S.umat[1]) + fixed_mul(z, S.umat[2]),
+                          fixed_mul(y, S.umat[3]) + fixed_mul(z, S.umat[4]), fixed_mul(z, S.umat[5])};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const long long cell = u[k] >> 32;
+    const float w = static_cast<float>(static_cast<unsigned int>(u[k] & 0xffffffffll)) * 2.3283064365386963e-10f;
+    long long b = (cell - (kPmeOrder - 1)) % S.grid[k];
+    if (b < 0) b += S.grid[k];
+    sp.base[k] = static_cast<int>(b);
+    bspline5(w, sp.th[k], derivatives ? sp.dth[k] : nullptr);
+  }
+}
+
+// ---------------------------------------------------------------- spread --
+__global__ void __launch_bounds__(kThreads) k_spread(Dev d) {
+  for (int gs = blockIdx.x * blockDim.x + threadIdx.x; gs < d.n_slots; gs += gridDim.x * blockDim.x) {
+    const int a = d.order[gs];
+    if (a < 0) continue;
+    const float q = d.prm[gs].w;
+    if (q == 0.f) continue;
+    const SysDev& S = d.sys[d.slot_sys[gs]];
+    Spline sp;
+    spline_for(S, d.px[a], d.py[a], d.pz[a], sp, false);
+    const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
+    unsigned long long* grid = d.qgrid + S.grid_off;
+    for (int ix = 0; ix < kPmeOrder; ++ix) {
+      int gx = sp.base[0] + ix;
+      if (gx >= Kx) gx -= Kx;
+      const float wx = q * sp.th[0][ix];
+      for (int iy = 0; iy < kPmeOrder; ++iy) {
+        int gy = sp.base[1] + iy;
+        if (gy >= Ky) gy -= Ky;
+        const float wxy = wx * sp.th[1][iy];
+        unsigned long long* row = grid + (static_cast<long long>(gx) * Ky + gy) * Kz;
+#pragma unroll
+        for (int iz = 0; iz < kPmeOrder; ++iz) {
+          int gz = sp.base[2] + iz;
+          if (gz >= Kz) gz -= Kz;
+          add_fixed(&row[gz], wxy * sp.th[2][iz]);
+        }
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- z pass ---
+// int64 charge grid -> complex half spectrum along z, clearing the grid.
+__global__ void __launch_bounds__(kThreads) k_fft_z_forward(Dev d) {
+  extern __shared__ float2 smem[];
+  const FftWork w = d.fft_z[blockIdx.x];
+  const SysDev& S = d.sys[w.sys];
+  const int Kz = S.grid[2], kzh = S.kzh;
+  float2* A = smem;
+  float2* B = smem + w.n * Kz;
+  unsigned long long* grid = d.qgrid + S.grid_off + static_cast<long long>(w.a) * Kz;
+  for (int i = threadIdx.x; i < w.n * Kz; i += blockDim.x) {
+    const long long v = static_cast<long long>(grid[i]);
+    A[i] = make_float2(from_fixed(v), 0.f);
+    grid[i] = 0ull;
+  }
+  __syncthreads();
+  const float2* R = fft_lines(A, B, Kz, w.n, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], -1);
+  float2* out = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * kzh;
+  for (int i = threadIdx.x; i < w.n * kzh; i += blockDim.x) {
+    const int line = i / kzh, k = i - line * kzh;
+    out[i] = R[line * Kz + k];
+  }
+}
+
+// --------------------------------------------------------------- y pass ---
+__global__ void __launch_bounds__(kThreads) k_fft_y(Dev d, int sign) {
+  extern __shared__ float2 smem[];
+  const FftWork w = d.fft_y[blockIdx.x];
+  const SysDev& S = d.sys[w.sys];
+  const int Ky = S.grid[1], kzh = S.kzh;
+  float2* A = smem;
+  float2* B = smem + w.n * Ky;
+  float2* base = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh + w.b;
+  for (int i = threadIdx.x; i < w.n * Ky; i += blockDim.x) {
+    const int y = i / w.n, l = i - y * w.n;
+    A[l * Ky + y] = base[static_cast<long long>(y) * kzh + l];
+  }
+  __syncthreads();
+  const float2* R = fft_lines(A, B, Ky, w.n, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], sign);
+  for (int i = threadIdx.x; i < w.n * Ky; i += blockDim.x) {
+    const int y = i / w.n, l = i - y * w.n;
+    base[static_cast<long long>(y) * kzh + l] = R[l * Ky + y];
+  }
+}
+
+// ------------------------------------------- x pass with the convolution ---
+template <bool ENERGY>
+__global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
+  extern __shared__ float2 smem[];
+  __shared__ double partial[kThreads / 32];
+  const FftWork w = d.fft_x[blockIdx.x];
+  const SysDev& S = d.sys[w.sys];
+  const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  float2* A = smem;
+  float2* B = smem + w.n * Kx;
+  const long long stride = static_cast<long long>(Ky) * kzh;
+  float2* base = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * kzh + w.b;
+  for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
+    const int x = i / w.n, l = i - x * w.n;
+    A[l * Kx + x] = base[x * stride + l];
+  }
+  __syncthreads();
+  float2* R = fft_lines(A, B, Kx, w.n, S.radices[0], S.nradix[0], d.twiddles + S.tw_off[0], -1);
+  float2* other = R == A ? B : A;
+  // Convolution (pme-convolve.wgsl:34; pme.ts:160-209) on the half spectrum.
+  double energy = 0.0;
+  const int my = w.a;
+  const int mb = my <= Ky / 2 ? my : my - Ky;
+  const float* modx = d.moduli + S.mod_off;
+  const float* mody = modx + Kx;
+  const float* modz = mody + Ky;
+  const float two_pi = 6.283185307179586f;
+  for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
+    const int l = i / Kx, mx = i - l * Kx;
+    const int kz = w.b + l;
+    const int ma = mx <= Kx / 2 ? mx : mx - Kx;
+    const int mc = kz;  // kz <= Kz/2 on the half spectrum
+    float2 v = R[i];
+    float factor = 0.f;
+    if (mx != 0 || my != 0 || kz != 0) {
+      const float* M = S.inv_f;
+      const float kx = two_pi * ma * M[0];
+      const float ky = two_pi * (ma * M[3] + mb * M[4]);
+      const float kzv = two_pi * (ma * M[6] + mb * M[7] + mc * M[8]);
+      const float k2 = kx * kx + ky * ky + kzv * kzv;
+      factor = S.pme_pref * expf(k2 * S.exp_scale) / (k2 * modx[mx] * mody[my] * modz[kz]);
+    }
+    if (ENERGY) {
+      const double weight = (kz == 0 || (2 * kz == Kz)) ? 1.0 : 2.0;
+      energy += weight * static_cast<double>(factor) * (static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y);
+    }
+    v.x *= 2.f * factor;
+    v.y *= 2.f * factor;
+    R[i] = v;
+  }
+  __syncthreads();
+  const float2* Q = fft_lines(R, other, Kx, w.n, S.radices[0], S.nradix[0], d.twiddles + S.tw_off[0], +1);
+  for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
+    const int x = i / w.n, l = i - x * w.n;
+    base[x * stride + l] = Q[l * Kx + x];
+  }
+  if (ENERGY) {
+    // fixed-order block reduction in FP64: deterministic
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) energy += __shfl_xor_sync(0xffffffffu, energy, o);
+    if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = energy;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double total = 0.0;
+      for (int k = 0; k < (blockDim.x >> 5); ++k) total += partial[k];
+      d.mesh_partial[blockIdx.x] = total;
+    }
+  }
+}
+
+// ---------------------------------------------------------- z inverse ----
+// complex half spectrum -> real potential grid along z.
+__global__ void __launch_bounds__(kThreads) k_fft_z_inverse(Dev d) {
+  extern __shared__ float2 smem[];
+  const FftWork w = d.fft_z[blockIdx.x];
+  const SysDev& S = d.sys[w.sys];
+  const int Kz = S.grid[2], kzh = S.kzh;
+  float2* A = smem;
+  float2* B = smem + w.n * Kz;
+  const float2* in = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * kzh;
+  for (int i = threadIdx.x; i < w.n * kzh; i += blockDim.x) {
+    const int line = i / kzh, k = i - line * kzh;
+    A[line * Kz + k] = in[i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < w.n * (Kz - kzh); i += blockDim.x) {
+    const int line = i / (Kz - kzh), k = kzh + (i - line * (Kz - kzh));
+    const float2 c = A[line * Kz + (Kz - k)];
+    A[line * Kz + k] = make_float2(c.x, -c.y);
+  }
+  __syncthreads();
+  const float2* R = fft_lines(A, B, Kz, w.n, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], +1);
+  float* out = d.phi + S.grid_off + static_cast<long long>(w.a) * Kz;
+  for (int i = threadIdx.x; i < w.n * Kz; i += blockDim.x) out[i] = R[i].x;
+}
+
+// ---------------------------------------------------------------- gather --
+__global__ void __launch_bounds__(kThreads) k_gather(Dev d) {
+  for (int gs = blockIdx.x * blockDim.x + threadIdx.x; gs < d.n_slots; gs += gridDim.x * blockDim.x) {
+    const int a = d.order[gs];
+    if (a < 0) continue;
+    const float q = d.prm[gs].w;
+    if (q == 0.f) continue;
+    const SysDev& S = d.sys[d.slot_sys[gs]];
+    Spline sp;
+    spline_for(S, d.px[a], d.py[a], d.pz[a], sp, true);
+    const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
+    const float* grid = d.phi + S.grid_off;
+    float ga = 0.f, gb = 0.f, gc = 0.f;
+    for (int ix = 0; ix < kPmeOrder; ++ix) {
+      int gx = sp.base[0] + ix;
+      if (gx >= Kx) gx -= Kx;
+      for (int iy = 0; iy < kPmeOrder; ++iy) {
+        int gy = sp.base[1] + iy;
+        if (gy >= Ky) gy -= Ky;
+        const float* row = grid + (static_cast<long long>(gx) * Ky + gy) * Kz;
+        const float wxy = sp.th[0][ix] * sp.th[1][iy];
+        const float dxy = sp.dth[0][ix] * sp.th[1][iy];
+        const float xdy = sp.th[0][ix] * sp.dth[1][iy];
+#pragma unroll
+        for (int iz = 0; iz < kPmeOrder; ++iz) {
+          int gz = sp.base[2] + iz;
+          if (gz >= Kz) gz -= Kz;
+          const float p = row[gz];
+          ga = fmaf(p * dxy, sp.th[2][iz], ga);
+          gb = fmaf(p * xdy, sp.th[2][iz], gb);
+          gc = fmaf(p * wxy, sp.dth[2][iz], gc);
+        }
+      }
+    }
+    // F_v = -q sum_u (dE/du_u) K_u M[v][u]  (pme.ts:252-259)
+    const float* U = S.umat_f;
+    const float fx = -q * (ga * U[0] + gb * U[1] + gc * U[2]);
+    const float fy = -q * (ga * U[3] + gb * U[4] + gc * U[5]);
+    const float fz = -q * (ga * U[6] + gb * U[7] + gc * U[8]);
+    add_fixed(&d.fx[gs], fx);
+    add_fixed(&d.fy[gs], fy);
+    add_fixed(&d.fz[gs], fz);
+  }
+}
+
+int grid_blocks(int n) {
+  int b = (n + kThreads - 1) / kThreads;
+  if (b > 148 * 16) b = 148 * 16;
+  return b < 1 ? 1 : b;
+}
+
+}  // namespace
+
+// Shared-memory bytes for the largest work item of each pass, set by the host.
+struct PmeSmem { int z, y, x; };
+static PmeSmem g_smem{0, 0, 0};
+void set_pme_smem(int z, int y, int x) {
+  g_smem = {z, y, x};
+  cudaFuncSetAttribute(k_fft_z_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, z);
+  cudaFuncSetAttribute(k_fft_z_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, z);
+  cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, y);
+  cudaFuncSetAttribute(k_fft_x_convolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+  cudaFuncSetAttribute(k_fft_x_convolve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+}
+
+void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
+  if (d.n_fft_z == 0) return;
+  k_spread<<<grid_blocks(d.n_slots), kThreads, 0, st>>>(d);
+  k_fft_z_forward<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+  k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, -1);
+  if (energy) k_fft_x_convolve<true><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
+  else k_fft_x_convolve<false><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
+  k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, +1);
+  k_fft_z_inverse<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+  k_gather<<<grid_blocks(d.n_slots), kThreads, 0, st>>>(d);
+}
+
+}  // namespace mdb

@@ -1,0 +1,290 @@
+"""`StepLoop` over the C ABI: the reference's engine surface, in Python.
+
+Mirrors the public members of `StepLoop` (src/gpu/loop.ts:208-1116, paths
+relative to the reference project root) and its `Report` (loop.ts:173-199):
+`create` / `from_parsed`, `run`, `report`, `potential`, `positions`,
+`velocities`, `set_positions`, `set_velocities`, `set_box`,
+`advance_step_count`, `steps`, `barostat_statistics`, `mesh`,
+`box_vectors`, `verlet_flags`, `destroy`.  The per-group evaluators
+`evaluateDirectSpace` / `evaluateReciprocalSpace` / `evaluateBondedForce`
+become `evaluate()`.  Failures raise the reference's named errors.
+
+Every call goes to libmdb200 (CUDA, sm_100a).  There is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .system import State, System, UnsupportedForce, parse_state, parse_system
+
+BOLTZMANN = 0.008314462618153242
+
+
+class EngineError(RuntimeError):
+    """A failure reported by the engine, with its status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class CutoffTooLargeForBox(EngineError):
+    """src/reference/triclinic.ts:179."""
+
+
+class ClusterTooLarge(EngineError):
+    """src/engine/constraint-clusters.ts:71."""
+
+
+class NotSmooth(EngineError):
+    """src/reference/fft.ts:24."""
+
+
+class NoDevice(EngineError):
+    """No CUDA device is visible."""
+
+
+_ERRORS = {
+    abi.ERR_CUTOFF_TOO_LARGE_FOR_BOX: CutoffTooLargeForBox,
+    abi.ERR_CLUSTER_TOO_LARGE: ClusterTooLarge,
+    abi.ERR_NOT_SMOOTH: NotSmooth,
+    abi.ERR_NO_DEVICE: NoDevice,
+}
+
+
+@dataclasses.dataclass
+class RunOptions:
+    """`RunOptions`, src/gpu/loop.ts:117-168."""
+
+    time_step: float = 0.002
+    temperature: float = 300.0
+    friction: float = 1.0
+    constraint_tolerance: float = 1e-6
+    seed: int = 0
+    integrator: str = "lfmiddle"
+    verlet_skin: Optional[float] = None
+    max_batch: int = 100
+    mesh: Optional[Sequence[int]] = None
+    device: int = 0
+    graphs: bool = True
+    always_rebuild: bool = False
+
+    def to_c(self) -> abi.RunOptions:
+        o = abi.RunOptions()
+        o.time_step = self.time_step
+        o.temperature = self.temperature
+        o.friction = self.friction
+        o.constraint_tolerance = self.constraint_tolerance
+        o.seed = int(self.seed) & 0xFFFFFFFF
+        o.integrator = abi.INTEGRATOR_VERLET if self.integrator == "verlet" else abi.INTEGRATOR_LFMIDDLE
+        o.verlet_skin = -1.0 if self.verlet_skin is None else float(self.verlet_skin)
+        o.max_batch = int(self.max_batch)
+        o.mesh[:] = list(self.mesh) if self.mesh is not None else [0, 0, 0]
+        o.device = int(self.device)
+        o.flags = (0 if self.graphs else abi.FLAG_NO_GRAPH) | (abi.FLAG_ALWAYS_REBUILD if self.always_rebuild else 0)
+        return o
+
+
+@dataclasses.dataclass
+class Report:
+    """`Report`, src/gpu/loop.ts:173-199."""
+
+    step: int
+    time: float
+    potential_energy: float
+    kinetic_energy: float
+    temperature: float
+    energies: dict
+
+
+class StepLoop:
+    """One engine: a single system, or a batch of independent ones."""
+
+    def __init__(self, handle: C.c_void_p, lib: C.CDLL, systems: list, states: list, options: RunOptions):
+        self._handle = handle
+        self._lib = lib
+        self._systems = systems
+        self._options = options
+        self._start_step = int(states[0].step)
+        self._destroyed = False
+
+    # ---- construction ----------------------------------------------------
+    @classmethod
+    def create(cls, system_xml: str, state_xml: str, options: RunOptions | None = None) -> "StepLoop":
+        """`StepLoop.create`, loop.ts:268 -- from OpenMM XML text."""
+        return cls.from_parsed(parse_system(system_xml), parse_state(state_xml), options)
+
+    @classmethod
+    def from_parsed(cls, system: System, state: State, options: RunOptions | None = None) -> "StepLoop":
+        """`StepLoop.fromParsed`, loop.ts:278."""
+        return cls.batch([system], [state], options)
+
+    @classmethod
+    def batch(cls, systems: Sequence[System], states: Sequence[State],
+              options: RunOptions | None = None) -> "StepLoop":
+        """Many independent systems in one engine (no reference counterpart)."""
+        options = options or RunOptions()
+        lib = abi.load()
+        if len(systems) != len(states) or not systems:
+            raise ValueError("one state per system, and at least one system")
+        sys_handles = [s.desc() for s in systems]
+        st_handles = [s.desc() for s in states]
+        sys_array = (abi.SystemDesc * len(systems))(*[h.desc for h in sys_handles])
+        st_array = (abi.StateDesc * len(states))(*[h.desc for h in st_handles])
+        opts = options.to_c()
+        handle = C.c_void_p()
+        status = lib.mdb_batch_create(len(systems), sys_array, st_array, C.byref(opts), C.byref(handle))
+        if status != abi.OK:
+            message = lib.mdb_last_error(handle).decode() if handle.value else abi.load().mdb_status_string(status).decode()
+            if handle.value:
+                lib.mdb_destroy(handle, None)
+            raise _ERRORS.get(status, EngineError)(status, message)
+        return cls(handle, lib, list(systems), list(states), options)
+
+    # ---- internals -------------------------------------------------------
+    def _check(self, status: int) -> None:
+        if status != abi.OK:
+            message = self._lib.mdb_last_error(self._handle).decode()
+            raise _ERRORS.get(status, EngineError)(status, message or self._lib.mdb_status_string(status).decode())
+
+    def _n(self, system: int) -> int:
+        return self._systems[system].particle_count
+
+    @staticmethod
+    def _dp(a: np.ndarray):
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    # ---- stepping ----------------------------------------------------------
+    def run(self, steps: int) -> None:
+        """`StepLoop.run(n)`, loop.ts:651."""
+        self._check(self._lib.mdb_run(self._handle, int(steps)))
+
+    def run_timed(self, steps: int) -> float:
+        """Run and return the device time in ms (CUDA events on the engine stream)."""
+        ms = C.c_double()
+        self._check(self._lib.mdb_run_timed(self._handle, int(steps), C.byref(ms)))
+        return ms.value
+
+    @property
+    def steps(self) -> int:
+        v = C.c_int64()
+        self._check(self._lib.mdb_get_step(self._handle, C.byref(v)))
+        return v.value
+
+    def advance_step_count(self, step: int) -> None:
+        """`StepLoop.advanceStepCount`, loop.ts:564."""
+        if int(step) != step or step < 0:
+            raise ValueError(f"a step count must be a non-negative integer, got {step}")
+        self._check(self._lib.mdb_set_step(self._handle, int(step)))
+
+    # ---- state -------------------------------------------------------------
+    def positions(self, system: int = 0) -> np.ndarray:
+        out = np.zeros(self._n(system) * 3)
+        self._check(self._lib.mdb_get_positions(self._handle, system, self._dp(out)))
+        return out.reshape(-1, 3)
+
+    def velocities(self, system: int = 0) -> np.ndarray:
+        out = np.zeros(self._n(system) * 3)
+        self._check(self._lib.mdb_get_velocities(self._handle, system, self._dp(out)))
+        return out.reshape(-1, 3)
+
+    def set_positions(self, positions, system: int = 0) -> None:
+        p = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1))
+        if p.size != self._n(system) * 3:
+            raise ValueError(f"expected {self._n(system) * 3} coordinates, got {p.size}")
+        self._check(self._lib.mdb_set_positions(self._handle, system, self._dp(p)))
+
+    def set_velocities(self, velocities, system: int = 0) -> None:
+        v = np.ascontiguousarray(np.asarray(velocities, dtype=np.float64).reshape(-1))
+        if v.size != self._n(system) * 3:
+            raise ValueError(f"expected {self._n(system) * 3} velocities, got {v.size}")
+        self._check(self._lib.mdb_set_velocities(self._handle, system, self._dp(v)))
+
+    def set_box(self, vectors, system: int = 0) -> None:
+        b = np.ascontiguousarray(np.asarray(vectors, dtype=np.float64).reshape(9))
+        self._check(self._lib.mdb_set_box(self._handle, system, self._dp(b)))
+
+    def box_vectors(self, system: int = 0) -> np.ndarray:
+        b = np.zeros(9)
+        self._check(self._lib.mdb_get_box(self._handle, system, self._dp(b)))
+        return b.reshape(3, 3)
+
+    def mesh(self, system: int = 0) -> tuple:
+        m = (C.c_int32 * 3)()
+        self._check(self._lib.mdb_get_mesh(self._handle, system, m))
+        return tuple(m)
+
+    # ---- evaluation ----------------------------------------------------------
+    def evaluate(self, system: int = 0):
+        """Energies by group and forces (N, 3) at the current configuration."""
+        f = np.zeros(self._n(system) * 3)
+        e = abi.Energies()
+        self._check(self._lib.mdb_evaluate(self._handle, system, self._dp(f), C.byref(e)))
+        return e.as_dict(), f.reshape(-1, 3)
+
+    def potential(self, positions, system: int = 0):
+        """`StepLoop.potential(positions)`, loop.ts:870: (energy, forces), state unchanged."""
+        p = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1))
+        f = np.zeros_like(p)
+        e = abi.Energies()
+        self._check(self._lib.mdb_potential(self._handle, system, self._dp(p), self._dp(f), C.byref(e)))
+        return e.potential, f.reshape(-1, 3)
+
+    def report(self, system: int = 0) -> Report:
+        """`StepLoop.report()`, loop.ts:761."""
+        energies, _ = self.evaluate(system)
+        step = self.steps
+        return Report(step=step, time=step * self._options.time_step,
+                      potential_energy=energies["potential"], kinetic_energy=energies["kinetic"],
+                      temperature=energies["temperature"], energies=energies)
+
+    # ---- statistics -----------------------------------------------------------
+    def barostat_statistics(self, system: int = 0) -> dict:
+        s = abi.BarostatStats()
+        self._check(self._lib.mdb_get_barostat_stats(self._handle, system, C.byref(s)))
+        return {"attempts": s.attempts, "accepted": s.accepted, "volumeScale": s.volume_scale,
+                "screened": s.screened, "exactEvaluations": s.exact_evaluations}
+
+    def verlet_flags(self, system: int = 0) -> dict:
+        """`StepLoop.verletFlags`, loop.ts:941."""
+        s = abi.NeighbourStats()
+        self._check(self._lib.mdb_get_neighbour_stats(self._handle, system, C.byref(s)))
+        return {"rebuilds": s.rebuilds, "tiles": s.tiles, "tileCapacity": s.tile_capacity,
+                "blocks": s.blocks, "overflowed": bool(s.overflowed), "skin": s.skin}
+
+    def memory_report(self) -> dict:
+        buf = C.create_string_buffer(1 << 16)
+        total = C.c_int64()
+        self._check(self._lib.mdb_memory_report(self._handle, buf, len(buf), C.byref(total)))
+        out = {}
+        for item in buf.value.decode().split(";"):
+            if "=" in item:
+                k, v = item.split("=")
+                out[k] = int(v)
+        return out
+
+    def destroy(self) -> dict:
+        """`StepLoop.destroy()`, loop.ts:1113: {leaked: bytes}."""
+        if self._destroyed:
+            return {"leaked": 0}
+        leaked = C.c_int64()
+        self._lib.mdb_destroy(self._handle, C.byref(leaked))
+        self._destroyed = True
+        return {"leaked": leaked.value}
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order varies
+        try:
+            if not self._destroyed:
+                self.destroy()
+        except Exception:
+            pass
+
+
+__all__ = ["StepLoop", "RunOptions", "Report", "EngineError", "CutoffTooLargeForBox", "ClusterTooLarge",
+           "NotSmooth", "NoDevice", "UnsupportedForce"]

@@ -1,0 +1,172 @@
+"""Parity of the CUDA engine against the f64 oracle, through the C ABI.
+
+Tolerances are the reference's own (src/gpu/validate.ts:80-117,
+src/gpu/validate-loop.ts:90-100) and the north-star force bound:
+  forces                     relative RMS <= 1.1e-6 against the f64 oracle
+  direct-space group energy  1e-4 relative
+  reciprocal group energy    1e-5 relative
+  bonded energies            1e-5 relative
+  one LFMiddle step          positions 4e-7 nm, velocities 4e-4 nm/ps
+  repeat runs                bit-identical
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_nonbonded_system
+
+pytestmark = pytest.mark.gpu
+
+FORCE_REL_RMS = 1.1e-6
+
+
+def rel_rms(a, b):
+    a = np.asarray(a).reshape(-1)
+    b = np.asarray(b).reshape(-1)
+    return float(np.sqrt(((a - b) ** 2).sum() / (b**2).sum()))
+
+
+@pytest.fixture(scope="module")
+def mdb():
+    from mdb200 import steploop
+
+    return steploop
+
+
+@pytest.fixture(scope="module")
+def water():
+    from mdb200 import synth
+
+    return synth.config_water_2652()
+
+
+def make_loop(mdb, system, state, **kw):
+    opts = mdb.RunOptions(**kw)
+    return mdb.StepLoop.from_parsed(system, state, opts)
+
+
+def test_fixture_groups_and_forces(mdb, oracle):
+    """The reference's 10-particle OpenMM fixture (nonbonded-reference.test.ts)."""
+    system, state, g = golden_nonbonded_system()
+    mesh = (24, 24, 24)
+    loop = make_loop(mdb, system, state, mesh=mesh, friction=0.0)
+    e, f = loop.evaluate()
+    want, wf = oracle.potential(system, state.positions, grid=mesh)
+    for key in ("direct_coulomb", "direct_lj", "exclusion_correction", "exceptions"):
+        assert abs(e[key] - want[key]) <= 1e-4 * max(1.0, abs(want[key])), (key, e[key], want[key])
+    assert abs(e["reciprocal_group"] - want["reciprocal_group"]) <= 1e-5 * abs(want["reciprocal_group"])
+    assert abs(e["direct_group"] - want["direct_group"]) <= 1e-4 * abs(want["direct_group"])
+    err = rel_rms(f, wf)
+    print("fixture force rel RMS", err)
+    assert err < 2e-6, err
+    loop.destroy()
+
+
+def test_water_forces_and_groups(mdb, oracle, water):
+    system, state = water
+    loop = make_loop(mdb, system, state)
+    e, f = loop.evaluate()
+    want, wf = oracle.potential(system, state.positions, grid=(30, 30, 30))
+    err = rel_rms(f, wf)
+    print("water force rel RMS", err)
+    print({k: (e[k], want[k]) for k in want if k in e})
+    assert err <= FORCE_REL_RMS, err
+    assert abs(e["direct_group"] - want["direct_group"]) <= 1e-4 * abs(want["direct_group"])
+    assert abs(e["reciprocal_group"] - want["reciprocal_group"]) <= 1e-5 * abs(want["reciprocal_group"])
+    assert abs(e["direct_coulomb"] - want["direct_coulomb"]) <= 1e-4 * abs(want["direct_coulomb"]) + 1e-3
+    assert abs(e["direct_lj"] - want["direct_lj"]) <= 1e-4 * abs(want["direct_lj"])
+    loop.destroy()
+
+
+def test_one_step_matches_oracle(mdb, oracle, water):
+    """validate-loop.ts:90-94: one LFMiddle step, friction on, same Threefry stream."""
+    system, state = water
+    loop = make_loop(mdb, system, state, seed=11)
+    loop.run(1)
+    p, v = loop.positions(), loop.velocities()
+    op, ov, _ = oracle.run(system, state, 1, seed=11, grid=(30, 30, 30))
+    dp = np.abs(p - op).max()
+    dv = np.abs(v - ov).max()
+    print("one step: max |dx|", dp, "max |dv|", dv)
+    assert dp <= 4e-7, dp
+    assert dv <= 4e-4, dv
+    loop.destroy()
+
+
+def test_repeat_runs_are_bit_identical(mdb, water):
+    system, state = water
+    out = []
+    for _ in range(2):
+        loop = make_loop(mdb, system, state, seed=3)
+        loop.run(50)
+        out.append((loop.positions(), loop.velocities()))
+        loop.destroy()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_graph_and_direct_launch_agree(mdb, water):
+    system, state = water
+    res = []
+    for graphs in (True, False):
+        loop = make_loop(mdb, system, state, seed=3, graphs=graphs, max_batch=7)
+        loop.run(20)
+        res.append(loop.positions())
+        loop.destroy()
+    assert np.array_equal(res[0], res[1])
+
+
+def test_batch_equals_single(mdb, water):
+    """Two systems in one engine advance exactly as each does alone."""
+    from mdb200 import synth
+
+    system, state = water
+    other_sys, other_state = synth.water_box(n_waters=600, width=2.8, seed=7, grid=(28, 28, 28))
+    single = []
+    for s, st in ((system, state), (other_sys, other_state)):
+        loop = make_loop(mdb, s, st, seed=5)
+        loop.run(20)
+        single.append(loop.positions())
+        loop.destroy()
+    batch = mdb.StepLoop.batch([system, other_sys], [state, other_state], mdb.RunOptions(seed=5))
+    batch.run(20)
+    assert np.array_equal(batch.positions(0), single[0])
+    assert np.array_equal(batch.positions(1), single[1])
+    batch.destroy()
+
+
+def test_potential_leaves_state_and_matches_evaluate(mdb, water):
+    system, state = water
+    loop = make_loop(mdb, system, state)
+    before = loop.positions()
+    shifted = state.positions + 0.01
+    e_shift, f_shift = loop.potential(shifted)
+    assert np.array_equal(loop.positions(), before)
+    e0, f0 = loop.evaluate()
+    # A uniform translation changes nothing physical; what moves is f32
+    # rounding, relative to the largest energy group (|exclusion| ~ 2e5 here).
+    assert abs(e_shift - e0["potential"]) < 1e-7 * abs(e0["exclusion_correction"])
+    assert rel_rms(f_shift, f0) < 1e-5
+    loop.destroy()
+
+
+def test_dynamics_stay_bounded(mdb, water):
+    system, state = water
+    loop = make_loop(mdb, system, state, seed=2)
+    loop.run(300)
+    r = loop.report()
+    print("after 300 steps", r.temperature, r.potential_energy, loop.verlet_flags())
+    assert 150 < r.temperature < 450
+    assert loop.verlet_flags()["rebuilds"] >= 1
+    assert not loop.verlet_flags()["overflowed"]
+    loop.destroy()
+
+
+def test_cutoff_too_large_is_refused(mdb):
+    from mdb200 import synth
+
+    system, state = synth.water_box(n_waters=100, width=1.5, seed=1, grid=(16, 16, 16))
+    with pytest.raises(mdb.CutoffTooLargeForBox):
+        make_loop(mdb, system, state)
