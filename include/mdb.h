@@ -193,6 +193,7 @@ typedef struct mdb_energies {
   double temperature;          /* K, from `kinetic` and the constrained DoF */
   double degrees_of_freedom;
   double virial[9];            /* sum of r (x) F over pairs, lattice-resolved; kJ/mol */
+  double pairs_within_cutoff;  /* non-excluded pairs inside the cutoff (count) */
 } mdb_energies;
 
 /* Mirrors `StepLoop.barostatStatistics`, src/gpu/loop.ts:572. */
@@ -204,6 +205,31 @@ typedef struct mdb_barostat_stats {
   int64_t screened;        /* proposals decided by the surrogate stage alone */
   int64_t exact_evaluations;
 } mdb_barostat_stats;
+
+/*
+ * Device time per stage of one step, each stage launched alone on the
+ * engine's stream and timed with CUDA events over `repeats` launches.
+ * Mirrors `StepLoop.profileStep()`, src/gpu/loop.ts:705, and like it
+ * advances the system (the integrator stage runs `repeats` times).
+ */
+typedef struct mdb_profile {
+  int32_t launches_per_step;   /* kernels one graph-replayed step launches */
+  int32_t repeats;
+  double ms_step;              /* one whole step, as replayed from a graph */
+  double ms_list_check;        /* list kernels when no rebuild is due */
+  double ms_list_rebuild;      /* a full sort + tile-list rebuild */
+  double ms_nonbonded;
+  double ms_listed;
+  double ms_pme;               /* spread + 5 FFT passes + gather */
+  double ms_pme_spread;
+  double ms_pme_fft;
+  double ms_pme_gather;
+  double ms_integrate;
+  int64_t pairs_within_cutoff; /* at the configuration profiled */
+  int64_t tiles;
+  int64_t atoms;
+  int64_t mesh_points;
+} mdb_profile;
 
 /* Mirrors `StepLoop.verletFlags`, src/gpu/loop.ts:941. */
 typedef struct mdb_neighbour_stats {
@@ -310,6 +336,9 @@ int mdb_get_barostat_stats(const mdb_engine* engine, int32_t system,
                            mdb_barostat_stats* out);
 int mdb_get_neighbour_stats(mdb_engine* engine, int32_t system,
                             mdb_neighbour_stats* out);
+
+/* Per-stage device timing (see mdb_profile).  Replaces `StepLoop.profileStep`, loop.ts:705. */
+int mdb_profile_step(mdb_engine* engine, int32_t repeats, mdb_profile* out);
 
 /*
  * Device memory the engine holds, by owner label, as "label=bytes;" pairs in

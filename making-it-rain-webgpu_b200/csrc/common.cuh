@@ -40,7 +40,8 @@ enum EnergySlot : int {
   kEExclusion,
   kEException,
   kEVirial0,  // 9 virial components follow
-  kECount = kEVirial0 + 9
+  kEPairs = kEVirial0 + 9,  // in-cutoff pair count (an integer, not fixed point)
+  kECount
 };
 
 // Device status bits, OR-ed into `err` and turned into C-ABI codes by the host.

@@ -66,6 +66,7 @@ struct Dev {
   int* err;           // per system ErrorBit
   long long* rebuild_count;
   int* global_ticket;
+  unsigned int* list_barrier;  // count, generation: the cooperative list kernel's grid barrier
 
   // exclusions (every exception pair)
   const int2* excl;
@@ -106,13 +107,17 @@ struct Dev {
 };
 
 // ---- launchers (one per kernel file) ----
-void launch_rebuild_decide(const Dev& d, cudaStream_t s);
+int prepare_list_kernel(int device);                      // 0: no cooperative launch
+bool launch_list(const Dev& d, cudaStream_t s);            // sort + wrap + tiles, one launch
 void launch_rebuild_sort(const Dev& d, cudaStream_t s);     // phases 0-4
 void launch_wrap(const Dev& d, cudaStream_t s);
 void launch_rebuild_tiles(const Dev& d, cudaStream_t s);    // phases 5-9
 void launch_nonbonded(const Dev& d, bool energy, cudaStream_t s);
 void launch_listed(const Dev& d, bool energy, cudaStream_t s);
 void launch_pme(const Dev& d, bool energy, cudaStream_t s);
+void launch_pme_spread(const Dev& d, cudaStream_t s);
+void launch_pme_fft(const Dev& d, bool energy, cudaStream_t s);
+void launch_pme_gather(const Dev& d, cudaStream_t s);
 void launch_integrate(const Dev& d, cudaStream_t s);
 void launch_momentum(const Dev& d, cudaStream_t s);
 

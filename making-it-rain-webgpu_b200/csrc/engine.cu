@@ -37,7 +37,7 @@ using namespace mdb;
 
 namespace {
 
-constexpr double kCellWidth = 0.3;  // nm, fractional cells of the spatial sort
+constexpr double kCellWidth = 0.25;  // nm, fractional cells of the spatial sort
 constexpr int kIntegrateBlock = 128;
 constexpr int kFftTile = 16;
 
@@ -71,6 +71,7 @@ struct mdb_engine {
   std::string error;
   int n_mesh_items = 0;
   std::vector<int> fft_x_sys;  // system of each x-pass work item
+  bool coop_list = false;      // the list kernels run as one cooperative launch
 };
 
 namespace {
@@ -111,20 +112,47 @@ int upload(mdb_engine* e, const char* label, T*& out, const std::vector<T>& host
 
 long long to_fixed_host(double x) { return std::llround(x * 4294967296.0); }
 
-// Morton order of the fractional cells, so consecutive slots stay compact.
-std::vector<int> morton_map(const int* dim) {
+// Position of a cell along the 3D Hilbert curve of side 2^bits: Skilling's
+// axes-to-transpose conversion ("Programming the Hilbert curve", AIP Conf.
+// Proc. 707, 381, 2004), then the transposed bits interleaved.
+uint64_t hilbert_index(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t X[3] = {x, y, z};
+  const uint32_t M = 1u << (bits - 1);
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {
+    const uint32_t P = Q - 1;
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < 3; ++i) X[i] ^= X[i - 1];
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  for (int i = 0; i < 3; ++i) X[i] ^= t;
+  uint64_t h = 0;
+  for (int b = bits - 1; b >= 0; --b)
+    for (int i = 0; i < 3; ++i) h = (h << 1) | ((X[i] >> b) & 1u);
+  return h;
+}
+
+// Hilbert order of the fractional cells: consecutive cells are neighbours, so
+// 32 consecutive slots form a compact cluster and its bounding box is small.
+std::vector<int> cell_order_map(const int* dim) {
   const int n = dim[0] * dim[1] * dim[2];
+  int bits = 1;
+  while ((1 << bits) < std::max({dim[0], dim[1], dim[2]})) ++bits;
   std::vector<std::pair<uint64_t, int>> keys(n);
-  auto spread = [](uint64_t v) {
-    uint64_t r = 0;
-    for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
-    return r;
-  };
   for (int x = 0; x < dim[0]; ++x)
     for (int y = 0; y < dim[1]; ++y)
       for (int z = 0; z < dim[2]; ++z) {
         const int id = (x * dim[1] + y) * dim[2] + z;
-        keys[id] = {spread(x) | (spread(y) << 1) | (spread(z) << 2), id};
+        keys[id] = {hilbert_index(uint32_t(x), uint32_t(y), uint32_t(z), bits), id};
       }
   std::sort(keys.begin(), keys.end());
   std::vector<int> map(n);
@@ -179,11 +207,18 @@ int check_device_status(mdb_engine* e) {
   return MDB_OK;
 }
 
+// Sort, wrap and tile list: one cooperative launch when the device can, else
+// the phase kernels one by one.
+void list_kernels(mdb_engine* e, cudaStream_t st) {
+  if (e->coop_list && launch_list(e->d, st)) return;
+  launch_rebuild_sort(e->d, st);
+  launch_wrap(e->d, st);
+  launch_rebuild_tiles(e->d, st);
+}
+
 void launch_step(mdb_engine* e) {
   const Dev& d = e->d;
-  launch_rebuild_sort(d, e->s0);
-  launch_wrap(d, e->s0);
-  launch_rebuild_tiles(d, e->s0);
+  list_kernels(e, e->s0);
   cudaEventRecord(e->fork, e->s0);
   cudaStreamWaitEvent(e->s1, e->fork, 0);
   cudaStreamWaitEvent(e->s2, e->fork, 0);
@@ -362,7 +397,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     for (int k = 0; k < S.n_slots; ++k) slot_sys.push_back(s);
     for (int k = 0; k < S.n_blocks; ++k) block_sys.push_back(s);
     for (int k = 0; k < S.n_cells; ++k) cell_sys.push_back(s);
-    const std::vector<int> mm = morton_map(S.cdim);
+    const std::vector<int> mm = cell_order_map(S.cdim);
     cell_map.insert(cell_map.end(), mm.begin(), mm.end());
 
     // listed terms, global indices
@@ -502,7 +537,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "cell cursor", d.cell_cur, cells));
   TRY(upload(e, "cell system", tmp_i, cell_sys));
   d.cell_sys = tmp_i;
-  TRY(upload(e, "cell morton map", tmp_i, cell_map));
+  TRY(upload(e, "cell order map", tmp_i, cell_map));
   d.cell_map = tmp_i;
   TRY(alloc(e, "tiles", d.tiles, tiles));
   TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * 32));
@@ -514,6 +549,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "status", d.err, n));
   TRY(alloc(e, "rebuild count", d.rebuild_count, n));
   TRY(alloc(e, "launch ticket", d.global_ticket, 1));
+  TRY(alloc(e, "list grid barrier", d.list_barrier, 2));
   int2* ex_dev = nullptr;
   TRY(upload(e, "exclusions", ex_dev, excl));
   d.excl = ex_dev;
@@ -584,14 +620,33 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   CUDA_TRY(e, cudaEventCreate(&e->t1));
   CUDA_TRY(e, cudaDeviceSynchronize());
 
-  // first list and the first COM velocity
+  // first list and the first COM velocity, by the phase kernels
   request_rebuild(e, -1);
   launch_rebuild_sort(d, e->s0);
   launch_wrap(d, e->s0);
   launch_rebuild_tiles(d, e->s0);
   launch_momentum(d, e->s0);
   CUDA_TRY(e, cudaGetLastError());
-  return check_device_status(e);
+  int status = check_device_status(e);
+  if (status) return status;
+
+  // One cooperative launch for the list kernels, if the device has
+  // cooperative launch and a stream capture accepts it.
+  if (prepare_list_kernel(e->device) > 0 && !(e->opt.flags & MDB_FLAG_NO_GRAPH)) {
+    cudaGraph_t g = nullptr;
+    bool ok = cudaStreamBeginCapture(e->s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    ok = launch_list(d, e->s0) && ok;
+    ok = (cudaStreamEndCapture(e->s0, &g) == cudaSuccess) && ok;
+    cudaGraphExec_t exec = nullptr;
+    ok = ok && g && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();  // a refused probe leaves no sticky error behind
+    e->coop_list = ok;
+  } else if (prepare_list_kernel(e->device) > 0) {
+    e->coop_list = true;
+  }
+  return MDB_OK;
 }
 
 int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
@@ -599,9 +654,7 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
   const HostSystem& h = e->hs[s];
   const SysDev& S = e->sd[s];
   CUDA_TRY(e, cudaMemsetAsync(d.energy, 0, sizeof(unsigned long long) * d.S * kECount, e->s0));
-  launch_rebuild_sort(d, e->s0);
-  launch_wrap(d, e->s0);
-  launch_rebuild_tiles(d, e->s0);
+  list_kernels(e, e->s0);
   launch_pme(d, true, e->s0);
   launch_listed(d, true, e->s0);
   launch_nonbonded(d, true, e->s0);
@@ -641,6 +694,7 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
     out->direct_lj = val(kELj);
     out->exclusion_correction = val(kEExclusion);
     out->exceptions = val(kEException);
+    out->pairs_within_cutoff = double(static_cast<long long>(en[kEPairs]));
     out->dispersion = h.dispersion_energy;
     out->reciprocal_mesh = em;
     out->self_energy = h.self_energy;
@@ -1042,6 +1096,63 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   out->overflowed = (err & kErrTileCapacity) ? 1 : 0;
   out->skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
   return MDB_OK;
+}
+
+int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
+  if (!e || !out || repeats <= 0) return MDB_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  const Dev& d = e->d;
+  cudaStream_t st = e->s0;
+  auto time = [&](auto&& body) -> double {
+    cudaEventRecord(e->t0, st);
+    for (int r = 0; r < repeats; ++r) body();
+    cudaEventRecord(e->t1, st);
+    cudaEventSynchronize(e->t1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->t0, e->t1);
+    return double(ms) / repeats;
+  };
+  // pairs and tiles at this configuration
+  mdb_energies en{};
+  int status = evaluate(e, 0, nullptr, &en);
+  if (status) return status;
+  out->pairs_within_cutoff = int64_t(en.pairs_within_cutoff);
+  int tiles = 0;
+  cudaMemcpy(&tiles, d.tile_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost);
+  out->tiles = tiles;
+  out->atoms = d.n_atoms;
+  for (const auto& h : e->hs) out->mesh_points += int64_t(h.grid[0]) * h.grid[1] * h.grid[2];
+  out->repeats = repeats;
+  // whole step from a graph (warmed once)
+  status = run_steps(e, 1);
+  if (status) return status;
+  out->ms_step = time([&] { run_steps(e, 1); });
+  // the list kernels with no rebuild due, then with one forced
+  list_kernels(e, st);
+  CUDA_TRY(e, cudaMemsetAsync(d.any_rebuild, 0, sizeof(int), st));
+  out->ms_list_check = time([&] { list_kernels(e, st); });
+  std::vector<int> ones(d.S, 1);
+  const int one = 1;
+  out->ms_list_rebuild = time([&] {
+    cudaMemcpyAsync(d.rebuild_now, ones.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, st);
+    list_kernels(e, st);
+  });
+  out->ms_nonbonded = time([&] { launch_nonbonded(d, false, st); });
+  out->ms_listed = time([&] { launch_listed(d, false, st); });
+  out->ms_pme_spread = time([&] { launch_pme_spread(d, st); });
+  out->ms_pme_fft = time([&] { launch_pme_fft(d, false, st); });
+  out->ms_pme_gather = time([&] { launch_pme_gather(d, st); });
+  out->ms_pme = time([&] { launch_pme(d, false, st); });
+  out->ms_integrate = time([&] { launch_integrate(d, st); });
+  // 5 sort + 1 wrap + 6 tile-list kernels, 7 PME, listed, nonbonded, integrator
+  out->launches_per_step = 5 + 1 + 6 + (d.n_fft_z ? 7 : 0) + (d.n_bonds + d.n_angles + d.n_torsions +
+                                                              d.n_exceptions + d.n_restraints > 0 ? 1 : 0) + 1 + 1;
+  CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, st));
+  CUDA_TRY(e, cudaMemsetAsync(d.fy, 0, sizeof(long long) * d.n_slots, st));
+  CUDA_TRY(e, cudaMemsetAsync(d.fz, 0, sizeof(long long) * d.n_slots, st));
+  CUDA_TRY(e, cudaGetLastError());
+  return check_device_status(e);
 }
 
 int mdb_memory_report(const mdb_engine* e, char* buffer, int64_t capacity, int64_t* total_bytes) {

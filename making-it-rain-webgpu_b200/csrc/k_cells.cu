@@ -14,6 +14,8 @@
 // A rebuild happens only when the integrator saw an atom move more than skin/2
 // (verlet.wgsl:57), decided on the device; every phase kernel returns at once
 // when no system asked for one.
+#include <algorithm>
+
 #include "device_state.h"
 
 namespace mdb {
@@ -59,8 +61,7 @@ __device__ __forceinline__ int cell_index(unsigned int frac, int dim) {
 
 // ---------------------------------------------------------------- phases --
 
-__global__ void k_cells_clear(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_cells_clear(const Dev& d) {
   for (int c = grid_stride_start(); c < d.n_cells; c += grid_stride()) {
     if (!d.rebuild_now[d.cell_sys[c]]) continue;
     d.cell_cnt[c] = 0;
@@ -68,8 +69,7 @@ __global__ void k_cells_clear(Dev d) {
   }
 }
 
-__global__ void k_cells_assign(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_cells_assign(const Dev& d) {
   for (int a = grid_stride_start(); a < d.n_atoms; a += grid_stride()) {
     const int s = d.atom_sys[a];
     if (!d.rebuild_now[s]) continue;
@@ -121,8 +121,7 @@ __device__ int block_exclusive_scan(const int* in, int* out, int n) {
   return carry;
 }
 
-__global__ void k_cells_scan(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_cells_scan(const Dev& d) {
   for (int s = blockIdx.x; s < d.S; s += gridDim.x) {
     if (!d.rebuild_now[s]) continue;
     const SysDev& S = d.sys[s];
@@ -130,8 +129,7 @@ __global__ void k_cells_scan(Dev d) {
   }
 }
 
-__global__ void k_cells_scatter(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_cells_scatter(const Dev& d) {
   for (int a = grid_stride_start(); a < d.n_atoms; a += grid_stride()) {
     const int s = d.atom_sys[a];
     if (!d.rebuild_now[s]) continue;
@@ -144,8 +142,7 @@ __global__ void k_cells_scatter(Dev d) {
 // Ascending atom index inside each cell, by rank: the order is a function of
 // the positions alone, whatever order the scatter's atomics landed in
 // (cell-list.wgsl:319 sort_cells).
-__global__ void k_cells_order(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_cells_order(const Dev& d) {
   for (int gs = grid_stride_start(); gs < d.n_slots; gs += grid_stride()) {
     const int s = d.slot_sys[gs];
     if (!d.rebuild_now[s]) continue;
@@ -167,7 +164,7 @@ __global__ void k_cells_order(Dev d) {
 
 // Every step, every system: pair coordinates of each slot, folded into the
 // cell, as int32 at 2^pc_shift per nm (cell-list.wgsl:140 `wrap`).
-__global__ void k_wrap(Dev d) {
+__device__ void phase_wrap(const Dev& d) {
   for (int gs = grid_stride_start(); gs < d.n_slots; gs += grid_stride()) {
     const int a = d.order[gs];
     if (a < 0) {
@@ -183,8 +180,7 @@ __global__ void k_wrap(Dev d) {
 
 // Warp per block: parameters in slot order, bounding box, and the reference
 // positions the displacement test measures against.
-__global__ void k_tiles_blocks(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_tiles_blocks(const Dev& d) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < d.n_blocks; b += warps) {
@@ -254,8 +250,7 @@ __device__ __forceinline__ bool blocks_near(const SysDev& S, const Dev& d, int I
   return best < S.list2;
 }
 
-__global__ void k_tiles_count(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_tiles_count(const Dev& d) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < d.n_blocks; I += warps) {
@@ -273,8 +268,7 @@ __global__ void k_tiles_count(Dev d) {
   }
 }
 
-__global__ void k_tiles_scan(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_tiles_scan(const Dev& d) {
   for (int s = blockIdx.x; s < d.S; s += gridDim.x) {
     if (!d.rebuild_now[s]) continue;
     const SysDev& S = d.sys[s];
@@ -286,8 +280,7 @@ __global__ void k_tiles_scan(Dev d) {
   }
 }
 
-__global__ void k_tiles_fill(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_tiles_fill(const Dev& d) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < d.n_blocks; I += warps) {
@@ -322,8 +315,7 @@ __global__ void k_tiles_fill(Dev d) {
 }
 
 // Clear the mask bit of every excluded pair in the tile that holds it.
-__global__ void k_tiles_exclusions(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_tiles_exclusions(const Dev& d) {
   for (int e = grid_stride_start(); e < d.n_excl; e += grid_stride()) {
     const int s = d.excl_sys[e];
     if (!d.rebuild_now[s]) continue;
@@ -348,8 +340,7 @@ __global__ void k_tiles_exclusions(Dev d) {
   }
 }
 
-__global__ void k_tiles_finish(Dev d) {
-  if (!*d.any_rebuild) return;
+__device__ void phase_tiles_finish(const Dev& d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     int total = 0;
     for (int s = 0; s < d.S; ++s) {
@@ -363,12 +354,129 @@ __global__ void k_tiles_finish(Dev d) {
   }
 }
 
+// Grid-wide barrier for the cooperative list kernel: arrive on a counter,
+// the last arrival bumps the generation, the others wait on it with a bounded
+// spin.  A wait that gives up records kErrTimeout and returns, so a scheduling
+// fault becomes an error status and never a hung GPU.
+__device__ bool grid_barrier(unsigned int* bar, int* err) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned int* gen = bar + 1;
+    const unsigned int mine = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+      bar[0] = 0u;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*gen == mine) {
+        if (++spins > (1ll << 22)) {
+          atomicOr(err, kErrTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// One launch per step.  With no rebuild requested it only folds the pair
+// coordinates; otherwise it runs the sort and tile-list phases with a grid
+// barrier between them.
+__global__ void __launch_bounds__(kThreads) k_list(Dev d) {
+  const bool rebuild = *d.any_rebuild != 0;
+  if (!rebuild) {
+    phase_wrap(d);
+    return;
+  }
+  int* err = d.err;  // system 0's word carries a barrier timeout
+  phase_cells_clear(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_cells_assign(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_cells_scan(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_cells_scatter(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_cells_order(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_wrap(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_tiles_blocks(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_tiles_count(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_tiles_scan(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_tiles_fill(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_tiles_exclusions(d);
+  if (!grid_barrier(d.list_barrier, err)) return;
+  phase_tiles_finish(d);
+}
+
+// The same phases as separate launches (the path the graph-free debug mode
+// and devices without cooperative launch take).
+#define MDB_PHASE_KERNEL(name, guarded)                            \
+  __global__ void __launch_bounds__(kThreads) k_##name(Dev d) {   \
+    if (guarded && !*d.any_rebuild) return;                        \
+    phase_##name(d);                                               \
+  }
+MDB_PHASE_KERNEL(cells_clear, true)
+MDB_PHASE_KERNEL(cells_assign, true)
+MDB_PHASE_KERNEL(cells_scan, true)
+MDB_PHASE_KERNEL(cells_scatter, true)
+MDB_PHASE_KERNEL(cells_order, true)
+MDB_PHASE_KERNEL(wrap, false)
+MDB_PHASE_KERNEL(tiles_blocks, true)
+MDB_PHASE_KERNEL(tiles_count, true)
+MDB_PHASE_KERNEL(tiles_scan, true)
+MDB_PHASE_KERNEL(tiles_fill, true)
+MDB_PHASE_KERNEL(tiles_exclusions, true)
+MDB_PHASE_KERNEL(tiles_finish, true)
+#undef MDB_PHASE_KERNEL
+
 int blocks_for(int n, int threads, int cap = 148 * 8) {
   const int b = (n + threads - 1) / threads;
   return b < 1 ? 1 : (b > cap ? cap : b);
 }
 
+int g_list_grid = 0;
+
 }  // namespace
+
+// Size the cooperative grid once: every block resident at the same time.
+int prepare_list_kernel(int device) {
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list, kThreads, 0) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  g_list_grid = coop ? std::max(1, std::min(per_sm, 2)) * sms : 0;
+  return g_list_grid;
+}
+
+bool launch_list(const Dev& d, cudaStream_t st) {
+  if (g_list_grid <= 0) return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g_list_grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_list, d) == cudaSuccess;
+}
 
 void launch_rebuild_sort(const Dev& d, cudaStream_t st) {
   k_cells_clear<<<blocks_for(d.n_cells, kThreads), kThreads, 0, st>>>(d);

@@ -41,7 +41,7 @@ __device__ __forceinline__ float3 rel(const Atom& a, const Atom& o) {
 }
 
 // src/reference/settle.ts:198 -- exact 3x3 impulse solve for the velocities.
-__device__ void settle_velocities(Atom* at) {
+__device__ __forceinline__ void settle_velocities(Atom* at) {
   const float mA = at[0].im > 0 ? 1.f / at[0].im : 0.f, mB = at[1].im > 0 ? 1.f / at[1].im : 0.f,
               mC = at[2].im > 0 ? 1.f / at[2].im : 0.f;
   const float3 pB = rel(at[1], at[0]), pC = rel(at[2], at[0]);
@@ -82,7 +82,7 @@ __device__ void settle_velocities(Atom* at) {
 // src/reference/settle.ts:31 -- Miyamoto & Kollman in the reference frame.
 // `dp` holds each atom's trial displacement from its start position on input
 // and its constrained displacement on output.
-__device__ void settle_positions(const Atom* at, float3* dp, float d1, float d2) {
+__device__ __forceinline__ void settle_positions(const Atom* at, float3* dp, float d1, float d2) {
   const float m0 = 1.f / at[0].im, m1 = 1.f / at[1].im, m2 = 1.f / at[2].im;
   const float3 b0 = rel(at[1], at[0]), c0 = rel(at[2], at[0]);
   const float xb0 = b0.x, yb0 = b0.y, zb0 = b0.z, xc0 = c0.x, yc0 = c0.y, zc0 = c0.z;
@@ -139,68 +139,93 @@ __device__ void settle_positions(const Atom* at, float3* dp, float d1, float d2)
                       zcom + t31 * xc3d + t32 * yc3d + t33 * zc3d - zc0);
 }
 
-// src/reference/constraints.ts:195 -- RATTLE, Jacobi, over one cluster.
-__device__ bool rattle(Atom* at, const UnitDev& u, float tol) {
-  float3 rv[kMaxClusterConstraints];
-  float rl[kMaxClusterConstraints], rm[kMaxClusterConstraints], delta[kMaxClusterConstraints];
-  for (int c = 0; c < u.nc; ++c) {
-    rv[c] = rel(at[u.ci[c]], at[u.cj[c]]);
-    rl[c] = rv[c].x * rv[c].x + rv[c].y * rv[c].y + rv[c].z * rv[c].z;
-    const float sum = at[u.ci[c]].im + at[u.cj[c]].im;
-    rm[c] = sum == 0.f ? 0.f : 0.5f / sum;
+// src/reference/constraints.ts:195 -- RATTLE, Jacobi, over one cluster.  The
+// solve runs in FP64: its absolute 1e-6 convergence test sits at the rounding
+// noise of an f32 velocity difference along a bond, where an f32 iteration
+// stalls short of the tolerance and runs to the 150-iteration cap.
+__device__ __noinline__ bool rattle(Atom* at, const UnitDev& u, float tol) {
+  double rv[kMaxClusterConstraints][3];
+  double rl[kMaxClusterConstraints], rm[kMaxClusterConstraints], delta[kMaxClusterConstraints];
+  double v[kMaxClusterAtoms][3];
+  for (int k = 0; k < u.na; ++k) {
+    v[k][0] = at[k].vx; v[k][1] = at[k].vy; v[k][2] = at[k].vz;
   }
+  for (int c = 0; c < u.nc; ++c) {
+    const float3 r = rel(at[u.ci[c]], at[u.cj[c]]);
+    rv[c][0] = r.x; rv[c][1] = r.y; rv[c][2] = r.z;
+    rl[c] = rv[c][0] * rv[c][0] + rv[c][1] * rv[c][1] + rv[c][2] * rv[c][2];
+    const double sum = double(at[u.ci[c]].im) + at[u.cj[c]].im;
+    rm[c] = sum == 0.0 ? 0.0 : 0.5 / sum;
+  }
+  bool ok = false;
   for (int it = 0; it < kMaxShakeIterations; ++it) {
     int conv = 0;
     for (int c = 0; c < u.nc; ++c) {
-      const Atom &i = at[u.ci[c]], &j = at[u.cj[c]];
-      const float proj = (i.vx - j.vx) * rv[c].x + (i.vy - j.vy) * rv[c].y + (i.vz - j.vz) * rv[c].z;
-      delta[c] = rl[c] == 0.f ? 0.f : (-2.f * rm[c] * proj) / rl[c];
-      conv += fabsf(delta[c]) <= tol;
+      const int i = u.ci[c], j = u.cj[c];
+      const double proj = (v[i][0] - v[j][0]) * rv[c][0] + (v[i][1] - v[j][1]) * rv[c][1] + (v[i][2] - v[j][2]) * rv[c][2];
+      delta[c] = rl[c] == 0.0 ? 0.0 : (-2.0 * rm[c] * proj) / rl[c];
+      conv += fabs(delta[c]) <= tol;
     }
-    if (conv == u.nc) return true;
+    if (conv == u.nc) { ok = true; break; }
     for (int c = 0; c < u.nc; ++c) {
-      Atom &i = at[u.ci[c]], &j = at[u.cj[c]];
-      const float dx = rv[c].x * delta[c], dy = rv[c].y * delta[c], dz = rv[c].z * delta[c];
-      i.vx += dx * i.im; i.vy += dy * i.im; i.vz += dz * i.im;
-      j.vx -= dx * j.im; j.vy -= dy * j.im; j.vz -= dz * j.im;
+      const int i = u.ci[c], j = u.cj[c];
+      const double ii = at[i].im, jj = at[j].im;
+      for (int x = 0; x < 3; ++x) {
+        const double dr = rv[c][x] * delta[c];
+        v[i][x] += dr * ii;
+        v[j][x] -= dr * jj;
+      }
     }
   }
-  return false;
+  for (int k = 0; k < u.na; ++k) {
+    at[k].vx = float(v[k][0]); at[k].vy = float(v[k][1]); at[k].vz = float(v[k][2]);
+  }
+  return ok;
 }
 
 // src/reference/constraints.ts:130 -- SHAKE, Jacobi along the reference bond
-// vectors, over one cluster.  The trial bond vector is the exact reference
-// vector plus the difference of the two displacements, and the convergence
-// window is tested in FP64.
-__device__ bool shake(const Atom* at, float3* dp, const UnitDev& u, float tol) {
-  float3 rv[kMaxClusterConstraints];
-  float rm[kMaxClusterConstraints], delta[kMaxClusterConstraints];
+// vectors, over one cluster, in FP64 (convergence window and updates).  The
+// trial bond vector is the exact reference vector plus the difference of the
+// two displacements.
+__device__ __noinline__ bool shake(const Atom* at, float3* dp, const UnitDev& u, float tol) {
+  double rv[kMaxClusterConstraints][3];
+  double rm[kMaxClusterConstraints], delta[kMaxClusterConstraints];
+  double q[kMaxClusterAtoms][3];
+  for (int k = 0; k < u.na; ++k) {
+    q[k][0] = dp[k].x; q[k][1] = dp[k].y; q[k][2] = dp[k].z;
+  }
   for (int c = 0; c < u.nc; ++c) {
-    rv[c] = rel(at[u.ci[c]], at[u.cj[c]]);
-    const float sum = at[u.ci[c]].im + at[u.cj[c]].im;
-    rm[c] = sum == 0.f ? 0.f : 0.5f / sum;
+    const float3 r = rel(at[u.ci[c]], at[u.cj[c]]);
+    rv[c][0] = r.x; rv[c][1] = r.y; rv[c][2] = r.z;
+    const double sum = double(at[u.ci[c]].im) + at[u.cj[c]].im;
+    rm[c] = sum == 0.0 ? 0.0 : 0.5 / sum;
   }
   const double lo = 1.0 - 2.0 * tol + double(tol) * tol, hi = 1.0 + 2.0 * tol + double(tol) * tol;
+  bool ok = false;
   for (int it = 0; it < kMaxShakeIterations; ++it) {
     int conv = 0;
     for (int c = 0; c < u.nc; ++c) {
       const int i = u.ci[c], j = u.cj[c];
-      const float x = rv[c].x + dp[i].x - dp[j].x, y = rv[c].y + dp[i].y - dp[j].y, z = rv[c].z + dp[i].z - dp[j].z;
-      const double l2 = double(x) * x + double(y) * y + double(z) * z;
+      const double x = rv[c][0] + q[i][0] - q[j][0], y = rv[c][1] + q[i][1] - q[j][1], z = rv[c][2] + q[i][2] - q[j][2];
+      const double l2 = x * x + y * y + z * z;
       const double d2 = double(u.dist[c]) * u.dist[c];
-      const float proj = x * rv[c].x + y * rv[c].y + z * rv[c].z;
-      delta[c] = proj == 0.f ? 0.f : rm[c] * float(d2 - l2) / proj;
+      const double proj = x * rv[c][0] + y * rv[c][1] + z * rv[c][2];
+      delta[c] = proj == 0.0 ? 0.0 : rm[c] * (d2 - l2) / proj;
       conv += (l2 >= lo * d2 && l2 <= hi * d2);
     }
-    if (conv == u.nc) return true;
+    if (conv == u.nc) { ok = true; break; }
     for (int c = 0; c < u.nc; ++c) {
       const int i = u.ci[c], j = u.cj[c];
-      const float dx = rv[c].x * delta[c], dy = rv[c].y * delta[c], dz = rv[c].z * delta[c];
-      dp[i].x += dx * at[i].im; dp[i].y += dy * at[i].im; dp[i].z += dz * at[i].im;
-      dp[j].x -= dx * at[j].im; dp[j].y -= dy * at[j].im; dp[j].z -= dz * at[j].im;
+      const double ii = at[i].im, jj = at[j].im;
+      for (int x = 0; x < 3; ++x) {
+        const double dr = rv[c][x] * delta[c];
+        q[i][x] += dr * ii;
+        q[j][x] -= dr * jj;
+      }
     }
   }
-  return false;
+  for (int k = 0; k < u.na; ++k) dp[k] = make_float3(float(q[k][0]), float(q[k][1]), float(q[k][2]));
+  return ok;
 }
 
 __device__ __forceinline__ long long displace(float wanted, float& left_over) {
@@ -261,124 +286,161 @@ __device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance)
   }
 }
 
+// One unit through the whole step.  NA is the atom count known at compile
+// time (3 for a SETTLE water, 1 for a free atom), so those units live in
+// registers; SHAKE clusters take the general path with NA = 8 and `na` atoms.
+template <int NA, int KIND>
+__device__ __forceinline__ void integrate_unit(const Dev& d, const SysDev& S, const UnitDev* up, long long step,
+                                               bool com, float4 vc, double* mom, bool& moved, bool& bad) {
+  const RunDev& R = d.run;
+  const int na = KIND == kUnitShake ? up->na : NA;
+  Atom at[NA];
+  int atom[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    if (k >= na) break;
+    const int a = up->atom[k];
+    atom[k] = a;
+    Atom& A = at[k];
+    A.x = d.px[a]; A.y = d.py[a]; A.z = d.pz[a];
+    A.vx = d.vx[a]; A.vy = d.vy[a]; A.vz = d.vz[a];
+    A.rx = d.rx[a]; A.ry = d.ry[a]; A.rz = d.rz[a];
+    A.im = d.invm[a];
+    const int gs = S.slot_off + d.rank[a];
+    A.fx = from_fixed(static_cast<long long>(d.fx[gs]));
+    A.fy = from_fixed(static_cast<long long>(d.fy[gs]));
+    A.fz = from_fixed(static_cast<long long>(d.fz[gs]));
+    d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;  // consumer clears
+    if (com && A.im > 0.f) { A.vx -= vc.x; A.vy -= vc.y; A.vz -= vc.z; }
+  }
+  const float dt = R.dt;
+  long long tx[NA], ty[NA], tz[NA];  // drift, 2^32 fixed point
+  float3 dp[NA];
+  if (R.integrator == 0) {
+    // ---- LFMiddle ----
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+      if (k >= na) break;
+      Atom& A = at[k];
+      if (A.im == 0.f) continue;
+      A.vx += dt * A.im * A.fx; A.vy += dt * A.im * A.fy; A.vz += dt * A.im * A.fz;
+    }
+    if (KIND == kUnitSettle) settle_velocities(at);
+    else if (KIND == kUnitShake) bad |= !rattle(at, *up, R.tolerance);
+    const float half = 0.5f * dt;
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+      if (k >= na) break;
+      Atom& A = at[k];
+      tx[k] = ty[k] = tz[k] = 0;
+      if (A.im == 0.f) continue;
+      float n0 = 0.f, n1 = 0.f, n2 = 0.f;
+      if (R.draw_noise) {
+        const unsigned p = static_cast<unsigned>(atom[k] - S.atom_off);
+        const uint2 key = make_uint2(R.seed, kThermostatDomain);
+        const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
+        const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
+        n0 = g0.x; n1 = g0.y; n2 = g1.x;
+      }
+      const float noise = R.noise_scale * sqrtf(R.kt * A.im);
+      float lo;
+      tx[k] = displace(A.vx * half + A.rx, lo);
+      A.vx = R.velocity_scale * A.vx + noise * n0;
+      tx[k] += displace(A.vx * half + lo, A.rx);
+      ty[k] = displace(A.vy * half + A.ry, lo);
+      A.vy = R.velocity_scale * A.vy + noise * n1;
+      ty[k] += displace(A.vy * half + lo, A.ry);
+      tz[k] = displace(A.vz * half + A.rz, lo);
+      A.vz = R.velocity_scale * A.vz + noise * n2;
+      tz[k] += displace(A.vz * half + lo, A.rz);
+    }
+  } else {
+    // ---- velocity Verlet (integrate.wgsl:91-132) ----
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+      if (k >= na) break;
+      Atom& A = at[k];
+      tx[k] = ty[k] = tz[k] = 0;
+      if (A.im == 0.f) continue;
+      A.vx += A.im * A.fx * dt; A.vy += A.im * A.fy * dt; A.vz += A.im * A.fz * dt;
+      tx[k] = displace(A.vx * dt + A.rx, A.rx);
+      ty[k] = displace(A.vy * dt + A.ry, A.ry);
+      tz[k] = displace(A.vz * dt + A.rz, A.rz);
+    }
+  }
+  // position constraints, relative to the start-of-step positions
+  long long cx[NA], cy[NA], cz[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    if (k >= na) break;
+    dp[k] = make_float3(from_fixed(tx[k]), from_fixed(ty[k]), from_fixed(tz[k]));
+  }
+  if (KIND == kUnitFree) {
+    cx[0] = tx[0]; cy[0] = ty[0]; cz[0] = tz[0];
+  } else {
+    if (KIND == kUnitSettle) settle_positions(at, dp, up->dist[0], up->dist[1]);
+    else bad |= !shake(at, dp, *up, R.tolerance);
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+      if (k >= na) break;
+      if (at[k].im == 0.f) { cx[k] = tx[k]; cy[k] = ty[k]; cz[k] = tz[k]; continue; }
+      cx[k] = to_fixed(dp[k].x); cy[k] = to_fixed(dp[k].y); cz[k] = to_fixed(dp[k].z);
+    }
+  }
+  const float idt = 1.f / dt;
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    if (k >= na) break;
+    Atom& A = at[k];
+    const int a = atom[k];
+    if (A.im != 0.f) {
+      if (R.integrator == 0) {
+        A.vx += idt * from_fixed(cx[k] - tx[k]);
+        A.vy += idt * from_fixed(cy[k] - ty[k]);
+        A.vz += idt * from_fixed(cz[k] - tz[k]);
+      } else {
+        A.vx = idt * from_fixed(cx[k]);
+        A.vy = idt * from_fixed(cy[k]);
+        A.vz = idt * from_fixed(cz[k]);
+      }
+      A.x += cx[k]; A.y += cy[k]; A.z += cz[k];
+      d.px[a] = A.x; d.py[a] = A.y; d.pz[a] = A.z;
+      d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
+      d.rx[a] = A.rx; d.ry[a] = A.ry; d.rz[a] = A.rz;
+      const double m = 1.0 / A.im;
+      mom[0] += m * A.vx; mom[1] += m * A.vy; mom[2] += m * A.vz;
+      bad |= !isfinite(A.vx + A.vy + A.vz);
+    } else if (com) {
+      d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
+    }
+    const float ex = from_fixed(A.x - d.refx[a]), ey = from_fixed(A.y - d.refy[a]), ez = from_fixed(A.z - d.refz[a]);
+    moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
+  }
+}
+
+// SHAKE clusters out of line, so their larger frame does not cost the SETTLE
+// and free-atom paths registers.
+__device__ __noinline__ void integrate_shake_unit(const Dev& d, const SysDev& S, const UnitDev* up, long long step,
+                                                  bool com, float4 vc, double* mom, bool& moved, bool& bad) {
+  integrate_unit<kMaxClusterAtoms, kUnitShake>(d, S, up, step, com, vc, mom, moved, bad);
+}
+
 __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   __shared__ double red[3][kThreads / 32];
   const int b = blockIdx.x;
   const int s = d.iblk_sys[b];
   const SysDev& S = d.sys[s];
-  const RunDev& R = d.run;
   const long long step = d.step[s];
   const bool com = S.com_freq > 0 && (step % S.com_freq) == 0;
   const float4 vc = com ? d.vcom[s] : make_float4(0.f, 0.f, 0.f, 0.f);
   double mom[3] = {0, 0, 0};
   bool moved = false, bad = false;
-
   if (threadIdx.x < d.iblk_nunit[b]) {
-    const UnitDev u = d.units[d.iblk_unit0[b] + threadIdx.x];
-    Atom at[kMaxClusterAtoms];
-    for (int k = 0; k < u.na; ++k) {
-      const int a = u.atom[k];
-      Atom& A = at[k];
-      A.x = d.px[a]; A.y = d.py[a]; A.z = d.pz[a];
-      A.vx = d.vx[a]; A.vy = d.vy[a]; A.vz = d.vz[a];
-      A.rx = d.rx[a]; A.ry = d.ry[a]; A.rz = d.rz[a];
-      A.im = d.invm[a];
-      const int gs = S.slot_off + d.rank[a];
-      A.fx = from_fixed(static_cast<long long>(d.fx[gs]));
-      A.fy = from_fixed(static_cast<long long>(d.fy[gs]));
-      A.fz = from_fixed(static_cast<long long>(d.fz[gs]));
-      d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;  // consumer clears
-      if (com && A.im > 0.f) { A.vx -= vc.x; A.vy -= vc.y; A.vz -= vc.z; }
-    }
-    const float dt = R.dt;
-    long long tx[kMaxClusterAtoms], ty[kMaxClusterAtoms], tz[kMaxClusterAtoms];  // drift, fixed
-    float3 dp[kMaxClusterAtoms];
-    if (R.integrator == 0) {
-      // ---- LFMiddle ----
-      for (int k = 0; k < u.na; ++k) {
-        Atom& A = at[k];
-        if (A.im == 0.f) continue;
-        A.vx += dt * A.im * A.fx; A.vy += dt * A.im * A.fy; A.vz += dt * A.im * A.fz;
-      }
-      if (u.kind == kUnitSettle) settle_velocities(at);
-      else if (u.kind == kUnitShake) bad |= !rattle(at, u, R.tolerance);
-      const float half = 0.5f * dt;
-      for (int k = 0; k < u.na; ++k) {
-        Atom& A = at[k];
-        tx[k] = ty[k] = tz[k] = 0;
-        if (A.im == 0.f) continue;
-        float n0 = 0.f, n1 = 0.f, n2 = 0.f;
-        if (R.draw_noise) {
-          const unsigned p = static_cast<unsigned>(u.atom[k] - S.atom_off);
-          const uint2 key = make_uint2(R.seed, kThermostatDomain);
-          const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
-          const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
-          n0 = g0.x; n1 = g0.y; n2 = g1.x;
-        }
-        const float noise = R.noise_scale * sqrtf(R.kt * A.im);
-        float lo;
-        tx[k] = displace(A.vx * half + A.rx, lo);
-        A.vx = R.velocity_scale * A.vx + noise * n0;
-        tx[k] += displace(A.vx * half + lo, A.rx);
-        ty[k] = displace(A.vy * half + A.ry, lo);
-        A.vy = R.velocity_scale * A.vy + noise * n1;
-        ty[k] += displace(A.vy * half + lo, A.ry);
-        tz[k] = displace(A.vz * half + A.rz, lo);
-        A.vz = R.velocity_scale * A.vz + noise * n2;
-        tz[k] += displace(A.vz * half + lo, A.rz);
-      }
-    } else {
-      // ---- velocity Verlet (integrate.wgsl:91-132) ----
-      for (int k = 0; k < u.na; ++k) {
-        Atom& A = at[k];
-        tx[k] = ty[k] = tz[k] = 0;
-        if (A.im == 0.f) continue;
-        A.vx += A.im * A.fx * dt; A.vy += A.im * A.fy * dt; A.vz += A.im * A.fz * dt;
-        tx[k] = displace(A.vx * dt + A.rx, A.rx);
-        ty[k] = displace(A.vy * dt + A.ry, A.ry);
-        tz[k] = displace(A.vz * dt + A.rz, A.rz);
-      }
-    }
-    // position constraints, relative to the start-of-step positions
-    for (int k = 0; k < u.na; ++k) dp[k] = make_float3(from_fixed(tx[k]), from_fixed(ty[k]), from_fixed(tz[k]));
-    long long cx[kMaxClusterAtoms], cy[kMaxClusterAtoms], cz[kMaxClusterAtoms];
-    if (u.kind == kUnitFree) {
-      cx[0] = tx[0]; cy[0] = ty[0]; cz[0] = tz[0];
-    } else {
-      if (u.kind == kUnitSettle) settle_positions(at, dp, u.dist[0], u.dist[1]);
-      else bad |= !shake(at, dp, u, R.tolerance);
-      for (int k = 0; k < u.na; ++k) {
-        if (at[k].im == 0.f) { cx[k] = tx[k]; cy[k] = ty[k]; cz[k] = tz[k]; continue; }
-        cx[k] = to_fixed(dp[k].x); cy[k] = to_fixed(dp[k].y); cz[k] = to_fixed(dp[k].z);
-      }
-    }
-    const float idt = 1.f / dt;
-    for (int k = 0; k < u.na; ++k) {
-      Atom& A = at[k];
-      const int a = u.atom[k];
-      if (A.im != 0.f) {
-        if (R.integrator == 0) {
-          A.vx += idt * from_fixed(cx[k] - tx[k]);
-          A.vy += idt * from_fixed(cy[k] - ty[k]);
-          A.vz += idt * from_fixed(cz[k] - tz[k]);
-        } else {
-          A.vx = idt * from_fixed(cx[k]);
-          A.vy = idt * from_fixed(cy[k]);
-          A.vz = idt * from_fixed(cz[k]);
-        }
-        A.x += cx[k]; A.y += cy[k]; A.z += cz[k];
-        d.px[a] = A.x; d.py[a] = A.y; d.pz[a] = A.z;
-        d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
-        d.rx[a] = A.rx; d.ry[a] = A.ry; d.rz[a] = A.rz;
-        const double m = 1.0 / A.im;
-        mom[0] += m * A.vx; mom[1] += m * A.vy; mom[2] += m * A.vz;
-        bad |= !isfinite(A.vx + A.vy + A.vz);
-      } else if (com) {
-        d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
-      }
-      const float ex = from_fixed(A.x - d.refx[a]), ey = from_fixed(A.y - d.refy[a]), ez = from_fixed(A.z - d.refz[a]);
-      moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
-    }
+    const UnitDev* up = d.units + d.iblk_unit0[b] + threadIdx.x;
+    const int kind = up->kind;
+    if (kind == kUnitSettle) integrate_unit<3, kUnitSettle>(d, S, up, step, com, vc, mom, moved, bad);
+    else if (kind == kUnitFree) integrate_unit<1, kUnitFree>(d, S, up, step, com, vc, mom, moved, bad);
+    else integrate_shake_unit(d, S, up, step, com, vc, mom, moved, bad);
   }
   if (moved) atomicOr(&d.rebuild_flag[s], 1);
   if (bad) atomicAdd(&d.shake_failures[s], 1);

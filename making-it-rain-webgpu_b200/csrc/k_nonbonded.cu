@@ -58,7 +58,7 @@ template <bool ENERGY, bool TRICLINIC>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
                                            unsigned int mask, int lane, float& fix, float& fiy,
                                            float& fiz, float& fjx, float& fjy, float& fjz,
-                                           float& ecoul, float& elj) {
+                                           float& ecoul, float& elj, int& pairs) {
   const float alpha = S.alpha, a2sp = S.alpha_2_sqrtpi, cut2 = S.cut2, inv = S.pc_inv;
 #pragma unroll 4
   for (int k = 0; k < 32; ++k) {
@@ -92,6 +92,7 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
       if (ENERGY) {
         ecoul += coul;
         elj += 4.0f * eps * (s12 - s6);
+        pairs += 1;
       }
     }
     const int src = (lane + 1) & 31;
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
 
   long long aix = 0, aiy = 0, aiz = 0;
   int cur_row = -1;
-  long long ecoul64 = 0, elj64 = 0;
+  long long ecoul64 = 0, elj64 = 0, pairs64 = 0;
 
   auto flush_row = [&]() {
     if (cur_row >= 0) {
@@ -136,13 +137,14 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   };
   auto flush_energy = [&](int sys) {
     if (ENERGY) {
-      const long long c = warp_sum64(ecoul64), l = warp_sum64(elj64);
+      const long long c = warp_sum64(ecoul64), l = warp_sum64(elj64), p = warp_sum64(pairs64);
       if (lane == 0) {
         const int base = d.sys[sys].energy_base;
         add_fixed64(&d.energy[base + kECoulomb], c);
         add_fixed64(&d.energy[base + kELj], l);
+        add_fixed64(&d.energy[base + kEPairs], p);
       }
-      ecoul64 = elj64 = 0;
+      ecoul64 = elj64 = pairs64 = 0;
     }
   };
 
@@ -165,10 +167,11 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
     const float4 qj = d.prm[gj];
     const unsigned int mask = d.masks[ti * 32 + lane];
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
+    int np = 0;
     if (S.triclinic)
-      tile_pairs<ENERGY, true>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el);
+      tile_pairs<ENERGY, true>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np);
     else
-      tile_pairs<ENERGY, false>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el);
+      tile_pairs<ENERGY, false>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np);
     aix += to_fixed(fix);
     aiy += to_fixed(fiy);
     aiz += to_fixed(fiz);
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
     if (ENERGY) {
       ecoul64 += to_fixed(ec);
       elj64 += to_fixed(el);
+      pairs64 += np;
     }
   }
   flush_row();

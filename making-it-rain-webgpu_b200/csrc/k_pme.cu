@@ -435,16 +435,30 @@ void set_pme_smem(int z, int y, int x) {
   cudaFuncSetAttribute(k_fft_x_convolve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
 }
 
-void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
+void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
   k_spread<<<grid_blocks(d.n_slots), kThreads, 0, st>>>(d);
+}
+
+void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {
+  if (d.n_fft_z == 0) return;
   k_fft_z_forward<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
   k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, -1);
   if (energy) k_fft_x_convolve<true><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
   else k_fft_x_convolve<false><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
   k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, +1);
   k_fft_z_inverse<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+}
+
+void launch_pme_gather(const Dev& d, cudaStream_t st) {
+  if (d.n_fft_z == 0) return;
   k_gather<<<grid_blocks(d.n_slots), kThreads, 0, st>>>(d);
+}
+
+void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
+  launch_pme_spread(d, st);
+  launch_pme_fft(d, energy, st);
+  launch_pme_gather(d, st);
 }
 
 }  // namespace mdb

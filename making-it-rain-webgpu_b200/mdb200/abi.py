@@ -151,6 +151,7 @@ class Energies(C.Structure):
         ("temperature", C.c_double),
         ("degrees_of_freedom", C.c_double),
         ("virial", C.c_double * 9),
+        ("pairs_within_cutoff", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -167,6 +168,32 @@ class BarostatStats(C.Structure):
         ("screened", C.c_int64),
         ("exact_evaluations", C.c_int64),
     ]
+
+
+class Profile(C.Structure):
+    """`mdb_profile`."""
+
+    _fields_ = [
+        ("launches_per_step", C.c_int32),
+        ("repeats", C.c_int32),
+        ("ms_step", C.c_double),
+        ("ms_list_check", C.c_double),
+        ("ms_list_rebuild", C.c_double),
+        ("ms_nonbonded", C.c_double),
+        ("ms_listed", C.c_double),
+        ("ms_pme", C.c_double),
+        ("ms_pme_spread", C.c_double),
+        ("ms_pme_fft", C.c_double),
+        ("ms_pme_gather", C.c_double),
+        ("ms_integrate", C.c_double),
+        ("pairs_within_cutoff", C.c_int64),
+        ("tiles", C.c_int64),
+        ("atoms", C.c_int64),
+        ("mesh_points", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class NeighbourStats(C.Structure):
@@ -210,6 +237,7 @@ EXPORTS = {
     "mdb_get_barostat_stats": (C.c_int, [_E, C.c_int32, C.POINTER(BarostatStats)]),
     "mdb_get_neighbour_stats": (C.c_int, [_E, C.c_int32, C.POINTER(NeighbourStats)]),
     "mdb_memory_report": (C.c_int, [_E, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
+    "mdb_profile_step": (C.c_int, [_E, C.c_int32, C.POINTER(Profile)]),
 }
 
 _library = None

@@ -258,6 +258,12 @@ class StepLoop:
         return {"rebuilds": s.rebuilds, "tiles": s.tiles, "tileCapacity": s.tile_capacity,
                 "blocks": s.blocks, "overflowed": bool(s.overflowed), "skin": s.skin}
 
+    def profile_step(self, repeats: int = 20) -> dict:
+        """`StepLoop.profileStep`, loop.ts:705: device ms per stage.  Advances the system."""
+        p = abi.Profile()
+        self._check(self._lib.mdb_profile_step(self._handle, int(repeats), C.byref(p)))
+        return p.as_dict()
+
     def memory_report(self) -> dict:
         buf = C.create_string_buffer(1 << 16)
         total = C.c_int64()

@@ -69,25 +69,25 @@ def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
 def _lattice_sites(box: np.ndarray, count: int, rng: np.random.Generator, exclude=None, min_gap=0.0):
     """`count` sites on a uniform fractional lattice of the cell, chosen at random."""
     volume = abs(np.linalg.det(box))
-    per_axis = max(1, math.ceil((count * 1.0) ** (1 / 3) * 1.0))
-    while per_axis**3 < count:
+    per_axis = max(1, math.ceil(count ** (1 / 3)))
+    inv = np.linalg.inv(box)
+    for _ in range(64):
+        g = (np.arange(per_axis) + 0.5) / per_axis
+        frac = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+        jitter = rng.uniform(-0.05, 0.05, size=frac.shape) / per_axis
+        cart = (frac + jitter) @ box
+        if exclude is not None and len(exclude):
+            keep = np.ones(len(cart), dtype=bool)
+            for p in exclude:
+                f = (cart - p) @ inv
+                f -= np.round(f)
+                keep &= np.linalg.norm(f @ box, axis=1) > min_gap
+            cart = cart[keep]
+        if len(cart) >= count:
+            break
         per_axis += 1
-    g = (np.arange(per_axis) + 0.5) / per_axis
-    frac = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-    jitter = rng.uniform(-0.05, 0.05, size=frac.shape) / per_axis
-    cart = (frac + jitter) @ box
-    if exclude is not None and len(exclude):
-        keep = np.ones(len(cart), dtype=bool)
-        inv = np.linalg.inv(box)
-        for p in exclude:
-            d = cart - p
-            f = d @ inv
-            f -= np.round(f)
-            dist = np.linalg.norm(f @ box, axis=1)
-            keep &= dist > min_gap
-        cart = cart[keep]
-    if len(cart) < count:
-        raise ValueError(f"only {len(cart)} free lattice sites for {count} molecules (volume {volume:.2f} nm^3)")
+    else:
+        raise ValueError(f"no lattice leaves {count} free sites (volume {volume:.2f} nm^3)")
     pick = np.sort(rng.choice(len(cart), size=count, replace=False))
     return cart[pick]
 
@@ -209,3 +209,37 @@ def config_water_2652(seed: int = 1):
 
 def config_water_cube(width: float, seed: int = 1, grid=(0, 0, 0), **kw):
     return water_box(width=width, seed=seed, grid=grid, **kw)
+
+
+def ions_for(volume_nm3: float, molar: float = 0.15) -> int:
+    """Ion pairs for a salt concentration: c * V * N_A, rounded."""
+    return int(round(molar * volume_nm3 * 1e-24 * 6.02214076e23))
+
+
+def solvated(solute_system: System, solute_positions, width: float, shape: str = "cube", seed: int = 1,
+             grid=(0, 0, 0), molar: float = 0.15, **kw):
+    """A solute centred in a TIP3P cell with NaCl at `molar`, neutralised."""
+    from .system import Nonbonded  # noqa: F401  (kept for symmetry with water_box)
+
+    box = box_vectors(shape, width)
+    centre = 0.5 * box.sum(axis=0)
+    pos = np.asarray(solute_positions, dtype=np.float64)
+    pos = pos - pos.mean(axis=0) + centre
+    volume = abs(np.linalg.det(box))
+    pairs = ions_for(volume, molar)
+    net = float(np.round(solute_system.nonbonded.charge.sum()))
+    n_na = pairs + max(0, int(-net))
+    n_cl = pairs + max(0, int(net))
+    solute_volume = 0.02 * solute_system.particle_count
+    n_waters = int(round(WATER_DENSITY_PER_NM3 * (volume - solute_volume))) - (n_na + n_cl)
+    return water_box(n_waters=n_waters, width=width, shape=shape, seed=seed, n_na=n_na, n_cl=n_cl, grid=grid,
+                     solute=(solute_system, pos), **kw)
+
+
+def config_peptide_12k(seed: int = 1):
+    """Ala20 alpha-helix (phi -57, psi -47) with ACE/NME caps, ff14SB, HBond
+    constraints, in a 5.0 nm TIP3P cube with 0.15 M NaCl; mesh 50^3 (0.1 nm)."""
+    from . import peptide
+
+    solute, positions = peptide.helix(["ALA"] * 20)
+    return solvated(solute, positions, width=5.0, seed=seed, grid=(50, 50, 50))

@@ -1,0 +1,278 @@
+// addon.cc -- Node-API binding of libmdb200 for the TypeScript StepLoop shim
+// (../ts/step-loop.ts).  Written against Node-API's documented C interface
+// (node_api.h, NAPI_VERSION 8).  Neither Node nor its headers exist on the
+// build or GPU machines of this project, so this file is not compiled there;
+// a maintainer builds it with node-gyp next to libmdb200.so.
+//
+// Every method is synchronous: the engine returns when the device work it
+// queued has finished (loop.ts awaits `onSubmittedWorkDone` the same way).
+// Errors become JS exceptions whose `name` is the reference's error class
+// (UnsupportedForce, CutoffTooLargeForBox, ClusterTooLarge, NotSmooth, ...).
+#include <node_api.h>
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mdb.h"
+
+namespace {
+
+const char* error_name(int status) {
+  switch (status) {
+    case MDB_ERR_UNSUPPORTED_FORCE: return "UnsupportedForce";
+    case MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX: return "CutoffTooLargeForBox";
+    case MDB_ERR_CLUSTER_TOO_LARGE: return "ClusterTooLarge";
+    case MDB_ERR_NOT_SMOOTH: return "NotSmooth";
+    case MDB_ERR_RANGE: return "RangeError";
+    default: return "Error";
+  }
+}
+
+napi_value throw_status(napi_env env, int status, mdb_engine* e) {
+  std::string msg = e ? mdb_last_error(e) : mdb_status_string(status);
+  napi_value message, error, name;
+  napi_create_string_utf8(env, msg.c_str(), NAPI_AUTO_LENGTH, &message);
+  napi_create_error(env, nullptr, message, &error);
+  napi_create_string_utf8(env, error_name(status), NAPI_AUTO_LENGTH, &name);
+  napi_set_named_property(env, error, "name", name);
+  napi_throw(env, error);
+  return nullptr;
+}
+
+mdb_engine* engine_of(napi_env env, napi_value v) {
+  void* p = nullptr;
+  napi_get_value_external(env, v, &p);
+  return static_cast<mdb_engine*>(p);
+}
+
+template <typename T>
+T* typed_array(napi_env env, napi_value v, size_t* length) {
+  napi_typedarray_type type;
+  void* data = nullptr;
+  napi_value buffer;
+  size_t offset = 0;
+  napi_get_typedarray_info(env, v, &type, length, &data, &buffer, &offset);
+  return static_cast<T*>(data);
+}
+
+double number(napi_env env, napi_value obj, const char* key, double fallback) {
+  bool has = false;
+  napi_has_named_property(env, obj, key, &has);
+  if (!has) return fallback;
+  napi_value v;
+  napi_get_named_property(env, obj, key, &v);
+  double out = fallback;
+  napi_get_value_double(env, v, &out);
+  return out;
+}
+
+napi_value property(napi_env env, napi_value obj, const char* key) {
+  napi_value v = nullptr;
+  napi_get_named_property(env, obj, key, &v);
+  return v;
+}
+
+// OpenMMSystem (src/engine/system.ts:161) -> mdb_system_desc.  The typed
+// arrays are borrowed for the duration of the create call only.
+bool fill_system(napi_env env, napi_value sys, mdb_system_desc* d, std::vector<double>& box) {
+  std::memset(d, 0, sizeof(*d));
+  size_t n = 0;
+  d->masses = typed_array<double>(env, property(env, sys, "masses"), &n);
+  d->n_particles = int32_t(n);
+  napi_value bv = property(env, sys, "boxVectors");
+  for (uint32_t r = 0; r < 3; ++r) {
+    napi_value row;
+    napi_get_element(env, bv, r, &row);
+    for (uint32_t c = 0; c < 3; ++c) {
+      napi_value x;
+      napi_get_element(env, row, c, &x);
+      napi_get_value_double(env, x, &d->box[r * 3 + c]);
+    }
+  }
+  size_t nc = 0;
+  d->constraint_p1 = typed_array<int32_t>(env, property(env, sys, "constraintP1"), &nc);
+  d->constraint_p2 = typed_array<int32_t>(env, property(env, sys, "constraintP2"), &nc);
+  d->constraint_distance = typed_array<double>(env, property(env, sys, "constraintDistance"), &nc);
+  d->n_constraints = int32_t(nc);
+  napi_value forces = property(env, sys, "forces");
+  uint32_t count = 0;
+  napi_get_array_length(env, forces, &count);
+  for (uint32_t k = 0; k < count; ++k) {
+    napi_value f;
+    napi_get_element(env, forces, k, &f);
+    char type[64] = {0};
+    size_t len = 0;
+    napi_get_value_string_utf8(env, property(env, f, "type"), type, sizeof(type), &len);
+    size_t m = 0;
+    if (!std::strcmp(type, "NonbondedForce")) {
+      d->has_nonbonded = 1;
+      d->cutoff = number(env, f, "cutoff", 1.0);
+      d->ewald_tolerance = number(env, f, "ewaldTolerance", 5e-4);
+      d->alpha = number(env, f, "alpha", 0);
+      d->use_dispersion_correction = number(env, f, "useDispersionCorrection", 1) != 0;
+      d->charge = typed_array<double>(env, property(env, f, "charge"), &m);
+      d->sigma = typed_array<double>(env, property(env, f, "sigma"), &m);
+      d->epsilon = typed_array<double>(env, property(env, f, "epsilon"), &m);
+      d->exception_p1 = typed_array<int32_t>(env, property(env, f, "exceptionP1"), &m);
+      d->n_exceptions = int32_t(m);
+      d->exception_p2 = typed_array<int32_t>(env, property(env, f, "exceptionP2"), &m);
+      d->exception_charge_prod = typed_array<double>(env, property(env, f, "exceptionChargeProd"), &m);
+      d->exception_sigma = typed_array<double>(env, property(env, f, "exceptionSigma"), &m);
+      d->exception_epsilon = typed_array<double>(env, property(env, f, "exceptionEpsilon"), &m);
+    } else if (!std::strcmp(type, "HarmonicBondForce")) {
+      d->bond_p1 = typed_array<int32_t>(env, property(env, f, "p1"), &m);
+      d->n_bonds = int32_t(m);
+      d->bond_p2 = typed_array<int32_t>(env, property(env, f, "p2"), &m);
+      d->bond_length = typed_array<double>(env, property(env, f, "length"), &m);
+      d->bond_k = typed_array<double>(env, property(env, f, "k"), &m);
+    } else if (!std::strcmp(type, "HarmonicAngleForce")) {
+      d->angle_p1 = typed_array<int32_t>(env, property(env, f, "p1"), &m);
+      d->n_angles = int32_t(m);
+      d->angle_p2 = typed_array<int32_t>(env, property(env, f, "p2"), &m);
+      d->angle_p3 = typed_array<int32_t>(env, property(env, f, "p3"), &m);
+      d->angle_theta = typed_array<double>(env, property(env, f, "angle"), &m);
+      d->angle_k = typed_array<double>(env, property(env, f, "k"), &m);
+    } else if (!std::strcmp(type, "PeriodicTorsionForce")) {
+      d->torsion_p1 = typed_array<int32_t>(env, property(env, f, "p1"), &m);
+      d->n_torsions = int32_t(m);
+      d->torsion_p2 = typed_array<int32_t>(env, property(env, f, "p2"), &m);
+      d->torsion_p3 = typed_array<int32_t>(env, property(env, f, "p3"), &m);
+      d->torsion_p4 = typed_array<int32_t>(env, property(env, f, "p4"), &m);
+      d->torsion_periodicity = typed_array<int32_t>(env, property(env, f, "periodicity"), &m);
+      d->torsion_phase = typed_array<double>(env, property(env, f, "phase"), &m);
+      d->torsion_k = typed_array<double>(env, property(env, f, "k"), &m);
+    } else if (!std::strcmp(type, "CMMotionRemover")) {
+      d->com_frequency = int32_t(number(env, f, "frequency", 1));
+    } else if (!std::strcmp(type, "MonteCarloBarostat")) {
+      d->barostat_frequency = int32_t(number(env, f, "frequency", 25));
+      d->barostat_pressure = number(env, f, "defaultPressure", 1);
+      d->barostat_temperature = number(env, f, "defaultTemperature", 300);
+    }
+  }
+  (void)box;
+  return d->n_particles > 0;
+}
+
+napi_value Create(napi_env env, napi_callback_info info) {
+  size_t argc = 3;
+  napi_value argv[3];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_system_desc sys;
+  std::vector<double> box;
+  if (!fill_system(env, argv[0], &sys, box)) return throw_status(env, MDB_ERR_INVALID_ARGUMENT, nullptr);
+  mdb_state_desc st;
+  std::memset(&st, 0, sizeof(st));
+  size_t n = 0;
+  st.positions = typed_array<double>(env, property(env, argv[1], "positions"), &n);
+  bool has_v = false;
+  napi_has_named_property(env, argv[1], "velocities", &has_v);
+  if (has_v) st.velocities = typed_array<double>(env, property(env, argv[1], "velocities"), &n);
+  std::memcpy(st.box, sys.box, sizeof(st.box));
+  mdb_run_options o;
+  std::memset(&o, 0, sizeof(o));
+  o.time_step = number(env, argv[2], "timeStep", 0.002);
+  o.temperature = number(env, argv[2], "temperature", 300);
+  o.friction = number(env, argv[2], "friction", 1);
+  o.constraint_tolerance = number(env, argv[2], "constraintTolerance", 1e-6);
+  o.seed = uint32_t(number(env, argv[2], "seed", 0));
+  o.verlet_skin = number(env, argv[2], "verletSkin", -1);
+  o.max_batch = int32_t(number(env, argv[2], "maxBatch", 100));
+  mdb_engine* e = nullptr;
+  const int status = mdb_create(&sys, &st, &o, &e);
+  if (status != MDB_OK) {
+    napi_value r = throw_status(env, status, e);
+    if (e) mdb_destroy(e, nullptr);
+    return r;
+  }
+  napi_value handle;
+  napi_create_external(env, e, nullptr, nullptr, &handle);
+  return handle;
+}
+
+napi_value Run(napi_env env, napi_callback_info info) {
+  size_t argc = 2;
+  napi_value argv[2];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  int64_t steps = 0;
+  napi_get_value_int64(env, argv[1], &steps);
+  const int status = mdb_run(e, steps);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  return nullptr;
+}
+
+napi_value CopyOut(napi_env env, napi_callback_info info, int (*fn)(mdb_engine*, int32_t, double*)) {
+  size_t argc = 2;
+  napi_value argv[2];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  size_t n = 0;
+  double* out = typed_array<double>(env, argv[1], &n);
+  const int status = fn(e, 0, out);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  return nullptr;
+}
+
+napi_value Positions(napi_env env, napi_callback_info info) { return CopyOut(env, info, mdb_get_positions); }
+napi_value Velocities(napi_env env, napi_callback_info info) { return CopyOut(env, info, mdb_get_velocities); }
+
+napi_value Evaluate(napi_env env, napi_callback_info info) {
+  size_t argc = 2;
+  napi_value argv[2];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  napi_valuetype t;
+  napi_typeof(env, argv[1], &t);
+  size_t n = 0;
+  double* forces = t == napi_null ? nullptr : typed_array<double>(env, argv[1], &n);
+  mdb_energies en;
+  const int status = mdb_evaluate(e, 0, forces, &en);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_value obj;
+  napi_create_object(env, &obj);
+  auto put = [&](const char* k, double v) {
+    napi_value x;
+    napi_create_double(env, v, &x);
+    napi_set_named_property(env, obj, k, x);
+  };
+  put("potential", en.potential);
+  put("kinetic", en.kinetic);
+  put("temperature", en.temperature);
+  put("directGroup", en.direct_group);
+  put("reciprocalGroup", en.reciprocal_group);
+  put("HarmonicBondForce", en.bond);
+  put("HarmonicAngleForce", en.angle);
+  put("PeriodicTorsionForce", en.torsion);
+  return obj;
+}
+
+napi_value Destroy(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  int64_t leaked = 0;
+  mdb_destroy(engine_of(env, argv[0]), &leaked);
+  napi_value obj, v;
+  napi_create_object(env, &obj);
+  napi_create_int64(env, leaked, &v);
+  napi_set_named_property(env, obj, "leaked", v);
+  return obj;
+}
+
+napi_value Init(napi_env env, napi_value exports) {
+  const napi_property_descriptor props[] = {
+      {"create", nullptr, Create, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"run", nullptr, Run, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"positions", nullptr, Positions, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"velocities", nullptr, Velocities, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"evaluate", nullptr, Evaluate, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"destroy", nullptr, Destroy, nullptr, nullptr, nullptr, napi_default, nullptr},
+  };
+  napi_define_properties(env, exports, sizeof(props) / sizeof(props[0]), props);
+  return exports;
+}
+
+}  // namespace
+
+NAPI_MODULE(NODE_GYP_MODULE_NAME, Init)

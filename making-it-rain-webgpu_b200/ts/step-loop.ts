@@ -1,0 +1,160 @@
+/**
+ * StepLoop over libmdb200 -- the TypeScript surface of src/gpu/loop.ts,
+ * backed by the B200 engine through the Node-API addon in ../napi/addon.cc.
+ *
+ * Same public members, same units, same named errors as the reference's
+ * `StepLoop` (src/gpu/loop.ts:208-1116), so `LoopEngine` (src/gpu/engine.ts)
+ * and `runProtocol` (src/engine/protocol.ts) can take it unchanged.  Every call
+ * is synchronous in the addon; the Promises resolve after it returns.
+ *
+ * Not verified on this machine: there is no Node runtime and no node_api.h
+ * here or on the GPU box.  The Python mirror (mdb200/steploop.py) exercises
+ * the same C ABI in the tests.
+ */
+
+import type { OpenMMState } from "../../src/engine/state.js";
+import type { OpenMMSystem } from "../../src/engine/system.js";
+import type { RunOptions, Report } from "../../src/gpu/loop.js";
+
+// eslint-disable-next-line @typescript-eslint/no-require-imports
+const addon = require("./build/Release/mdb200.node") as MdbAddon;
+
+type Vec3 = [number, number, number];
+
+interface Energies {
+  readonly potential: number;
+  readonly kinetic: number;
+  readonly temperature: number;
+  readonly directGroup: number;
+  readonly reciprocalGroup: number;
+  readonly [group: string]: number;
+}
+
+interface MdbAddon {
+  create(system: OpenMMSystem, state: OpenMMState, options: RunOptions): unknown;
+  run(handle: unknown, steps: number): void;
+  evaluate(handle: unknown, forces: Float64Array | null): Energies;
+  potential(handle: unknown, positions: Float64Array, forces: Float64Array): Energies;
+  positions(handle: unknown, out: Float64Array): void;
+  velocities(handle: unknown, out: Float64Array): void;
+  setPositions(handle: unknown, positions: Float64Array): void;
+  setVelocities(handle: unknown, velocities: Float64Array): void;
+  setBox(handle: unknown, vectors: Float64Array): void;
+  box(handle: unknown): Float64Array;
+  mesh(handle: unknown): Int32Array;
+  setStep(handle: unknown, step: number): void;
+  step(handle: unknown): number;
+  barostat(handle: unknown): { attempts: number; accepted: number; volumeScale: number };
+  neighbours(handle: unknown): { rebuilds: number; tiles: number; overflowed: boolean };
+  destroy(handle: unknown): { leaked: number };
+}
+
+export class StepLoop {
+  private constructor(
+    private readonly handle: unknown,
+    private readonly system: OpenMMSystem,
+    private readonly options: RunOptions,
+  ) {}
+
+  /** `StepLoop.fromParsed`, loop.ts:278.  The GPU device is chosen by `options`. */
+  static async fromParsed(
+    _device: unknown,
+    system: OpenMMSystem,
+    state: OpenMMState,
+    options: RunOptions,
+  ): Promise<StepLoop> {
+    return new StepLoop(addon.create(system, state, options), system, options);
+  }
+
+  get steps(): number {
+    return addon.step(this.handle);
+  }
+
+  advanceStepCount(step: number): void {
+    if (!Number.isInteger(step) || step < 0) {
+      throw new Error(`a step count must be a non-negative integer, got ${step}`);
+    }
+    addon.setStep(this.handle, step);
+  }
+
+  /** `StepLoop.run(n)`, loop.ts:651 -- barostat attempts included. */
+  async run(steps: number): Promise<void> {
+    if (steps > 0) addon.run(this.handle, steps);
+  }
+
+  async report(): Promise<Report> {
+    const e = addon.evaluate(this.handle, null);
+    const step = this.steps;
+    return {
+      step,
+      time: step * this.options.timeStep,
+      potentialEnergy: e.potential,
+      kineticEnergy: e.kinetic,
+      shiftedKineticEnergy: e.kinetic,
+      totalEnergy: e.potential + e.kinetic,
+      temperature: e.temperature,
+    };
+  }
+
+  async potential(positions: Float64Array): Promise<{ energy: number; forces: Float64Array }> {
+    const forces = new Float64Array(this.system.particleCount * 3);
+    const e = addon.potential(this.handle, positions, forces);
+    return { energy: e.potential, forces };
+  }
+
+  async positions(): Promise<Float64Array> {
+    const out = new Float64Array(this.system.particleCount * 3);
+    addon.positions(this.handle, out);
+    return out;
+  }
+
+  async velocities(): Promise<Float64Array> {
+    const out = new Float64Array(this.system.particleCount * 3);
+    addon.velocities(this.handle, out);
+    return out;
+  }
+
+  setPositions(positions: Float64Array): void {
+    if (positions.length !== this.system.particleCount * 3) {
+      throw new Error(`expected ${this.system.particleCount * 3} coordinates, got ${positions.length}`);
+    }
+    addon.setPositions(this.handle, positions);
+  }
+
+  setVelocities(velocities: Float64Array): void {
+    if (velocities.length !== this.system.particleCount * 3) {
+      throw new Error(`expected ${this.system.particleCount * 3} velocities, got ${velocities.length}`);
+    }
+    addon.setVelocities(this.handle, velocities);
+  }
+
+  setBox(vectors: readonly [Vec3, Vec3, Vec3]): void {
+    addon.setBox(this.handle, Float64Array.from(vectors.flat()));
+  }
+
+  get mesh(): Vec3 {
+    const m = addon.mesh(this.handle);
+    return [m[0] as number, m[1] as number, m[2] as number];
+  }
+
+  get boxVectorsNow(): [Vec3, Vec3, Vec3] {
+    const b = addon.box(this.handle);
+    return [
+      [b[0] as number, b[1] as number, b[2] as number],
+      [b[3] as number, b[4] as number, b[5] as number],
+      [b[6] as number, b[7] as number, b[8] as number],
+    ];
+  }
+
+  get barostatStatistics() {
+    return addon.barostat(this.handle);
+  }
+
+  async verletFlags() {
+    return addon.neighbours(this.handle);
+  }
+
+  destroy(): { leaked: number } {
+    return addon.destroy(this.handle);
+  }
+}

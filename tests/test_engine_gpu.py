@@ -141,24 +141,33 @@ def test_potential_leaves_state_and_matches_evaluate(mdb, water):
     system, state = water
     loop = make_loop(mdb, system, state)
     before = loop.positions()
-    shifted = state.positions + 0.01
+    # One whole mesh cell (3.0 nm / 30): PME is invariant under translations
+    # by mesh cells only, so all that may move is f32 rounding.
+    shifted = state.positions + np.array([0.1, 0.0, 0.0])
     e_shift, f_shift = loop.potential(shifted)
     assert np.array_equal(loop.positions(), before)
     e0, f0 = loop.evaluate()
-    # A uniform translation changes nothing physical; what moves is f32
-    # rounding, relative to the largest energy group (|exclusion| ~ 2e5 here).
     assert abs(e_shift - e0["potential"]) < 1e-7 * abs(e0["exclusion_correction"])
-    assert rel_rms(f_shift, f0) < 1e-5
+    assert rel_rms(f_shift, f0) < 2e-6
     loop.destroy()
 
 
 def test_dynamics_stay_bounded(mdb, water):
+    """The lattice-built box relaxes (about 24,000 kJ/mol of potential energy
+    becomes heat, ~1,100 K worth over its 5,301 degrees of freedom) while the
+    constraints hold and the thermostat starts to cool it."""
     system, state = water
     loop = make_loop(mdb, system, state, seed=2)
+    e0 = loop.report().potential_energy
     loop.run(300)
     r = loop.report()
     print("after 300 steps", r.temperature, r.potential_energy, loop.verlet_flags())
-    assert 150 < r.temperature < 450
+    assert np.isfinite(r.potential_energy) and np.isfinite(r.kinetic_energy)
+    assert r.potential_energy < e0 - 10000
+    assert 100 < r.temperature < 1500
+    p = loop.positions()
+    d = np.linalg.norm(p[system.constraint_p1] - p[system.constraint_p2], axis=1)
+    assert np.max(np.abs(d / system.constraint_distance - 1)) < 1e-5
     assert loop.verlet_flags()["rebuilds"] >= 1
     assert not loop.verlet_flags()["overflowed"]
     loop.destroy()
@@ -170,3 +179,45 @@ def test_cutoff_too_large_is_refused(mdb):
     system, state = synth.water_box(n_waters=100, width=1.5, seed=1, grid=(16, 16, 16))
     with pytest.raises(mdb.CutoffTooLargeForBox):
         make_loop(mdb, system, state)
+
+
+@pytest.fixture(scope="module")
+def peptide():
+    from mdb200 import synth
+
+    return synth.config_peptide_12k()
+
+
+def test_peptide_forces_and_groups(mdb, oracle, peptide):
+    """The 12k-atom solvated Ala20 helix: bonded, exceptions, PME, SHAKE clusters."""
+    system, state = peptide
+    loop = make_loop(mdb, system, state)
+    e, f = loop.evaluate()
+    want, wf = oracle.potential(system, state.positions, grid=(50, 50, 50), threads=8)
+    err = rel_rms(f, wf)
+    print("peptide force rel RMS", err)
+    assert err <= FORCE_REL_RMS, err
+    for key in ("bond", "angle", "torsion"):
+        assert abs(e[key] - want[key]) <= 1e-5 * abs(want[key]) + 1e-4, (key, e[key], want[key])
+    assert abs(e["direct_group"] - want["direct_group"]) <= 1e-4 * abs(want["direct_group"])
+    assert abs(e["reciprocal_group"] - want["reciprocal_group"]) <= 1e-5 * abs(want["reciprocal_group"])
+    assert abs(e["exceptions"] - want["exceptions"]) <= 1e-5 * abs(want["exceptions"])
+    assert e["pairs_within_cutoff"] == want["pairs_within_cutoff"]
+    loop.destroy()
+
+
+def test_peptide_one_step_with_shake(mdb, oracle, peptide):
+    system, state = peptide
+    loop = make_loop(mdb, system, state, seed=4)
+    loop.run(1)
+    p, v = loop.positions(), loop.velocities()
+    op, ov, _ = oracle.run(system, state, 1, seed=4, grid=(50, 50, 50), threads=8)
+    dp = np.abs(p - op).max()
+    dv = np.abs(v - ov).max()
+    print("peptide one step: max |dx|", dp, "max |dv|", dv)
+    assert dp <= 4e-7, dp
+    assert dv <= 4e-4, dv
+    # every constraint holds to the SHAKE tolerance
+    d = np.linalg.norm(p[system.constraint_p1] - p[system.constraint_p2], axis=1)
+    assert np.max(np.abs(d / system.constraint_distance - 1)) < 2e-6
+    loop.destroy()
