@@ -337,6 +337,34 @@ int mdb_get_barostat_stats(const mdb_engine* engine, int32_t system,
 int mdb_get_neighbour_stats(mdb_engine* engine, int32_t system,
                             mdb_neighbour_stats* out);
 
+/*
+ * Reciprocal-space PME (mesh energy and forces) that allocates nothing.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code running inside another framework's memory pool, a host that
+ * only receives device buffers from its own allocator, or a loop that must
+ * not allocate once started: the caller passes its own device buffers, and
+ * every intermediate lives in one fixed-size device array inside the library,
+ * so no cudaMalloc/cudaFree or allocating library call is made.
+ *
+ *   positions  device, 3n doubles, nm            charges  device, n doubles, e
+ *   forces     device, 3n doubles, overwritten with the reciprocal forces
+ *   energy     device, 1 double, the mesh sum (no self or net-charge term)
+ *   box        host, 9 doubles; mesh host, 3 ints; alpha in nm^-1
+ *   stream     a cudaStream_t, or NULL for the default stream
+ *
+ * Limits: at most 262,144 mesh points (64^3) and 128 points per axis, each
+ * axis 2/3/5/7-smooth; larger meshes return MDB_ERR_CAPACITY and non-smooth
+ * ones MDB_ERR_NOT_SMOOTH, before any device work.  The array (about 5.3 MB)
+ * stays resident on every device that loads the library until the process
+ * exits.  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  Every call shares the
+ * array and leaves its contents behind (the charge grid is cleared at the
+ * start of each call); calls whose device work overlaps race on it.
+ */
+int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* charges,
+                           const double box[9], double alpha, const int32_t mesh[3],
+                           double* forces, double* energy, void* stream);
+
 /* Per-stage device timing (see mdb_profile).  Replaces `StepLoop.profileStep`, loop.ts:705. */
 int mdb_profile_step(mdb_engine* engine, int32_t repeats, mdb_profile* out);
 

@@ -21,7 +21,13 @@
 //     x forward + convolution + x inverse in one pass, y inverse, z
 //     complex-to-real.  The reference's 7-13 global passes per direction and
 //     its separate load/convolve passes disappear.
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
 #include "device_state.h"
+#include "prep.h"
 
 namespace mdb {
 namespace {
@@ -462,3 +468,373 @@ void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
 }
 
 }  // namespace mdb
+
+// ===========================================================================
+// Reciprocal-space PME with no allocation: for callers that cannot allocate
+// device memory themselves -- code running inside another framework's memory
+// pool, a host whose only device memory is what its own allocator hands out,
+// or a real-time loop that forbids allocation after start-up.  The caller
+// passes its own device buffers for the inputs and outputs; every
+// intermediate (charge grid, half spectrum, potential, B-spline moduli,
+// twiddles, energy partials) lives in one file-scope device array of fixed
+// size, so this path never calls cudaMalloc, cudaFree or any allocating
+// library routine.
+//
+// Limits: at most kNoAllocMaxMeshPoints mesh points (64^3) and
+// kNoAllocMaxAxis points per axis.  Every call uses the same array and leaves
+// its contents behind; the charge grid is cleared at the start of each call.
+// Two calls whose device work overlaps (different streams, or different host
+// threads on one device) race on the array and must be serialised by the
+// caller.
+// ===========================================================================
+namespace mdb {
+namespace {
+
+constexpr long long kNoAllocMaxMeshPoints = 64ll * 64 * 64;
+constexpr int kNoAllocMaxAxis = 128;
+constexpr int kNoAllocMaxPartials = kNoAllocMaxAxis * ((kNoAllocMaxAxis / 2 + 1 + 15) / 16);
+
+// Byte offsets of the pieces inside the scratch array.
+constexpr size_t kNaGrid = 0;                                           // int64 x K
+constexpr size_t kNaSpectrum = kNaGrid + 8 * kNoAllocMaxMeshPoints;     // float2 x Kh (<= K)
+constexpr size_t kNaPotential = kNaSpectrum + 8 * kNoAllocMaxMeshPoints;  // f32 x K
+constexpr size_t kNaModuli = kNaPotential + 4 * kNoAllocMaxMeshPoints;  // f32 x 3 axes
+constexpr size_t kNaTwiddles = kNaModuli + 4 * 3 * kNoAllocMaxAxis;     // float2 x 3 axes
+constexpr size_t kNaPartials = kNaTwiddles + 8 * 3 * kNoAllocMaxAxis;   // f64 per x-pass CTA
+constexpr size_t kNaBytes = kNaPartials + 8 * kNoAllocMaxPartials;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+struct NaPtrs {
+  unsigned long long* grid;
+  float2* spectrum;
+  float* potential;
+  float* moduli;
+  float2* twiddles;
+  double* partials;
+};
+
+// Moduli |b(m)|^2 of the order-5 spline (bspline.ts:102) and the twiddles
+// exp(-2 pi i j / K) of each axis, computed on the device in FP64; and the
+// charge grid cleared, because the array keeps the previous call's contents.
+__global__ void k_na_setup(SysDev S, NaPtrs p) {
+  const long long K = static_cast<long long>(S.grid[0]) * S.grid[1] * S.grid[2];
+  for (long long i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) p.grid[i] = 0ull;
+  if (blockIdx.x != 0) return;
+  const double knots[4] = {1.0 / 24, 11.0 / 24, 11.0 / 24, 1.0 / 24};
+  for (int axis = 0; axis < 3; ++axis) {
+    const int n = S.grid[axis];
+    float* mod = p.moduli + axis * kNoAllocMaxAxis;
+    for (int m = threadIdx.x; m < n; m += blockDim.x) {
+      double re = 0, im = 0;
+      for (int k = 0; k < 4 && k < n; ++k) {
+        double s, c;
+        sincospi(2.0 * double((static_cast<long long>(m) * k) % n) / n, &s, &c);
+        re += knots[k] * c;
+        im += knots[k] * s;
+      }
+      mod[m] = float(re * re + im * im);
+      double s, c;
+      sincospi(-2.0 * m / n, &s, &c);
+      p.twiddles[axis * kNoAllocMaxAxis + m] = make_float2(float(c), float(s));
+    }
+  }
+  __syncthreads();
+  // bspline.ts:126 -- replace a vanishing modulus by its neighbours' mean
+  for (int axis = 0; axis < 3; ++axis) {
+    const int n = S.grid[axis];
+    float* mod = p.moduli + axis * kNoAllocMaxAxis;
+    if (threadIdx.x == 0)
+      for (int m = 0; m < n; ++m)
+        if (mod[m] < 1e-7f) mod[m] = 0.5f * (mod[(m - 1 + n) % n] + mod[(m + 1) % n]);
+  }
+}
+
+__device__ __forceinline__ long long fixed_from_double(double x) { return __double2ll_rn(x * 4294967296.0); }
+
+__global__ void k_na_spread(SysDev S, NaPtrs p, int n, const double* pos, const double* charge) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float q = float(charge[i]);
+    if (q == 0.f) continue;
+    Spline sp;
+    spline_for(S, fixed_from_double(pos[3 * i]), fixed_from_double(pos[3 * i + 1]),
+               fixed_from_double(pos[3 * i + 2]), sp, false);
+    const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
+    for (int ix = 0; ix < kPmeOrder; ++ix) {
+      int gx = sp.base[0] + ix;
+      if (gx >= Kx) gx -= Kx;
+      const float wx = q * sp.th[0][ix];
+      for (int iy = 0; iy < kPmeOrder; ++iy) {
+        int gy = sp.base[1] + iy;
+        if (gy >= Ky) gy -= Ky;
+        const float wxy = wx * sp.th[1][iy];
+        unsigned long long* row = p.grid + (static_cast<long long>(gx) * Ky + gy) * Kz;
+        for (int iz = 0; iz < kPmeOrder; ++iz) {
+          int gz = sp.base[2] + iz;
+          if (gz >= Kz) gz -= Kz;
+          add_fixed(&row[gz], wxy * sp.th[2][iz]);
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_na_z_forward(SysDev S, NaPtrs p, int lines_per_block) {
+  extern __shared__ float2 smem[];
+  const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  const int line0 = blockIdx.x * lines_per_block;
+  const int nl = min(lines_per_block, Kx * Ky - line0);
+  if (nl <= 0) return;
+  float2* A = smem;
+  float2* B = smem + nl * Kz;
+  unsigned long long* grid = p.grid + static_cast<long long>(line0) * Kz;
+  for (int i = threadIdx.x; i < nl * Kz; i += blockDim.x) {
+    A[i] = make_float2(from_fixed(static_cast<long long>(grid[i])), 0.f);
+    grid[i] = 0ull;
+  }
+  __syncthreads();
+  const float2* R = fft_lines(A, B, Kz, nl, S.radices[2], S.nradix[2], p.twiddles + 2 * kNoAllocMaxAxis, -1);
+  float2* out = p.spectrum + static_cast<long long>(line0) * kzh;
+  for (int i = threadIdx.x; i < nl * kzh; i += blockDim.x) {
+    const int line = i / kzh, k = i - line * kzh;
+    out[i] = R[line * Kz + k];
+  }
+}
+
+__global__ void k_na_y(SysDev S, NaPtrs p, int sign) {
+  extern __shared__ float2 smem[];
+  const int Ky = S.grid[1], kzh = S.kzh;
+  const int tiles = (kzh + 15) / 16;
+  const int x = blockIdx.x / tiles, kz0 = (blockIdx.x % tiles) * 16;
+  const int nk = min(16, kzh - kz0);
+  float2* A = smem;
+  float2* B = smem + nk * Ky;
+  float2* base = p.spectrum + static_cast<long long>(x) * Ky * kzh + kz0;
+  for (int i = threadIdx.x; i < nk * Ky; i += blockDim.x) {
+    const int y = i / nk, l = i - y * nk;
+    A[l * Ky + y] = base[static_cast<long long>(y) * kzh + l];
+  }
+  __syncthreads();
+  const float2* R = fft_lines(A, B, Ky, nk, S.radices[1], S.nradix[1], p.twiddles + kNoAllocMaxAxis, sign);
+  for (int i = threadIdx.x; i < nk * Ky; i += blockDim.x) {
+    const int y = i / nk, l = i - y * nk;
+    base[static_cast<long long>(y) * kzh + l] = R[l * Ky + y];
+  }
+}
+
+__global__ void k_na_x_convolve(SysDev S, NaPtrs p) {
+  extern __shared__ float2 smem[];
+  __shared__ double partial[kThreads / 32];
+  const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  const int tiles = (kzh + 15) / 16;
+  const int my = blockIdx.x / tiles, kz0 = (blockIdx.x % tiles) * 16;
+  const int nk = min(16, kzh - kz0);
+  float2* A = smem;
+  float2* B = smem + nk * Kx;
+  const long long stride = static_cast<long long>(Ky) * kzh;
+  float2* base = p.spectrum + static_cast<long long>(my) * kzh + kz0;
+  for (int i = threadIdx.x; i < nk * Kx; i += blockDim.x) {
+    const int x = i / nk, l = i - x * nk;
+    A[l * Kx + x] = base[x * stride + l];
+  }
+  __syncthreads();
+  float2* R = fft_lines(A, B, Kx, nk, S.radices[0], S.nradix[0], p.twiddles, -1);
+  float2* other = R == A ? B : A;
+  const int mb = my <= Ky / 2 ? my : my - Ky;
+  const float* modx = p.moduli;
+  const float* mody = p.moduli + kNoAllocMaxAxis;
+  const float* modz = p.moduli + 2 * kNoAllocMaxAxis;
+  double energy = 0.0;
+  for (int i = threadIdx.x; i < nk * Kx; i += blockDim.x) {
+    const int l = i / Kx, mx = i - l * Kx;
+    const int kz = kz0 + l;
+    const int ma = mx <= Kx / 2 ? mx : mx - Kx;
+    float2 v = R[i];
+    float factor = 0.f;
+    if (mx != 0 || my != 0 || kz != 0) {
+      const float* M = S.inv_f;
+      const float two_pi = 6.283185307179586f;
+      const float kx = two_pi * ma * M[0];
+      const float ky = two_pi * (ma * M[3] + mb * M[4]);
+      const float kzv = two_pi * (ma * M[6] + mb * M[7] + kz * M[8]);
+      const float k2 = kx * kx + ky * ky + kzv * kzv;
+      factor = S.pme_pref * expf(k2 * S.exp_scale) / (k2 * modx[mx] * mody[my] * modz[kz]);
+    }
+    const double weight = (kz == 0 || (2 * kz == Kz)) ? 1.0 : 2.0;
+    energy += weight * double(factor) * (double(v.x) * v.x + double(v.y) * v.y);
+    v.x *= 2.f * factor;
+    v.y *= 2.f * factor;
+    R[i] = v;
+  }
+  __syncthreads();
+  const float2* Q = fft_lines(R, other, Kx, nk, S.radices[0], S.nradix[0], p.twiddles, +1);
+  for (int i = threadIdx.x; i < nk * Kx; i += blockDim.x) {
+    const int x = i / nk, l = i - x * nk;
+    base[x * stride + l] = Q[l * Kx + x];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) energy += __shfl_xor_sync(0xffffffffu, energy, o);
+  if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = energy;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int k = 0; k < (blockDim.x >> 5); ++k) total += partial[k];
+    p.partials[blockIdx.x] = total;
+  }
+}
+
+__global__ void k_na_z_inverse(SysDev S, NaPtrs p, int lines_per_block) {
+  extern __shared__ float2 smem[];
+  const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  const int line0 = blockIdx.x * lines_per_block;
+  const int nl = min(lines_per_block, Kx * Ky - line0);
+  if (nl <= 0) return;
+  float2* A = smem;
+  float2* B = smem + nl * Kz;
+  const float2* in = p.spectrum + static_cast<long long>(line0) * kzh;
+  for (int i = threadIdx.x; i < nl * kzh; i += blockDim.x) {
+    const int line = i / kzh, k = i - line * kzh;
+    A[line * Kz + k] = in[i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nl * (Kz - kzh); i += blockDim.x) {
+    const int line = i / (Kz - kzh), k = kzh + (i - line * (Kz - kzh));
+    const float2 c = A[line * Kz + (Kz - k)];
+    A[line * Kz + k] = make_float2(c.x, -c.y);
+  }
+  __syncthreads();
+  const float2* R = fft_lines(A, B, Kz, nl, S.radices[2], S.nradix[2], p.twiddles + 2 * kNoAllocMaxAxis, +1);
+  float* out = p.potential + static_cast<long long>(line0) * Kz;
+  for (int i = threadIdx.x; i < nl * Kz; i += blockDim.x) out[i] = R[i].x;
+}
+
+__global__ void k_na_gather(SysDev S, NaPtrs p, int n, const double* pos, const double* charge, double* forces) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float q = float(charge[i]);
+    if (q == 0.f) {
+      forces[3 * i] = forces[3 * i + 1] = forces[3 * i + 2] = 0.0;
+      continue;
+    }
+    Spline sp;
+    spline_for(S, fixed_from_double(pos[3 * i]), fixed_from_double(pos[3 * i + 1]),
+               fixed_from_double(pos[3 * i + 2]), sp, true);
+    const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
+    float ga = 0.f, gb = 0.f, gc = 0.f;
+    for (int ix = 0; ix < kPmeOrder; ++ix) {
+      int gx = sp.base[0] + ix;
+      if (gx >= Kx) gx -= Kx;
+      for (int iy = 0; iy < kPmeOrder; ++iy) {
+        int gy = sp.base[1] + iy;
+        if (gy >= Ky) gy -= Ky;
+        const float* row = p.potential + (static_cast<long long>(gx) * Ky + gy) * Kz;
+        const float wxy = sp.th[0][ix] * sp.th[1][iy];
+        const float dxy = sp.dth[0][ix] * sp.th[1][iy];
+        const float xdy = sp.th[0][ix] * sp.dth[1][iy];
+        for (int iz = 0; iz < kPmeOrder; ++iz) {
+          int gz = sp.base[2] + iz;
+          if (gz >= Kz) gz -= Kz;
+          const float v = row[gz];
+          ga = fmaf(v * dxy, sp.th[2][iz], ga);
+          gb = fmaf(v * xdy, sp.th[2][iz], gb);
+          gc = fmaf(v * wxy, sp.dth[2][iz], gc);
+        }
+      }
+    }
+    const float* U = S.umat_f;
+    forces[3 * i] = -q * (ga * U[0] + gb * U[1] + gc * U[2]);
+    forces[3 * i + 1] = -q * (ga * U[3] + gb * U[4] + gc * U[5]);
+    forces[3 * i + 2] = -q * (ga * U[6] + gb * U[7] + gc * U[8]);
+  }
+}
+
+__global__ void k_na_energy(NaPtrs p, int count, double* energy) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double total = 0.0;
+    for (int k = 0; k < count; ++k) total += p.partials[k];
+    *energy = total;
+  }
+}
+
+// The scratch array's device address, looked up once per device with that
+// device current.  In host code `g_noalloc_scratch` names a host-side stand-in,
+// never device memory, so kernels must be given this address instead.
+std::mutex g_noalloc_mutex;
+std::array<unsigned char*, 64> g_noalloc_address{};
+
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= int(g_noalloc_address.size())) return MDB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_address[device]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || ptr == nullptr) return MDB_ERR_DEVICE;
+    g_noalloc_address[device] = static_cast<unsigned char*>(ptr);
+  }
+  *out = g_noalloc_address[device];
+  return MDB_OK;
+}
+
+}  // namespace
+}  // namespace mdb
+
+extern "C" int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* charges,
+                                      const double box[9], double alpha, const int32_t mesh[3], double* forces,
+                                      double* energy, void* stream) {
+  using namespace mdb;
+  if (n < 0 || !box || !mesh || !energy || !(alpha > 0) || (n > 0 && (!positions || !charges || !forces)))
+    return MDB_ERR_INVALID_ARGUMENT;
+  long long points = 1;
+  for (int k = 0; k < 3; ++k) {
+    if (mesh[k] < 2 || mesh[k] > kNoAllocMaxAxis) return MDB_ERR_CAPACITY;
+    points *= mesh[k];
+  }
+  if (points > kNoAllocMaxMeshPoints) return MDB_ERR_CAPACITY;
+  SysDev S;
+  std::memset(&S, 0, sizeof(S));
+  for (int k = 0; k < 3; ++k) {
+    S.grid[k] = mesh[k];
+    if (!plan_radices(mesh[k], S.radices[k], &S.nradix[k])) return MDB_ERR_NOT_SMOOTH;
+  }
+  S.kzh = mesh[2] / 2 + 1;
+  double B[9], M[9];
+  if (!reduce_box(box, B)) return MDB_ERR_INVALID_ARGUMENT;
+  inverse_box(B, M);
+  for (int i = 0; i < 9; ++i) S.inv_f[i] = float(M[i]);
+  const double um[6] = {mesh[0] * M[0], mesh[0] * M[3], mesh[0] * M[6], mesh[1] * M[4], mesh[1] * M[7], mesh[2] * M[8]};
+  for (int i = 0; i < 6; ++i) S.umat[i] = std::llround(um[i] * 4294967296.0);
+  for (int v = 0; v < 3; ++v)
+    for (int u = 0; u < 3; ++u) S.umat_f[v * 3 + u] = float(mesh[u] * M[v * 3 + u]);
+  S.pme_pref = float(kOne4PiEps0 * 2 * 3.14159265358979323846 / box_volume(B));
+  S.exp_scale = float(-1.0 / (4 * alpha * alpha));
+
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return MDB_ERR_NO_DEVICE;
+  unsigned char* base = nullptr;
+  const int status = noalloc_scratch(device, &base);
+  if (status != MDB_OK) return status;
+  NaPtrs p;
+  p.grid = reinterpret_cast<unsigned long long*>(base + kNaGrid);
+  p.spectrum = reinterpret_cast<float2*>(base + kNaSpectrum);
+  p.potential = reinterpret_cast<float*>(base + kNaPotential);
+  p.moduli = reinterpret_cast<float*>(base + kNaModuli);
+  p.twiddles = reinterpret_cast<float2*>(base + kNaTwiddles);
+  p.partials = reinterpret_cast<double*>(base + kNaPartials);
+
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int lines = std::max(1, 2048 / mesh[2]);
+  const int z_blocks = int((mesh[0] * mesh[1] + lines - 1) / lines);
+  const int tiles = (S.kzh + 15) / 16;
+  const int z_smem = 2 * lines * mesh[2] * int(sizeof(float2));
+  const int y_smem = 2 * 16 * mesh[1] * int(sizeof(float2));
+  const int x_smem = 2 * 16 * mesh[0] * int(sizeof(float2));
+  const int atom_blocks = std::max(1, std::min((n + kThreads - 1) / kThreads, 148 * 8));
+  k_na_setup<<<std::max(1, int(std::min<long long>((points + kThreads - 1) / kThreads, 148 * 8))), kThreads, 0, st>>>(S, p);
+  if (n > 0) k_na_spread<<<atom_blocks, kThreads, 0, st>>>(S, p, n, positions, charges);
+  k_na_z_forward<<<z_blocks, kThreads, z_smem, st>>>(S, p, lines);
+  k_na_y<<<mesh[0] * tiles, kThreads, y_smem, st>>>(S, p, -1);
+  k_na_x_convolve<<<mesh[1] * tiles, kThreads, x_smem, st>>>(S, p);
+  k_na_y<<<mesh[0] * tiles, kThreads, y_smem, st>>>(S, p, +1);
+  k_na_z_inverse<<<z_blocks, kThreads, z_smem, st>>>(S, p, lines);
+  if (n > 0) k_na_gather<<<atom_blocks, kThreads, 0, st>>>(S, p, n, positions, charges, forces);
+  k_na_energy<<<1, 32, 0, st>>>(p, mesh[1] * tiles, energy);
+  return cudaGetLastError() == cudaSuccess ? MDB_OK : MDB_ERR_DEVICE;
+}

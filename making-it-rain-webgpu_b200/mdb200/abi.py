@@ -238,6 +238,10 @@ EXPORTS = {
     "mdb_get_neighbour_stats": (C.c_int, [_E, C.c_int32, C.POINTER(NeighbourStats)]),
     "mdb_memory_report": (C.c_int, [_E, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "mdb_profile_step": (C.c_int, [_E, C.c_int32, C.POINTER(Profile)]),
+    "mdb_reciprocal_noalloc": (
+        C.c_int,
+        [C.c_int32, C.c_void_p, C.c_void_p, _dp, C.c_double, _ip, C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
 }
 
 _library = None
