@@ -53,7 +53,14 @@ enum ErrorBit : int {
   kErrCellCapacity = 16
 };
 
-enum UnitKind : int { kUnitFree = 0, kUnitSettle = 1, kUnitShake = 2 };
+// kUnitStar: a SHAKE cluster whose constraints all join atom 0 to atoms
+// 1..nc (X-H_n, nc <= 3), solved with compile-time sizes.
+enum UnitKind : int { kUnitFree = 0, kUnitSettle = 1, kUnitShake = 2, kUnitStar = 3 };
+
+// Integrate blocks: kIntegrateUnits units per block, their atoms staged in a
+// shared-memory table of at most kIntegrateTable entries.
+constexpr int kIntegrateUnits = 32;
+constexpr int kIntegrateTable = kIntegrateUnits * kMaxClusterAtoms;
 
 // One integration unit: a free atom, a SETTLE water, or a SHAKE cluster.
 struct UnitDev {
@@ -61,6 +68,7 @@ struct UnitDev {
   int sys;
   int na;
   int nc;
+  int base;                     // first entry of the unit's atoms in its block's table
   int atom[kMaxClusterAtoms];   // global atom indices
   float dist[kMaxClusterConstraints];
   unsigned char ci[kMaxClusterConstraints];

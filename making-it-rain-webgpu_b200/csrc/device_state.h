@@ -99,6 +99,9 @@ struct Dev {
   const int* iblk_sys;
   const int* iblk_unit0;
   const int* iblk_nunit;
+  const int* iblk_atom0;  // first table entry of each integrate block in `iatom`
+  const int* iblk_natom;
+  const int* iatom;       // global atom index of every table entry, block by block
   double* mom_partial;  // 3 per integrate block
   float4* vcom;         // per system, for the next step's COM removal
   long long* step;      // per system

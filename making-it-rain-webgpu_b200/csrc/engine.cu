@@ -38,8 +38,7 @@ using namespace mdb;
 namespace {
 
 constexpr double kCellWidth = 0.25;  // nm, fractional cells of the spatial sort
-constexpr int kIntegrateBlock = 128;
-constexpr int kFftTile = 16;
+constexpr int kFftTile = 8;  // kz columns per y- and x-pass CTA
 
 struct Allocation {
   std::string label;
@@ -313,7 +312,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   std::vector<float2> twiddles;
   std::vector<FftWork> wz, wy, wx;
   std::vector<UnitDev> units;
-  std::vector<int> iblk_sys, iblk_unit0, iblk_nunit;
+  std::vector<int> iblk_sys, iblk_unit0, iblk_nunit, iblk_atom0, iblk_natom, iatom;
   int atoms = 0, slots = 0, blocks = 0, cells = 0, tiles = 0, units_n = 0, iblk = 0;
   long long grid_pts = 0, cgrid_pts = 0;
   int smem_z = 0, smem_y = 0, smem_x = 0;
@@ -366,7 +365,9 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     }
     // FFT work items
     const int Kx = h.grid[0], Ky = h.grid[1], Kz = h.grid[2];
-    const int lines = std::max(1, 2048 / Kz);
+    // lines per z-pass CTA: at most 2048 points in shared memory, and enough
+    // CTAs (about two per SM) that a small mesh still fills the device
+    const int lines = std::max(1, std::min(2048 / Kz, (Kx * Ky + 295) / 296));
     for (int l = 0; l < Kx * Ky; l += lines) wz.push_back({s, l, 0, std::min(lines, Kx * Ky - l)});
     smem_z = std::max(smem_z, 2 * lines * Kz * int(sizeof(float2)));
     for (int x = 0; x < Kx; ++x)
@@ -450,6 +451,25 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
         u.cj[k] = (unsigned char)(std::find(cl.atoms.begin(), cl.atoms.end(), h.cp2[c]) - cl.atoms.begin());
         u.dist[k] = float(h.cdist[c]);
       }
+      // An X-H_n star (one atom in every constraint, nc = na - 1 <= 3) is
+      // reordered to centre first and spoke c at position c + 1.
+      if (u.nc >= 1 && u.nc <= 3 && u.na == u.nc + 1) {
+        for (int centre : {int(u.ci[0]), int(u.cj[0])}) {
+          bool star = true;
+          for (int k = 0; k < u.nc; ++k) star &= u.ci[k] == centre || u.cj[k] == centre;
+          if (!star) continue;
+          int atom[kMaxClusterAtoms];
+          atom[0] = u.atom[centre];
+          for (int k = 0; k < u.nc; ++k) {
+            atom[k + 1] = u.atom[u.ci[k] == centre ? u.cj[k] : u.ci[k]];
+            u.ci[k] = 0;
+            u.cj[k] = (unsigned char)(k + 1);
+          }
+          for (int k = 0; k < u.na; ++k) u.atom[k] = atom[k];
+          u.kind = kUnitStar;
+          break;
+        }
+      }
       su.push_back(u);
     }
     for (int a : h.free_atoms) {
@@ -463,10 +483,20 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     S.unit_off = units_n;
     S.n_units = int(su.size());
     S.iblk_off = iblk;
-    for (int u0 = 0; u0 < S.n_units; u0 += kIntegrateBlock) {
+    for (int u0 = 0; u0 < S.n_units; u0 += kIntegrateUnits) {
+      const int nu = std::min(kIntegrateUnits, S.n_units - u0);
       iblk_sys.push_back(s);
       iblk_unit0.push_back(units_n + u0);
-      iblk_nunit.push_back(std::min(kIntegrateBlock, S.n_units - u0));
+      iblk_nunit.push_back(nu);
+      iblk_atom0.push_back(int(iatom.size()));
+      int entries = 0;
+      for (int k = 0; k < nu; ++k) {
+        UnitDev& u = su[u0 + k];
+        u.base = entries;
+        for (int j = 0; j < u.na; ++j) iatom.push_back(u.atom[j]);
+        entries += u.na;
+      }
+      iblk_natom.push_back(entries);  // <= kIntegrateTable: na <= kMaxClusterAtoms
       ++iblk;
     }
     S.n_iblk = iblk - S.iblk_off;
@@ -599,6 +629,12 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.iblk_unit0 = tmp_i;
   TRY(upload(e, "integrate block count", tmp_i, iblk_nunit));
   d.iblk_nunit = tmp_i;
+  TRY(upload(e, "integrate block table start", tmp_i, iblk_atom0));
+  d.iblk_atom0 = tmp_i;
+  TRY(upload(e, "integrate block table size", tmp_i, iblk_natom));
+  d.iblk_natom = tmp_i;
+  TRY(upload(e, "integrate block table", tmp_i, iatom));
+  d.iatom = tmp_i;
   TRY(alloc(e, "momentum partials", d.mom_partial, size_t(iblk) * 3));
   TRY(alloc(e, "com velocity", d.vcom, n));
   std::vector<long long> steps(n);

@@ -234,6 +234,108 @@ __device__ __forceinline__ long long displace(float wanted, float& left_over) {
   return taken;
 }
 
+// ------------------------------------------------------- star clusters ----
+// Most SHAKE clusters are an X-H_n star (every constraint joins the centre,
+// atom 0, to one spoke, atom c + 1): C-H, CH2, CH3, N-H, NH3+.  Written for
+// that shape with the constraint count known at compile time, the FP64 solves
+// stay in registers; the general `rattle`/`shake` above index their arrays at
+// run time and spill to local memory.  Same Jacobi iterations, same order.
+template <int NC>
+__device__ bool rattle_star(const long long* x, const long long* y, const long long* z, float* vx, float* vy,
+                            float* vz, const float* im, float tol) {
+  constexpr int NA = NC + 1;
+  double v[NA][3], w[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    v[k][0] = vx[k]; v[k][1] = vy[k]; v[k][2] = vz[k];
+    w[k] = im[k];
+  }
+  double rv[NC][3], rl[NC], rm[NC], delta[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    rv[c][0] = from_fixed(x[0] - x[c + 1]);
+    rv[c][1] = from_fixed(y[0] - y[c + 1]);
+    rv[c][2] = from_fixed(z[0] - z[c + 1]);
+    rl[c] = rv[c][0] * rv[c][0] + rv[c][1] * rv[c][1] + rv[c][2] * rv[c][2];
+    const double sum = w[0] + w[c + 1];
+    rm[c] = sum == 0.0 ? 0.0 : 0.5 / sum;
+  }
+  bool ok = false;
+  for (int it = 0; it < kMaxShakeIterations; ++it) {
+    int conv = 0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const double proj = (v[0][0] - v[c + 1][0]) * rv[c][0] + (v[0][1] - v[c + 1][1]) * rv[c][1] +
+                          (v[0][2] - v[c + 1][2]) * rv[c][2];
+      delta[c] = rl[c] == 0.0 ? 0.0 : (-2.0 * rm[c] * proj) / rl[c];
+      conv += fabs(delta[c]) <= tol;
+    }
+    if (conv == NC) { ok = true; break; }
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double dr = rv[c][k] * delta[c];
+        v[0][k] += dr * w[0];
+        v[c + 1][k] -= dr * w[c + 1];
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    vx[k] = float(v[k][0]); vy[k] = float(v[k][1]); vz[k] = float(v[k][2]);
+  }
+  return ok;
+}
+
+// `dp` holds the trial displacements on input and the constrained ones on output.
+template <int NC>
+__device__ bool shake_star(const long long* x, const long long* y, const long long* z, const float* im,
+                           const float* dist, float3* dp, float tol) {
+  constexpr int NA = NC + 1;
+  double q[NA][3], w[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    q[k][0] = dp[k].x; q[k][1] = dp[k].y; q[k][2] = dp[k].z;
+    w[k] = im[k];
+  }
+  double rv[NC][3], rm[NC], d2[NC], delta[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    rv[c][0] = from_fixed(x[0] - x[c + 1]);
+    rv[c][1] = from_fixed(y[0] - y[c + 1]);
+    rv[c][2] = from_fixed(z[0] - z[c + 1]);
+    const double sum = w[0] + w[c + 1];
+    rm[c] = sum == 0.0 ? 0.0 : 0.5 / sum;
+    d2[c] = double(dist[c]) * dist[c];
+  }
+  const double lo = 1.0 - 2.0 * tol + double(tol) * tol, hi = 1.0 + 2.0 * tol + double(tol) * tol;
+  bool ok = false;
+  for (int it = 0; it < kMaxShakeIterations; ++it) {
+    int conv = 0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const double ex = rv[c][0] + q[0][0] - q[c + 1][0], ey = rv[c][1] + q[0][1] - q[c + 1][1],
+                   ez = rv[c][2] + q[0][2] - q[c + 1][2];
+      const double l2 = ex * ex + ey * ey + ez * ez;
+      const double proj = ex * rv[c][0] + ey * rv[c][1] + ez * rv[c][2];
+      delta[c] = proj == 0.0 ? 0.0 : rm[c] * (d2[c] - l2) / proj;
+      conv += (l2 >= lo * d2[c] && l2 <= hi * d2[c]);
+    }
+    if (conv == NC) { ok = true; break; }
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double dr = rv[c][k] * delta[c];
+        q[0][k] += dr * w[0];
+        q[c + 1][k] -= dr * w[c + 1];
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < NA; ++k) dp[k] = make_float3(float(q[k][0]), float(q[k][1]), float(q[k][2]));
+  return ok;
+}
+
 __device__ void block_sum3(double* v, double (*red)[kThreads / 32]) {
 #pragma unroll
   for (int k = 0; k < 3; ++k)
@@ -251,22 +353,26 @@ __device__ void block_sum3(double* v, double (*red)[kThreads / 32]) {
 }
 
 // The last block of a system turns the block momenta into the next step's
-// COM velocity and advances the step; the last block of the launch snapshots
-// the rebuild requests for the next step's list kernels.
-__device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance) {
+// COM velocity (a fixed-order block reduction, so runs stay bit-identical) and
+// advances the step; the last block of the launch snapshots the rebuild
+// requests for the next step's list kernels.
+__device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance, double (*red)[kThreads / 32]) {
   __shared__ int last_of_system, last_of_launch;
   __threadfence();
   if (threadIdx.x == 0) last_of_system = atomicAdd(&d.done_count[s], 1) == S.n_iblk - 1;
   __syncthreads();
-  if (last_of_system && threadIdx.x == 0) {
+  if (last_of_system) {
     __threadfence();
     double p[3] = {0, 0, 0};
-    for (int b = S.iblk_off; b < S.iblk_off + S.n_iblk; ++b)
-      for (int k = 0; k < 3; ++k) p[k] += d.mom_partial[b * 3 + k];
-    const double m = S.total_mass > 0 ? S.total_mass : 1.0;
-    d.vcom[s] = make_float4(float(p[0] / m), float(p[1] / m), float(p[2] / m), 0.f);
-    if (advance) d.step[s] += 1;
-    d.done_count[s] = 0;
+    for (int i = threadIdx.x; i < S.n_iblk; i += kThreads)
+      for (int k = 0; k < 3; ++k) p[k] += __ldcg(&d.mom_partial[(S.iblk_off + i) * 3 + k]);
+    block_sum3(p, red);
+    if (threadIdx.x == 0) {
+      const double m = S.total_mass > 0 ? S.total_mass : 1.0;
+      d.vcom[s] = make_float4(float(p[0] / m), float(p[1] / m), float(p[2] / m), 0.f);
+      if (advance) d.step[s] += 1;
+      d.done_count[s] = 0;
+    }
   }
   if (!advance) return;
   __threadfence();
@@ -276,7 +382,7 @@ __device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance)
     __threadfence();
     int any = 0;
     for (int k = 0; k < d.S; ++k) {
-      const int f = d.rebuild_flag[k] | d.run.always_rebuild;
+      const int f = __ldcg(&d.rebuild_flag[k]) | d.run.always_rebuild;
       d.rebuild_now[k] = f;
       d.rebuild_flag[k] = 0;
       any |= f;
@@ -286,168 +392,258 @@ __device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance)
   }
 }
 
-// One unit through the whole step.  NA is the atom count known at compile
-// time (3 for a SETTLE water, 1 for a free atom), so those units live in
-// registers; SHAKE clusters take the general path with NA = 8 and `na` atoms.
-template <int NA, int KIND>
-__device__ __forceinline__ void integrate_unit(const Dev& d, const SysDev& S, const UnitDev* up, long long step,
-                                               bool com, float4 vc, double* mom, bool& moved, bool& bad) {
-  const RunDev& R = d.run;
-  const int na = KIND == kUnitShake ? up->na : NA;
-  Atom at[NA];
-  int atom[NA];
+// One integrate block: up to kIntegrateUnits units and their atoms, staged in
+// shared memory between phases that alternate between one thread per atom
+// (loads, kick, noise, drift, finish: the bulk of the arithmetic and every
+// global access) and one thread per unit (the constraint solves).
+struct Stage {
+  long long x[kIntegrateTable], y[kIntegrateTable], z[kIntegrateTable];     // start-of-step positions
+  long long tx[kIntegrateTable], ty[kIntegrateTable], tz[kIntegrateTable];  // unconstrained drift
+  long long cx[kIntegrateTable], cy[kIntegrateTable], cz[kIntegrateTable];  // constrained drift
+  float vx[kIntegrateTable], vy[kIntegrateTable], vz[kIntegrateTable], im[kIntegrateTable];
+};
+
+constexpr int kPerThread = kIntegrateTable / kThreads;
+
+__device__ __forceinline__ Atom staged_atom(const Stage& sh, int e) {
+  Atom A;
+  A.x = sh.x[e]; A.y = sh.y[e]; A.z = sh.z[e];
+  A.vx = sh.vx[e]; A.vy = sh.vy[e]; A.vz = sh.vz[e];
+  A.im = sh.im[e];
+  return A;
+}
+
+__device__ __noinline__ void cluster_velocities(Stage& sh, const UnitDev& u, float tol, bool& bad) {
+  const int e = u.base;
+  Atom at[kMaxClusterAtoms];
+  for (int k = 0; k < u.na; ++k) at[k] = staged_atom(sh, e + k);
+  bad |= !rattle(at, u, tol);
+  for (int k = 0; k < u.na; ++k) { sh.vx[e + k] = at[k].vx; sh.vy[e + k] = at[k].vy; sh.vz[e + k] = at[k].vz; }
+}
+
+// Velocity constraints of one unit (LFMiddle, after the kick).
+__device__ void unit_velocities(Stage& sh, const UnitDev& u, float tol, bool& bad) {
+  const int e = u.base;
+  if (u.kind == kUnitSettle) {
+    Atom at[3];
 #pragma unroll
-  for (int k = 0; k < NA; ++k) {
-    if (k >= na) break;
-    const int a = up->atom[k];
-    atom[k] = a;
-    Atom& A = at[k];
-    A.x = d.px[a]; A.y = d.py[a]; A.z = d.pz[a];
-    A.vx = d.vx[a]; A.vy = d.vy[a]; A.vz = d.vz[a];
-    A.rx = d.rx[a]; A.ry = d.ry[a]; A.rz = d.rz[a];
-    A.im = d.invm[a];
-    const int gs = S.slot_off + d.rank[a];
-    A.fx = from_fixed(static_cast<long long>(d.fx[gs]));
-    A.fy = from_fixed(static_cast<long long>(d.fy[gs]));
-    A.fz = from_fixed(static_cast<long long>(d.fz[gs]));
-    d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;  // consumer clears
-    if (com && A.im > 0.f) { A.vx -= vc.x; A.vy -= vc.y; A.vz -= vc.z; }
-  }
-  const float dt = R.dt;
-  long long tx[NA], ty[NA], tz[NA];  // drift, 2^32 fixed point
-  float3 dp[NA];
-  if (R.integrator == 0) {
-    // ---- LFMiddle ----
+    for (int k = 0; k < 3; ++k) at[k] = staged_atom(sh, e + k);
+    settle_velocities(at);
 #pragma unroll
-    for (int k = 0; k < NA; ++k) {
-      if (k >= na) break;
-      Atom& A = at[k];
-      if (A.im == 0.f) continue;
-      A.vx += dt * A.im * A.fx; A.vy += dt * A.im * A.fy; A.vz += dt * A.im * A.fz;
+    for (int k = 0; k < 3; ++k) { sh.vx[e + k] = at[k].vx; sh.vy[e + k] = at[k].vy; sh.vz[e + k] = at[k].vz; }
+  } else if (u.kind == kUnitStar) {
+    switch (u.nc) {
+      case 1: bad |= !rattle_star<1>(sh.x + e, sh.y + e, sh.z + e, sh.vx + e, sh.vy + e, sh.vz + e, sh.im + e, tol); break;
+      case 2: bad |= !rattle_star<2>(sh.x + e, sh.y + e, sh.z + e, sh.vx + e, sh.vy + e, sh.vz + e, sh.im + e, tol); break;
+      default: bad |= !rattle_star<3>(sh.x + e, sh.y + e, sh.z + e, sh.vx + e, sh.vy + e, sh.vz + e, sh.im + e, tol); break;
     }
-    if (KIND == kUnitSettle) settle_velocities(at);
-    else if (KIND == kUnitShake) bad |= !rattle(at, *up, R.tolerance);
-    const float half = 0.5f * dt;
-#pragma unroll
-    for (int k = 0; k < NA; ++k) {
-      if (k >= na) break;
-      Atom& A = at[k];
-      tx[k] = ty[k] = tz[k] = 0;
-      if (A.im == 0.f) continue;
-      float n0 = 0.f, n1 = 0.f, n2 = 0.f;
-      if (R.draw_noise) {
-        const unsigned p = static_cast<unsigned>(atom[k] - S.atom_off);
-        const uint2 key = make_uint2(R.seed, kThermostatDomain);
-        const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
-        const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
-        n0 = g0.x; n1 = g0.y; n2 = g1.x;
-      }
-      const float noise = R.noise_scale * sqrtf(R.kt * A.im);
-      float lo;
-      tx[k] = displace(A.vx * half + A.rx, lo);
-      A.vx = R.velocity_scale * A.vx + noise * n0;
-      tx[k] += displace(A.vx * half + lo, A.rx);
-      ty[k] = displace(A.vy * half + A.ry, lo);
-      A.vy = R.velocity_scale * A.vy + noise * n1;
-      ty[k] += displace(A.vy * half + lo, A.ry);
-      tz[k] = displace(A.vz * half + A.rz, lo);
-      A.vz = R.velocity_scale * A.vz + noise * n2;
-      tz[k] += displace(A.vz * half + lo, A.rz);
-    }
-  } else {
-    // ---- velocity Verlet (integrate.wgsl:91-132) ----
-#pragma unroll
-    for (int k = 0; k < NA; ++k) {
-      if (k >= na) break;
-      Atom& A = at[k];
-      tx[k] = ty[k] = tz[k] = 0;
-      if (A.im == 0.f) continue;
-      A.vx += A.im * A.fx * dt; A.vy += A.im * A.fy * dt; A.vz += A.im * A.fz * dt;
-      tx[k] = displace(A.vx * dt + A.rx, A.rx);
-      ty[k] = displace(A.vy * dt + A.ry, A.ry);
-      tz[k] = displace(A.vz * dt + A.rz, A.rz);
-    }
-  }
-  // position constraints, relative to the start-of-step positions
-  long long cx[NA], cy[NA], cz[NA];
-#pragma unroll
-  for (int k = 0; k < NA; ++k) {
-    if (k >= na) break;
-    dp[k] = make_float3(from_fixed(tx[k]), from_fixed(ty[k]), from_fixed(tz[k]));
-  }
-  if (KIND == kUnitFree) {
-    cx[0] = tx[0]; cy[0] = ty[0]; cz[0] = tz[0];
-  } else {
-    if (KIND == kUnitSettle) settle_positions(at, dp, up->dist[0], up->dist[1]);
-    else bad |= !shake(at, dp, *up, R.tolerance);
-#pragma unroll
-    for (int k = 0; k < NA; ++k) {
-      if (k >= na) break;
-      if (at[k].im == 0.f) { cx[k] = tx[k]; cy[k] = ty[k]; cz[k] = tz[k]; continue; }
-      cx[k] = to_fixed(dp[k].x); cy[k] = to_fixed(dp[k].y); cz[k] = to_fixed(dp[k].z);
-    }
-  }
-  const float idt = 1.f / dt;
-#pragma unroll
-  for (int k = 0; k < NA; ++k) {
-    if (k >= na) break;
-    Atom& A = at[k];
-    const int a = atom[k];
-    if (A.im != 0.f) {
-      if (R.integrator == 0) {
-        A.vx += idt * from_fixed(cx[k] - tx[k]);
-        A.vy += idt * from_fixed(cy[k] - ty[k]);
-        A.vz += idt * from_fixed(cz[k] - tz[k]);
-      } else {
-        A.vx = idt * from_fixed(cx[k]);
-        A.vy = idt * from_fixed(cy[k]);
-        A.vz = idt * from_fixed(cz[k]);
-      }
-      A.x += cx[k]; A.y += cy[k]; A.z += cz[k];
-      d.px[a] = A.x; d.py[a] = A.y; d.pz[a] = A.z;
-      d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
-      d.rx[a] = A.rx; d.ry[a] = A.ry; d.rz[a] = A.rz;
-      const double m = 1.0 / A.im;
-      mom[0] += m * A.vx; mom[1] += m * A.vy; mom[2] += m * A.vz;
-      bad |= !isfinite(A.vx + A.vy + A.vz);
-    } else if (com) {
-      d.vx[a] = A.vx; d.vy[a] = A.vy; d.vz[a] = A.vz;
-    }
-    const float ex = from_fixed(A.x - d.refx[a]), ey = from_fixed(A.y - d.refy[a]), ez = from_fixed(A.z - d.refz[a]);
-    moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
+  } else if (u.kind == kUnitShake) {
+    cluster_velocities(sh, u, tol, bad);
   }
 }
 
-// SHAKE clusters out of line, so their larger frame does not cost the SETTLE
-// and free-atom paths registers.
-__device__ __noinline__ void integrate_shake_unit(const Dev& d, const SysDev& S, const UnitDev* up, long long step,
-                                                  bool com, float4 vc, double* mom, bool& moved, bool& bad) {
-  integrate_unit<kMaxClusterAtoms, kUnitShake>(d, S, up, step, com, vc, mom, moved, bad);
+__device__ __forceinline__ void store_constrained(Stage& sh, int e, float3 dp) {
+  if (sh.im[e] == 0.f) {
+    sh.cx[e] = sh.tx[e]; sh.cy[e] = sh.ty[e]; sh.cz[e] = sh.tz[e];
+  } else {
+    sh.cx[e] = to_fixed(dp.x); sh.cy[e] = to_fixed(dp.y); sh.cz[e] = to_fixed(dp.z);
+  }
+}
+
+__device__ __forceinline__ float3 staged_drift(const Stage& sh, int e) {
+  return make_float3(from_fixed(sh.tx[e]), from_fixed(sh.ty[e]), from_fixed(sh.tz[e]));
+}
+
+template <int NC>
+__device__ __forceinline__ void star_positions(Stage& sh, const UnitDev& u, float tol, bool& bad) {
+  const int e = u.base;
+  float3 dp[NC + 1];
+#pragma unroll
+  for (int k = 0; k <= NC; ++k) dp[k] = staged_drift(sh, e + k);
+  bad |= !shake_star<NC>(sh.x + e, sh.y + e, sh.z + e, sh.im + e, u.dist, dp, tol);
+#pragma unroll
+  for (int k = 0; k <= NC; ++k) store_constrained(sh, e + k, dp[k]);
+}
+
+__device__ __noinline__ void cluster_positions(Stage& sh, const UnitDev& u, float tol, bool& bad) {
+  const int e = u.base;
+  Atom at[kMaxClusterAtoms];
+  float3 dp[kMaxClusterAtoms];
+  for (int k = 0; k < u.na; ++k) {
+    at[k] = staged_atom(sh, e + k);
+    dp[k] = staged_drift(sh, e + k);
+  }
+  bad |= !shake(at, dp, u, tol);
+  for (int k = 0; k < u.na; ++k) store_constrained(sh, e + k, dp[k]);
+}
+
+// Position constraints of one unit: cx = constrained drift (the unconstrained
+// drift for free and massless atoms).
+__device__ void unit_positions(Stage& sh, const UnitDev& u, float tol, bool& bad) {
+  const int e = u.base;
+  if (u.kind == kUnitFree) {
+    sh.cx[e] = sh.tx[e]; sh.cy[e] = sh.ty[e]; sh.cz[e] = sh.tz[e];
+  } else if (u.kind == kUnitSettle) {
+    Atom at[3];
+    float3 dp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      at[k] = staged_atom(sh, e + k);
+      dp[k] = staged_drift(sh, e + k);
+    }
+    settle_positions(at, dp, u.dist[0], u.dist[1]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) store_constrained(sh, e + k, dp[k]);
+  } else if (u.kind == kUnitStar) {
+    switch (u.nc) {
+      case 1: star_positions<1>(sh, u, tol, bad); break;
+      case 2: star_positions<2>(sh, u, tol, bad); break;
+      default: star_positions<3>(sh, u, tol, bad); break;
+    }
+  } else {
+    cluster_positions(sh, u, tol, bad);
+  }
 }
 
 __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
+  __shared__ Stage sh;
   __shared__ double red[3][kThreads / 32];
   const int b = blockIdx.x;
   const int s = d.iblk_sys[b];
   const SysDev& S = d.sys[s];
+  const RunDev& R = d.run;
   const long long step = d.step[s];
   const bool com = S.com_freq > 0 && (step % S.com_freq) == 0;
   const float4 vc = com ? d.vcom[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const int natom = d.iblk_natom[b], atom0 = d.iblk_atom0[b], nunit = d.iblk_nunit[b];
+  const UnitDev* units = d.units + d.iblk_unit0[b];
+  const float dt = R.dt;
+  const bool lfm = R.integrator == 0;
+
+  int atom[kPerThread];
+  long long px[kPerThread], py[kPerThread], pz[kPerThread];
+  float vx[kPerThread], vy[kPerThread], vz[kPerThread], rx[kPerThread], ry[kPerThread], rz[kPerThread];
+  float im[kPerThread], n0[kPerThread], n1[kPerThread], n2[kPerThread];
+
+  // ---- atoms: load, clear the force slot, COM removal, kick, noise draw
+#pragma unroll
+  for (int j = 0; j < kPerThread; ++j) {
+    const int e = threadIdx.x + j * kThreads;
+    atom[j] = -1;
+    if (e >= natom) continue;
+    const int a = d.iatom[atom0 + e];
+    atom[j] = a;
+    px[j] = d.px[a]; py[j] = d.py[a]; pz[j] = d.pz[a];
+    vx[j] = d.vx[a]; vy[j] = d.vy[a]; vz[j] = d.vz[a];
+    rx[j] = d.rx[a]; ry[j] = d.ry[a]; rz[j] = d.rz[a];
+    im[j] = d.invm[a];
+    const int gs = S.slot_off + d.rank[a];
+    const float fx = from_fixed(static_cast<long long>(d.fx[gs]));
+    const float fy = from_fixed(static_cast<long long>(d.fy[gs]));
+    const float fz = from_fixed(static_cast<long long>(d.fz[gs]));
+    d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;  // consumer clears
+    if (com && im[j] > 0.f) { vx[j] -= vc.x; vy[j] -= vc.y; vz[j] -= vc.z; }
+    n0[j] = n1[j] = n2[j] = 0.f;
+    if (im[j] != 0.f) {
+      if (lfm) {
+        vx[j] += dt * im[j] * fx; vy[j] += dt * im[j] * fy; vz[j] += dt * im[j] * fz;
+        if (R.draw_noise) {
+          const unsigned p = static_cast<unsigned>(a - S.atom_off);
+          const uint2 key = make_uint2(R.seed, kThermostatDomain);
+          const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
+          const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
+          n0[j] = g0.x; n1[j] = g0.y; n2[j] = g1.x;
+        }
+      } else {
+        vx[j] += im[j] * fx * dt; vy[j] += im[j] * fy * dt; vz[j] += im[j] * fz * dt;
+      }
+    }
+    sh.x[e] = px[j]; sh.y[e] = py[j]; sh.z[e] = pz[j];
+    sh.vx[e] = vx[j]; sh.vy[e] = vy[j]; sh.vz[e] = vz[j];
+    sh.im[e] = im[j];
+  }
+  __syncthreads();
+
+  // ---- units: SETTLE-v / RATTLE (LFMiddle)
+  bool bad = false;
+  if (lfm && threadIdx.x < nunit) unit_velocities(sh, units[threadIdx.x], R.tolerance, bad);
+  __syncthreads();
+
+  // ---- atoms: drift (fixed point, residual feedback) with the thermostat between the halves
+  const float half = 0.5f * dt;
+#pragma unroll
+  for (int j = 0; j < kPerThread; ++j) {
+    const int e = threadIdx.x + j * kThreads;
+    if (atom[j] < 0) continue;
+    long long tx = 0, ty = 0, tz = 0;
+    if (im[j] != 0.f) {
+      vx[j] = sh.vx[e]; vy[j] = sh.vy[e]; vz[j] = sh.vz[e];
+      if (lfm) {
+        const float noise = R.noise_scale * sqrtf(R.kt * im[j]);
+        float lo;
+        tx = displace(vx[j] * half + rx[j], lo);
+        vx[j] = R.velocity_scale * vx[j] + noise * n0[j];
+        tx += displace(vx[j] * half + lo, rx[j]);
+        ty = displace(vy[j] * half + ry[j], lo);
+        vy[j] = R.velocity_scale * vy[j] + noise * n1[j];
+        ty += displace(vy[j] * half + lo, ry[j]);
+        tz = displace(vz[j] * half + rz[j], lo);
+        vz[j] = R.velocity_scale * vz[j] + noise * n2[j];
+        tz += displace(vz[j] * half + lo, rz[j]);
+      } else {
+        tx = displace(vx[j] * dt + rx[j], rx[j]);
+        ty = displace(vy[j] * dt + ry[j], ry[j]);
+        tz = displace(vz[j] * dt + rz[j], rz[j]);
+      }
+    }
+    sh.tx[e] = tx; sh.ty[e] = ty; sh.tz[e] = tz;
+  }
+  __syncthreads();
+
+  // ---- units: SETTLE / SHAKE on the drifted positions
+  if (threadIdx.x < nunit) unit_positions(sh, units[threadIdx.x], R.tolerance, bad);
+  __syncthreads();
+
+  // ---- atoms: velocity correction, store, rebuild test, momentum
+  const float idt = 1.f / dt;
   double mom[3] = {0, 0, 0};
-  bool moved = false, bad = false;
-  if (threadIdx.x < d.iblk_nunit[b]) {
-    const UnitDev* up = d.units + d.iblk_unit0[b] + threadIdx.x;
-    const int kind = up->kind;
-    if (kind == kUnitSettle) integrate_unit<3, kUnitSettle>(d, S, up, step, com, vc, mom, moved, bad);
-    else if (kind == kUnitFree) integrate_unit<1, kUnitFree>(d, S, up, step, com, vc, mom, moved, bad);
-    else integrate_shake_unit(d, S, up, step, com, vc, mom, moved, bad);
+  bool moved = false;
+#pragma unroll
+  for (int j = 0; j < kPerThread; ++j) {
+    const int e = threadIdx.x + j * kThreads;
+    const int a = atom[j];
+    if (a < 0) continue;
+    const long long cx = sh.cx[e], cy = sh.cy[e], cz = sh.cz[e];
+    if (im[j] != 0.f) {
+      if (lfm) {
+        vx[j] += idt * from_fixed(cx - sh.tx[e]);
+        vy[j] += idt * from_fixed(cy - sh.ty[e]);
+        vz[j] += idt * from_fixed(cz - sh.tz[e]);
+      } else {
+        vx[j] = idt * from_fixed(cx);
+        vy[j] = idt * from_fixed(cy);
+        vz[j] = idt * from_fixed(cz);
+      }
+      px[j] += cx; py[j] += cy; pz[j] += cz;
+      d.px[a] = px[j]; d.py[a] = py[j]; d.pz[a] = pz[j];
+      d.vx[a] = vx[j]; d.vy[a] = vy[j]; d.vz[a] = vz[j];
+      d.rx[a] = rx[j]; d.ry[a] = ry[j]; d.rz[a] = rz[j];
+      const double m = 1.0 / im[j];
+      mom[0] += m * vx[j]; mom[1] += m * vy[j]; mom[2] += m * vz[j];
+      bad |= !isfinite(vx[j] + vy[j] + vz[j]);
+    } else if (com) {
+      d.vx[a] = vx[j]; d.vy[a] = vy[j]; d.vz[a] = vz[j];
+    }
+    const float ex = from_fixed(px[j] - d.refx[a]), ey = from_fixed(py[j] - d.refy[a]),
+                ez = from_fixed(pz[j] - d.refz[a]);
+    moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
   }
   if (moved) atomicOr(&d.rebuild_flag[s], 1);
   if (bad) atomicAdd(&d.shake_failures[s], 1);
   block_sum3(mom, red);
   if (threadIdx.x == 0)
     for (int k = 0; k < 3; ++k) d.mom_partial[b * 3 + k] = mom[k];
-  finish_block(d, s, S, true);
+  finish_block(d, s, S, true, red);
 }
 
 // The momentum of the current velocities, for the first COM removal after the
@@ -458,20 +654,17 @@ __global__ void __launch_bounds__(kThreads) k_momentum(Dev d) {
   const int s = d.iblk_sys[b];
   const SysDev& S = d.sys[s];
   double mom[3] = {0, 0, 0};
-  if (threadIdx.x < d.iblk_nunit[b]) {
-    const UnitDev u = d.units[d.iblk_unit0[b] + threadIdx.x];
-    for (int k = 0; k < u.na; ++k) {
-      const int a = u.atom[k];
-      const float im = d.invm[a];
-      if (im == 0.f) continue;
-      const double m = 1.0 / im;
-      mom[0] += m * d.vx[a]; mom[1] += m * d.vy[a]; mom[2] += m * d.vz[a];
-    }
+  for (int e = threadIdx.x; e < d.iblk_natom[b]; e += kThreads) {
+    const int a = d.iatom[d.iblk_atom0[b] + e];
+    const float im = d.invm[a];
+    if (im == 0.f) continue;
+    const double m = 1.0 / im;
+    mom[0] += m * d.vx[a]; mom[1] += m * d.vy[a]; mom[2] += m * d.vz[a];
   }
   block_sum3(mom, red);
   if (threadIdx.x == 0)
     for (int k = 0; k < 3; ++k) d.mom_partial[b * 3 + k] = mom[k];
-  finish_block(d, s, S, false);
+  finish_block(d, s, S, false, red);
 }
 
 }  // namespace

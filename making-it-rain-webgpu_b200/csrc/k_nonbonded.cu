@@ -54,6 +54,24 @@ __device__ __forceinline__ void min_image(const SysDev& S, int& dx, int& dy, int
   }
 }
 
+// erfc(x) = exp(-x^2) P(u): P fits erfcx on x in [0, 3.6] as a degree-7
+// polynomial in u = 3.111 t - 2.111, t = 1/(1 + x/2) (fit_erfcx.py in this
+// directory derives the coefficients).  The kernel then needs one exponential
+// per pair, shared with the Gaussian term of the force.
+__device__ __forceinline__ float erfcx_poly(float x) {
+  const float t = __fdividef(1.0f, fmaf(0.5f, x, 1.0f));
+  const float u = fmaf(t, 3.1111111111111116f, -2.1111111111111116f);
+  float p = 2.8532681218254e-05f;
+  p = fmaf(p, u, 7.591772236827632e-05f);
+  p = fmaf(p, u, -0.0007059478100949549f);
+  p = fmaf(p, u, -0.0015110844839526505f);
+  p = fmaf(p, u, 0.01997081313517268f);
+  p = fmaf(p, u, 0.1346654154149635f);
+  p = fmaf(p, u, 0.40507415765174865f);
+  p = fmaf(p, u, 0.4424026315060776f);
+  return p;
+}
+
 template <bool ENERGY, bool TRICLINIC>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
                                            unsigned int mask, int lane, float& fix, float& fiy,
@@ -73,8 +91,8 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
       const float r = r2 * rinv;
       const float qq = qi.x * qj.x;
       const float x = alpha * r;
-      const float screened = erfcf(x);
       const float gauss = __expf(-x * x);
+      const float screened = gauss * erfcx_poly(x);
       const float coul = qq * screened * rinv;
       const float eps = qi.z * qj.z;
       const float sig = qi.y + qj.y;

@@ -204,8 +204,14 @@ __device__ __forceinline__ void spline_for(const SysDev& S, long long x, long lo
 }
 
 // ---------------------------------------------------------------- spread --
+// Slots are spatially sorted, so 32 consecutive slots would send 32 atoms'
+// 125 atomics to largely the same grid points at once and serialise in L2.
+// Lane l of warp w takes slot l * W + w instead (W = slots / 32): the 32 atoms
+// of one warp instruction sit far apart on the mesh.
 __global__ void __launch_bounds__(kThreads) k_spread(Dev d) {
-  for (int gs = blockIdx.x * blockDim.x + threadIdx.x; gs < d.n_slots; gs += gridDim.x * blockDim.x) {
+  const int W = d.n_slots >> 5;
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < d.n_slots; it += gridDim.x * blockDim.x) {
+    const int gs = (it & 31) * W + (it >> 5);
     const int a = d.order[gs];
     if (a < 0) continue;
     const float q = d.prm[gs].w;

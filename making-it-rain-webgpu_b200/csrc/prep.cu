@@ -206,6 +206,14 @@ int prepare_system(const mdb_system_desc& in, const mdb_state_desc& state, const
     return MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX;
   }
   h.alpha = in.alpha != 0 ? in.alpha : ewald_alpha(h.cutoff, h.tolerance);
+  // The pair kernel's screened-Coulomb polynomial is fitted for alpha r <= 3.6,
+  // which covers Ewald tolerances down to about 1e-6.
+  if (!(h.alpha > 0) || h.alpha * h.cutoff > 3.6) {
+    msg << "alpha * cutoff = " << h.alpha * h.cutoff
+        << " exceeds 3.6, the range the pair kernel's erfc is fitted on (Ewald tolerance below ~1e-6)";
+    error = msg.str();
+    return MDB_ERR_INVALID_ARGUMENT;
+  }
   for (int k = 0; k < 3; ++k) {
     int g = opt.mesh[k] > 0 ? opt.mesh[k] : in.grid[k];
     // potential.ts:79 -- the mesh from the box *diagonal*
