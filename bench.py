@@ -94,7 +94,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -104,10 +104,13 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self) -> dict:
+    def summary(self, start: float, end: float) -> dict:
+        """Samples taken between `start` and `end` (perf_counter seconds)."""
         sm, mx, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in self.lines:
+        for stamp, line in self.lines:
+            if not start <= stamp <= end:
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -150,7 +153,7 @@ def cpu_time_oracle(system, state, steps_hint: int, budget_s: float, threads: in
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--stride", type=int, default=100)
     ap.add_argument("--config", default=None)
@@ -200,6 +203,9 @@ def main() -> None:
     loop = steploop.StepLoop.from_parsed(system, state, opts)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
+    # clocks are sampled from before the warm-up, so nvidia-smi is running when
+    # the timed region starts; only samples inside that region are reported
+    clocks = ClockSampler(local).__enter__()
     # warm-up: graphs for the stride and the remainder, lists, clocks
     loop.run(args.warmup)
     stride = min(args.stride, args.steps)
@@ -216,12 +222,15 @@ def main() -> None:
 
     barrier()
     device_ms = 0.0
-    with ClockSampler(local) as clocks:
-        for s in strides:
-            flush_l2(flush)
-            torch.cuda.synchronize()
-            device_ms += loop.run_timed(s)
+    timed_start = time.perf_counter()
+    for s in strides:
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        device_ms += loop.run_timed(s)
     barrier()
+    timed_end = time.perf_counter()
+    time.sleep(0.3)  # let the sampler flush the last line of the region
+    clocks.__exit__(None, None, None)
     total_s = device_ms / 1000.0
     if world > 1:
         import torch.distributed as dist
@@ -299,7 +308,7 @@ def main() -> None:
                      "peak_source": "nominal FP32 issue rate, 148 SM x 128 lanes x 2 flop x 1.965 GHz",
                      "algorithmic": f"{FLOP_PER_PAIR:.0f} flop x {pairs} in-cutoff pairs per launch",
                      "hbm_peak_gbs": hbm_peak, "stages": stages},
-        "clocks": clocks.summary(),
+        "clocks": clocks.summary(timed_start, timed_end),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -192,7 +192,10 @@ typedef struct mdb_energies {
   double kinetic;              /* from the velocities as they are (kinetic.ts:31) */
   double temperature;          /* K, from `kinetic` and the constrained DoF */
   double degrees_of_freedom;
-  double virial[9];            /* sum of r (x) F over pairs, lattice-resolved; kJ/mol */
+  double virial[9];            /* W[3a+b] = sum r_a F_b = -dU/d eps_ab under the strain x -> (1+eps) x
+                                  of positions and box: pairs, exceptions, bonded terms, PME mesh,
+                                  dispersion and net-charge corrections (not restraints); kJ/mol.
+                                  No reference counterpart. */
   double pairs_within_cutoff;  /* non-excluded pairs inside the cutoff (count) */
 } mdb_energies;
 

@@ -87,6 +87,7 @@ struct Dev {
   const float* moduli;
   const float2* twiddles;
   double* mesh_partial;  // one per x-pass work item
+  double* mesh_virial;   // six per x-pass work item: xx yy zz xy xz yz
   const FftWork* fft_z; int n_fft_z;
   const FftWork* fft_y; int n_fft_y;
   const FftWork* fft_x; int n_fft_x;

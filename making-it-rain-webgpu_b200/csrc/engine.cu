@@ -611,6 +611,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.moduli = mod_dev;
   d.twiddles = tw_dev;
   TRY(alloc(e, "pme energy partials", d.mesh_partial, wx.size()));
+  TRY(alloc(e, "pme virial partials", d.mesh_virial, wx.size() * 6));
   FftWork* w_dev = nullptr;
   TRY(upload(e, "fft z work", w_dev, wz));
   d.fft_z = w_dev; d.n_fft_z = int(wz.size());
@@ -719,9 +720,14 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
     auto val = [&](int k) { return double((long long)en[k]) / 4294967296.0; };
     std::vector<double> mesh(e->n_mesh_items);
     cudaMemcpy(mesh.data(), d.mesh_partial, sizeof(double) * e->n_mesh_items, cudaMemcpyDeviceToHost);
-    double em = 0;
+    std::vector<double> mesh_vir(size_t(e->n_mesh_items) * 6);
+    cudaMemcpy(mesh_vir.data(), d.mesh_virial, sizeof(double) * mesh_vir.size(), cudaMemcpyDeviceToHost);
+    double em = 0, wm[6] = {0, 0, 0, 0, 0, 0};
     for (int k = 0; k < e->n_mesh_items; ++k)
-      if (e->fft_x_sys[k] == s) em += mesh[k];
+      if (e->fft_x_sys[k] == s) {
+        em += mesh[k];
+        for (int c = 0; c < 6; ++c) wm[c] += mesh_vir[size_t(k) * 6 + c];
+      }
     out->bond = val(kEBond);
     out->angle = val(kEAngle);
     out->torsion = val(kETorsion);
@@ -738,6 +744,16 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
     out->direct_group = out->direct_coulomb + out->direct_lj + out->exclusion_correction + out->exceptions +
                         out->dispersion;
     out->reciprocal_group = out->reciprocal_mesh + out->self_energy + out->net_charge;
+    // virial: pairs, exceptions and bonded terms from the device accumulators,
+    // the mesh sum's from the FP64 partials, and the 1/V corrections on the
+    // diagonal (restraints are left out: their anchors do not scale)
+    for (int k = 0; k < 9; ++k) out->virial[k] = val(kEVirial0 + k);
+    const int sym[6][2] = {{0, 0}, {4, 4}, {8, 8}, {1, 3}, {2, 6}, {5, 7}};
+    for (int c = 0; c < 6; ++c) {
+      out->virial[sym[c][0]] += wm[c];
+      if (sym[c][1] != sym[c][0]) out->virial[sym[c][1]] += wm[c];
+    }
+    for (int a = 0; a < 3; ++a) out->virial[4 * a] += out->dispersion + out->net_charge;
     out->potential = out->bond + out->angle + out->torsion + out->restraint + out->direct_group +
                      out->reciprocal_group;
     // kinetic energy from the velocities as they are (kinetic.ts:31)

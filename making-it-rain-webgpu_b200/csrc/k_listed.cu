@@ -53,6 +53,19 @@ __device__ __forceinline__ void add_energy(const Dev& d, const SysDev& S, int sl
   if (ENERGY) add_fixed(&d.energy[S.energy_base + slot], e);
 }
 
+// Virial contribution r (x) F of one atom of a term, r measured from the
+// term's first atom (energy evaluations only; a 3x3 row-major tensor).
+template <bool ENERGY>
+__device__ __forceinline__ void add_virial(const Dev& d, const SysDev& S, float3 r, float fx, float fy, float fz) {
+  if (!ENERGY) return;
+  unsigned long long* w = &d.energy[S.energy_base + kEVirial0];
+  const float rr[3] = {r.x, r.y, r.z}, ff[3] = {fx, fy, fz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) add_fixed(&w[3 * a + b], rr[a] * ff[b]);
+}
+
 template <bool ENERGY>
 __device__ void bond(const Dev& d, const BondDev& t) {
   const SysDev& S = d.sys[t.sys];
@@ -63,6 +76,7 @@ __device__ void bond(const Dev& d, const BondDev& t) {
   const float sc = t.k * dr / r;
   add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);
   add_force(d, S, t.b, -sc * v.x, -sc * v.y, -sc * v.z);
+  add_virial<ENERGY>(d, S, v, -sc * v.x, -sc * v.y, -sc * v.z);
 }
 
 template <bool ENERGY>
@@ -89,6 +103,8 @@ __device__ void angle(const Dev& d, const AngleDev& t) {
   add_force(d, S, t.a, f1x, f1y, f1z);
   add_force(d, S, t.c, f3x, f3y, f3z);
   add_force(d, S, t.b, -f1x - f3x, -f1y - f3y, -f1z - f3z);
+  add_virial<ENERGY>(d, S, v1, f1x, f1y, f1z);
+  add_virial<ENERGY>(d, S, v2, f3x, f3y, f3z);
 }
 
 template <bool ENERGY>
@@ -118,6 +134,15 @@ __device__ void torsion(const Dev& d, const TorsionDev& t) {
   add_force(d, S, t.b, -(1.f + ss) * f1x + tt * f4x, -(1.f + ss) * f1y + tt * f4y, -(1.f + ss) * f1z + tt * f4z);
   add_force(d, S, t.c, ss * f1x - (1.f + tt) * f4x, ss * f1y - (1.f + tt) * f4y, ss * f1z - (1.f + tt) * f4z);
   add_force(d, S, t.d, f4x, f4y, f4z);
+  if (ENERGY) {
+    const float3 rc = make_float3(b1.x + b2.x, b1.y + b2.y, b1.z + b2.z);
+    const float3 rd = make_float3(rc.x + b3.x, rc.y + b3.y, rc.z + b3.z);
+    add_virial<ENERGY>(d, S, b1, -(1.f + ss) * f1x + tt * f4x, -(1.f + ss) * f1y + tt * f4y,
+                       -(1.f + ss) * f1z + tt * f4z);
+    add_virial<ENERGY>(d, S, rc, ss * f1x - (1.f + tt) * f4x, ss * f1y - (1.f + tt) * f4y,
+                       ss * f1z - (1.f + tt) * f4z);
+    add_virial<ENERGY>(d, S, rd, f4x, f4y, f4z);
+  }
 }
 
 template <bool ENERGY>
@@ -150,6 +175,7 @@ __device__ void exception(const Dev& d, const ExceptionDev& t) {
     const float sc = dEdR * rinv;
     add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);
     add_force(d, S, t.b, -sc * v.x, -sc * v.y, -sc * v.z);
+    add_virial<ENERGY>(d, S, v, -sc * v.x, -sc * v.y, -sc * v.z);
   }
 }
 

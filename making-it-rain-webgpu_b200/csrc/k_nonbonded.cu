@@ -76,7 +76,7 @@ template <bool ENERGY, bool TRICLINIC>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
                                            unsigned int mask, int lane, float& fix, float& fiy,
                                            float& fiz, float& fjx, float& fjy, float& fjz,
-                                           float& ecoul, float& elj, int& pairs) {
+                                           float& ecoul, float& elj, int& pairs, float* vir) {
   const float alpha = S.alpha, a2sp = S.alpha_2_sqrtpi, cut2 = S.cut2, inv = S.pc_inv;
 #pragma unroll 4
   for (int k = 0; k < 32; ++k) {
@@ -111,6 +111,13 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
         ecoul += coul;
         elj += 4.0f * eps * (s12 - s6);
         pairs += 1;
+        // virial (r_i - r_j) (x) F_i = -fs r (x) r, symmetric: xx yy zz xy xz yz
+        vir[0] -= fs * rx * rx;
+        vir[1] -= fs * ry * ry;
+        vir[2] -= fs * rz * rz;
+        vir[3] -= fs * rx * ry;
+        vir[4] -= fs * rx * rz;
+        vir[5] -= fs * ry * rz;
       }
     }
     const int src = (lane + 1) & 31;
@@ -141,6 +148,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   long long aix = 0, aiy = 0, aiz = 0;
   int cur_row = -1;
   long long ecoul64 = 0, elj64 = 0, pairs64 = 0;
+  long long vir64[6] = {0, 0, 0, 0, 0, 0};
 
   auto flush_row = [&]() {
     if (cur_row >= 0) {
@@ -153,6 +161,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
     }
     aix = aiy = aiz = 0;
   };
+  auto base_of = [&](int sys) { return d.sys[sys].energy_base; };
   auto flush_energy = [&](int sys) {
     if (ENERGY) {
       const long long c = warp_sum64(ecoul64), l = warp_sum64(elj64), p = warp_sum64(pairs64);
@@ -161,6 +170,17 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
         add_fixed64(&d.energy[base + kECoulomb], c);
         add_fixed64(&d.energy[base + kELj], l);
         add_fixed64(&d.energy[base + kEPairs], p);
+      }
+      // slots: row-major 3x3, the symmetric pair tensor written to both halves
+      const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const long long v = warp_sum64(vir64[k]);
+        if (lane == 0) {
+          add_fixed64(&d.energy[base_of(sys) + kEVirial0 + slot[k]], v);
+          if (mirror[k] >= 0) add_fixed64(&d.energy[base_of(sys) + kEVirial0 + mirror[k]], v);
+        }
+        vir64[k] = 0;
       }
       ecoul64 = elj64 = pairs64 = 0;
     }
@@ -185,11 +205,12 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
     const float4 qj = d.prm[gj];
     const unsigned int mask = d.masks[ti * 32 + lane];
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
+    float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int np = 0;
     if (S.triclinic)
-      tile_pairs<ENERGY, true>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np);
+      tile_pairs<ENERGY, true>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np, vir);
     else
-      tile_pairs<ENERGY, false>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np);
+      tile_pairs<ENERGY, false>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np, vir);
     aix += to_fixed(fix);
     aiy += to_fixed(fiy);
     aiz += to_fixed(fiz);
@@ -202,6 +223,8 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
       ecoul64 += to_fixed(ec);
       elj64 += to_fixed(el);
       pairs64 += np;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) vir64[k] += to_fixed(vir[k]);
     }
   }
   flush_row();

@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_y(Dev d, int sign) {
 template <bool ENERGY>
 __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   extern __shared__ float2 smem[];
-  __shared__ double partial[kThreads / 32];
+  __shared__ double partial[7][kThreads / 32];
   const FftWork w = d.fft_x[blockIdx.x];
   const SysDev& S = d.sys[w.sys];
   const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   float2* other = R == A ? B : A;
   // Convolution (pme-convolve.wgsl:34; pme.ts:160-209) on the half spectrum.
   double energy = 0.0;
+  double vir[6] = {0, 0, 0, 0, 0, 0};  // xx yy zz xy xz yz
   const int my = w.a;
   const int mb = my <= Ky / 2 ? my : my - Ky;
   const float* modx = d.moduli + S.mod_off;
@@ -319,18 +320,29 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
     const int ma = mx <= Kx / 2 ? mx : mx - Kx;
     const int mc = kz;  // kz <= Kz/2 on the half spectrum
     float2 v = R[i];
-    float factor = 0.f;
+    float factor = 0.f, kx = 0.f, ky = 0.f, kzv = 0.f, k2 = 1.f;
     if (mx != 0 || my != 0 || kz != 0) {
       const float* M = S.inv_f;
-      const float kx = two_pi * ma * M[0];
-      const float ky = two_pi * (ma * M[3] + mb * M[4]);
-      const float kzv = two_pi * (ma * M[6] + mb * M[7] + mc * M[8]);
-      const float k2 = kx * kx + ky * ky + kzv * kzv;
+      kx = two_pi * ma * M[0];
+      ky = two_pi * (ma * M[3] + mb * M[4]);
+      kzv = two_pi * (ma * M[6] + mb * M[7] + mc * M[8]);
+      k2 = kx * kx + ky * ky + kzv * kzv;
       factor = S.pme_pref * expf(k2 * S.exp_scale) / (k2 * modx[mx] * mody[my] * modz[kz]);
     }
     if (ENERGY) {
       const double weight = (kz == 0 || (2 * kz == Kz)) ? 1.0 : 2.0;
-      energy += weight * static_cast<double>(factor) * (static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y);
+      const double ek =
+          weight * static_cast<double>(factor) * (static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y);
+      energy += ek;
+      // -dE_k/d eps_ab = E_k (delta_ab - 2 k_a k_b (1/k^2 + 1/(4 alpha^2)))
+      const double c = 2.0 * (1.0 / static_cast<double>(k2) - static_cast<double>(S.exp_scale));
+      const double ka = kx, kb = ky, kc = kzv;
+      vir[0] += ek * (1.0 - c * ka * ka);
+      vir[1] += ek * (1.0 - c * kb * kb);
+      vir[2] += ek * (1.0 - c * kc * kc);
+      vir[3] -= ek * c * ka * kb;
+      vir[4] -= ek * c * ka * kc;
+      vir[5] -= ek * c * kb * kc;
     }
     v.x *= 2.f * factor;
     v.y *= 2.f * factor;
@@ -344,14 +356,19 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   }
   if (ENERGY) {
     // fixed-order block reduction in FP64: deterministic
+    double val[7] = {energy, vir[0], vir[1], vir[2], vir[3], vir[4], vir[5]};
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) energy += __shfl_xor_sync(0xffffffffu, energy, o);
-    if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = energy;
+    for (int c = 0; c < 7; ++c) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) val[c] += __shfl_xor_sync(0xffffffffu, val[c], o);
+      if ((threadIdx.x & 31) == 0) partial[c][threadIdx.x >> 5] = val[c];
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 7) {
       double total = 0.0;
-      for (int k = 0; k < (blockDim.x >> 5); ++k) total += partial[k];
-      d.mesh_partial[blockIdx.x] = total;
+      for (int k = 0; k < (blockDim.x >> 5); ++k) total += partial[threadIdx.x][k];
+      if (threadIdx.x == 0) d.mesh_partial[blockIdx.x] = total;
+      else d.mesh_virial[blockIdx.x * 6 + threadIdx.x - 1] = total;
     }
   }
 }

@@ -352,7 +352,21 @@ std::unordered_set<uint64_t> exclusion_set(const mdb_system_desc* s) {
 
 // --------------------------------------------------------- nonbonded ------
 // src/reference/forces/nonbonded.ts:279 -- one non-excluded pair.
-struct PairAcc { double coulomb = 0, lj = 0; int64_t pairs = 0; };
+// Virial tensor W[3a+b] = sum r_a F_b over every interaction (r the
+// separation, F the force on the atom it points from) = -dU/d eps_ab for the
+// affine strain x -> (1 + eps) x of positions and box.  Filled only while
+// orc_potential_virial runs; position restraints are left out (their anchors
+// do not move with the box).  No reference counterpart: the reference has no
+// virial.
+double* g_virial = nullptr;
+
+inline void add_virial(double* w, double rx, double ry, double rz, double fx, double fy, double fz) {
+  const double r[3] = {rx, ry, rz}, f[3] = {fx, fy, fz};
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) w[3 * a + b] += r[a] * f[b];
+}
+
+struct PairAcc { double coulomb = 0, lj = 0; int64_t pairs = 0; double vir[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}; };
 
 inline void pair_interaction(const mdb_system_desc* s, const double* pos, const double* box,
                              double alpha, double cut2, int i, int j, double* forces,
@@ -385,6 +399,11 @@ inline void pair_interaction(const mdb_system_desc* s, const double* pos, const 
     forces[3 * j] -= sc * dx;
     forces[3 * j + 1] -= sc * dy;
     forces[3 * j + 2] -= sc * dz;
+  }
+  if (g_virial) {
+    // pair (i, j): r_i - r_j = -d, force on i = (dEdR / r) d
+    const double sc = dEdR / r;
+    add_virial(acc.vir, -dx, -dy, -dz, sc * dx, sc * dy, sc * dz);
   }
   if (coulomb != 0 || lj != 0) acc.pairs++;
   acc.coulomb += coulomb;
@@ -420,6 +439,10 @@ void exception_terms(const mdb_system_desc* s, const double* pos, const double* 
       const double s6 = std::pow(sig * sig / r2, 3), s12 = s6 * s6;
       exceptions += 4 * eps * (s12 - s6);
       dEdR += (4 * eps / r) * (6 * s6 - 12 * s12);
+    }
+    if (g_virial && dEdR != 0) {
+      const double sc = dEdR / r;
+      add_virial(g_virial, -dx, -dy, -dz, sc * dx, sc * dy, sc * dz);
     }
     if (forces && dEdR != 0) {
       const double sc = dEdR / r;
@@ -569,6 +592,7 @@ void direct_pairs(const mdb_system_desc* s, const double* pos, const double* box
     total.coulomb += ta[t].coulomb;
     total.lj += ta[t].lj;
     total.pairs += ta[t].pairs;
+    for (int k = 0; k < 9; ++k) total.vir[k] += ta[t].vir[k];
     if (forces)
       for (size_t k = 0; k < size_t(3) * n; ++k) forces[k] += tf[t][k];
   }
@@ -634,6 +658,12 @@ double reciprocal_space(const mdb_system_desc* s, const double* pos, const doubl
         const double modulus = mx_[x] * my_[y] * mz_[z];
         const double factor = (pref * std::exp(k2 * expScale)) / (k2 * modulus);
         energy += factor * std::norm(v);
+        if (g_virial) {
+          // -dE_k/d eps_ab = E_k (delta_ab - 2 k_a k_b (1/k^2 + 1/(4 alpha^2)))
+          const double ek = factor * std::norm(v), c = 2 * (1 / k2 - expScale);
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) g_virial[3 * a + b] += ek * ((a == b ? 1.0 : 0.0) - c * k[a] * k[b]);
+        }
         v *= 2 * factor;
       }
     }
@@ -680,6 +710,7 @@ double harmonic_bonds(const mdb_system_desc* s, const double* pos, double* f) {
       const double sc = k * dr / r;
       f[a] += sc * dx; f[a + 1] += sc * dy; f[a + 2] += sc * dz;
       f[b] -= sc * dx; f[b + 1] -= sc * dy; f[b + 2] -= sc * dz;
+      if (g_virial) add_virial(g_virial, dx, dy, dz, -sc * dx, -sc * dy, -sc * dz);
     }
   }
   return e;
@@ -708,6 +739,10 @@ double harmonic_angles(const mdb_system_desc* s, const double* pos, double* f) {
     f[a] += f1x; f[a + 1] += f1y; f[a + 2] += f1z;
     f[c] += f3x; f[c + 1] += f3y; f[c + 2] += f3z;
     f[b] -= f1x + f3x; f[b + 1] -= f1y + f3y; f[b + 2] -= f1z + f3z;
+    if (g_virial) {
+      add_virial(g_virial, v1x, v1y, v1z, f1x, f1y, f1z);
+      add_virial(g_virial, v2x, v2y, v2z, f3x, f3y, f3z);
+    }
   }
   return e;
 }
@@ -744,6 +779,13 @@ double periodic_torsions(const mdb_system_desc* s, const double* pos, double* f)
     f[c] += ss * f1x - (1 + tt) * f4x; f[c + 1] += ss * f1y - (1 + tt) * f4y;
     f[c + 2] += ss * f1z - (1 + tt) * f4z;
     f[d] += f4x; f[d + 1] += f4y; f[d + 2] += f4z;
+    if (g_virial) {
+      add_virial(g_virial, b1x, b1y, b1z, -(1 + ss) * f1x + tt * f4x, -(1 + ss) * f1y + tt * f4y,
+                 -(1 + ss) * f1z + tt * f4z);
+      add_virial(g_virial, b1x + b2x, b1y + b2y, b1z + b2z, ss * f1x - (1 + tt) * f4x,
+                 ss * f1y - (1 + tt) * f4y, ss * f1z - (1 + tt) * f4z);
+      add_virial(g_virial, b1x + b2x + b3x, b1y + b2y + b3y, b1z + b2z + b3z, f4x, f4y, f4z);
+    }
   }
   return e;
 }
@@ -1163,6 +1205,8 @@ Potential evaluate(const mdb_system_desc* s, const double* pos, const double* bo
     e.direct_coulomb = acc.coulomb;
     e.direct_lj = acc.lj;
     e.pairs_within_cutoff = acc.pairs;
+    if (g_virial)
+      for (int k = 0; k < 9; ++k) g_virial[k] += acc.vir[k];
     exception_terms(s, pos, box.data(), alpha, forces, e.exclusion_correction, e.exceptions);
     const double volume = box_volume(box.data());
     e.dispersion = s->use_dispersion_correction ? dispersion_correction(s, volume) : 0;
@@ -1175,6 +1219,8 @@ Potential evaluate(const mdb_system_desc* s, const double* pos, const double* bo
     e.self_energy = self_energy(s, alpha);
     e.net_charge = net_charge_correction(s, alpha, volume);
     e.reciprocal_group = e.reciprocal_mesh + e.self_energy + e.net_charge;
+    if (g_virial)  // both scale as 1/V
+      for (int a = 0; a < 3; ++a) g_virial[4 * a] += e.dispersion + e.net_charge;
   }
   e.potential = e.bond + e.angle + e.torsion + e.restraint + e.direct_group + e.reciprocal_group;
   return out;
@@ -1331,6 +1377,22 @@ int32_t orc_potential(const mdb_system_desc* sys, const double* positions, const
                       const int32_t* grid, int32_t threads, int32_t naive_direct, double* forces,
                       orc_energies* out) {
   Potential p = evaluate(sys, positions, box, grid, threads, naive_direct != 0, forces);
+  if (out) *out = p.e;
+  return p.status;
+}
+
+int32_t orc_potential_virial(const mdb_system_desc* sys, const double* positions, const double box[9],
+                             const int32_t* grid, int32_t threads, double* forces, orc_energies* out,
+                             double virial[9]) {
+  std::vector<double> scratch;
+  if (!forces) {
+    scratch.assign(3 * size_t(sys->n_particles), 0.0);
+    forces = scratch.data();
+  }
+  std::fill(virial, virial + 9, 0.0);
+  g_virial = virial;
+  Potential p = evaluate(sys, positions, box, grid, threads, false, forces);
+  g_virial = nullptr;
   if (out) *out = p.e;
   return p.status;
 }

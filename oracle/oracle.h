@@ -83,6 +83,15 @@ int32_t orc_potential(const mdb_system_desc* sys, const double* positions,
                       const double box[9], const int32_t* grid, int32_t threads,
                       int32_t naive_direct, double* forces, orc_energies* out);
 
+/* The same evaluation plus the virial tensor W[3a+b] = sum r_a F_b
+ * (= -dU/d eps_ab under the affine strain x -> (1 + eps) x of positions and
+ * box), pairs, exceptions, bonded terms, the PME mesh sum and the 1/V
+ * dispersion and net-charge corrections; restraints excluded.  No reference
+ * counterpart.  Not thread-safe (a module-level accumulator). */
+int32_t orc_potential_virial(const mdb_system_desc* sys, const double* positions, const double box[9],
+                             const int32_t* grid, int32_t threads, double* forces, orc_energies* out,
+                             double virial[9]);
+
 /* Exact Ewald reciprocal sum (src/reference/forces/ewald.ts), k-space only. */
 int32_t orc_ewald_reciprocal(const mdb_system_desc* sys, const double* positions,
                              const double box[9], double alpha, int32_t kmax,

@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
         "orc_bspline_moduli": (None, [C.c_int32, _dp]),
         "orc_potential": (C.c_int32, [_SD, _dp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, _dp,
                                       C.POINTER(Energies)]),
+        "orc_potential_virial": (C.c_int32, [_SD, _dp, _dp, C.POINTER(C.c_int32), C.c_int32, _dp,
+                                             C.POINTER(Energies), _dp]),
         "orc_ewald_reciprocal": (C.c_int32, [_SD, _dp, _dp, C.c_double, C.c_int32, _dp, _dp]),
         "orc_split_counts": (C.c_int32, [_SD] + [C.POINTER(C.c_int32)] * 4),
         "orc_degrees_of_freedom": (C.c_double, [_SD]),
@@ -124,6 +126,21 @@ def potential(system: System, positions, box=None, grid=None, threads: int = 1, 
     if status != 0:
         raise RuntimeError(f"oracle potential failed with status {status}")
     return e.as_dict(), (f.reshape(-1, 3) if f is not None else None)
+
+
+def potential_virial(system: System, positions, box=None, grid=None, threads: int = 1):
+    """Energies, forces (N, 3) and the 3x3 virial W_ab = sum r_a F_b = -dU/d eps_ab."""
+    handle = system.desc()
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1))
+    b = _box(system.box if box is None else box)
+    f = np.zeros_like(pos)
+    w = np.zeros(9)
+    e = Energies()
+    g = (C.c_int32 * 3)(*(grid if grid is not None else (0, 0, 0)))
+    status = lib().orc_potential_virial(handle.pointer(), _p(pos), _p(b), g, threads, _p(f), C.byref(e), _p(w))
+    if status != 0:
+        raise RuntimeError(f"oracle potential failed with status {status}")
+    return e.as_dict(), f.reshape(-1, 3), w.reshape(3, 3)
 
 
 def ewald_reciprocal(system: System, positions, alpha: float, kmax: int, box=None):
