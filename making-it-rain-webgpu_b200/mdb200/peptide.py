@@ -294,3 +294,82 @@ def parameterise(atoms, constrain_hbonds: bool = True, cutoff: float = 1.0, ewal
 
 def helix(sequence, phi=-57.0, psi=-47.0):
     return parameterise(build_chain(sequence, phi, psi))
+
+
+# -------------------------------------------------------------- random coil --
+# The 27k-atom workload's solute: a seeded 60-residue Ala-Gly-Lys-Glu chain
+# whose backbone angles come from the extended basins (beta, polyproline II)
+# and right-handed alpha turns, grown so that no two atoms of residues two or
+# more apart clash and its bounding sphere fits a truncated octahedron of
+# about 7.15 nm at OpenMM's 1.0 nm padding (src/prep/solvate.ts:390).
+AGKE60 = ("ALA", "GLY", "LYS", "GLU") * 15
+COIL_BASINS = np.array([[-120.0, 135.0], [-70.0, 145.0], [-63.0, -43.0]])
+COIL_WEIGHTS = np.array([0.33, 0.22, 0.45])
+COIL_DATA = Path(__file__).resolve().parent / "data" / "coil_angles.json"
+
+
+def bounding_radius(xyz) -> float:
+    """Radius of the sphere about the bounding box centre (solvate.ts:364)."""
+    xyz = np.asarray(xyz)
+    centre = 0.5 * (xyz.min(axis=0) + xyz.max(axis=0))
+    return float(np.linalg.norm(xyz - centre, axis=1).max())
+
+
+def _clashes(atoms, new_residue: int) -> bool:
+    """Does any atom of `new_residue` come too close to an atom of a residue at
+    least two before it (0.30 nm between heavy atoms, 0.20 nm otherwise)?"""
+    xyz = np.array([a[3] for a in atoms])
+    res = np.array([a[0] for a in atoms])
+    heavy = np.array([not a[2].startswith("H") for a in atoms])
+    new = res == new_residue
+    old = res <= new_residue - 2
+    if not old.any():
+        return False
+    d = np.linalg.norm(xyz[new][:, None] - xyz[old][None], axis=-1)
+    limit = np.where(heavy[new][:, None] & heavy[old][None], 0.30, 0.20)
+    return bool((d < limit).any())
+
+
+def coil_angles(sequence, seed: int, min_radius: float = 2.95, max_radius: float = 3.1, confine: float = 3.0,
+                tries: int = 24, budget: int = 20000):
+    """Per-residue (phi, psi) of a clash-free coil, grown with backtracking.
+
+    Residue k takes up to `tries` basin draws; a draw is kept when none of the
+    residue's atoms clashes with residues two or more before it and all stay
+    within `confine` nm of the first atom; when every draw fails the growth
+    backs up two residues.  A finished chain whose bounding radius exceeds
+    `max_radius` or falls short of `min_radius` (or whose caps clash) is
+    regrown.  Deterministic for a seed.
+    """
+    rng = np.random.default_rng(seed)
+    n = len(sequence)
+    phi, psi = np.zeros(n), np.zeros(n)
+    draws = 0
+    while draws < budget:
+        k = 0
+        while k < n and draws < budget:
+            placed = False
+            for _ in range(tries):
+                draws += 1
+                phi[k], psi[k] = COIL_BASINS[rng.choice(3, p=COIL_WEIGHTS)] + rng.normal(0, 12, 2)
+                atoms = [a for a in build_chain(sequence[:k + 1], phi[:k + 1], psi[:k + 1]) if a[0] <= k + 1]
+                xyz = np.array([a[3] for a in atoms if a[0] == k + 1])
+                if np.linalg.norm(xyz - atoms[0][3], axis=1).max() > confine or _clashes(atoms, k + 1):
+                    continue
+                placed = True
+                break
+            k = k + 1 if placed else max(0, k - 2)
+        if k < n:
+            break
+        atoms = build_chain(sequence, phi, psi)
+        xyz = np.array([a[3] for a in atoms])
+        if min_radius <= bounding_radius(xyz) <= max_radius and not _clashes(atoms, n + 1):
+            return phi.copy(), psi.copy()
+    raise RuntimeError(f"no clash-free coil of radius {min_radius}-{max_radius} nm after {draws} draws")
+
+
+def coil():
+    """The parameterised AGKE60 coil with the angles data/make_coil.py found
+    and stored in data/coil_angles.json (the seed is recorded there)."""
+    table = json.loads(COIL_DATA.read_text())
+    return parameterise(build_chain(tuple(table["sequence"]), np.array(table["phi"]), np.array(table["psi"])))

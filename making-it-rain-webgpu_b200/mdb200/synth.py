@@ -243,3 +243,16 @@ def config_peptide_12k(seed: int = 1):
 
     solute, positions = peptide.helix(["ALA"] * 20)
     return solvated(solute, positions, width=5.0, seed=seed, grid=(50, 50, 50))
+
+
+def config_octahedron_27k(seed: int = 1):
+    """60-residue (Ala-Gly-Lys-Glu)15 coil with ACE/NME caps, ff14SB, HBond
+    constraints, in a TIP3P truncated octahedron sized by OpenMM's padding
+    rule at 1.0 nm (src/prep/solvate.ts:390: width = 2 R + padding, R the
+    bounding-sphere radius), 0.15 M NaCl; mesh by the reference's rule from
+    the box diagonal.  About 27,000 atoms."""
+    from . import peptide
+
+    solute, positions = peptide.coil()
+    width = max(2.0 * peptide.bounding_radius(positions) + 1.0, 2.0)
+    return solvated(solute, positions, width=width, shape="octahedron", seed=seed)

@@ -221,3 +221,35 @@ def test_peptide_one_step_with_shake(mdb, oracle, peptide):
     d = np.linalg.norm(p[system.constraint_p1] - p[system.constraint_p2], axis=1)
     assert np.max(np.abs(d / system.constraint_distance - 1)) < 2e-6
     loop.destroy()
+
+
+@pytest.fixture(scope="module")
+def octahedron():
+    from mdb200 import synth
+
+    return synth.config_octahedron_27k()
+
+
+def test_octahedron_10k_steps_then_groups_match_oracle(mdb, oracle, octahedron):
+    """The 27k-atom truncated octahedron: run 10,000 LFMiddle steps, then the
+    per-force-group energies and forces at the final configuration against
+    the f64 oracle evaluated on the same positions."""
+    system, state = octahedron
+    loop = make_loop(mdb, system, state, seed=5)
+    loop.run(10000)
+    assert loop.steps == state.step + 10000
+    e, f = loop.evaluate()
+    pos = loop.positions()
+    mesh = tuple(loop.mesh())
+    want, wf = oracle.potential(system, pos, box=loop.box_vectors(), grid=mesh, threads=8)
+    err = rel_rms(f, wf)
+    print("octahedron after 10k steps: force rel RMS", err, "T", e["temperature"], "mesh", mesh)
+    assert err <= FORCE_REL_RMS, err
+    for key in ("bond", "angle", "torsion"):
+        assert abs(e[key] - want[key]) <= 1e-5 * abs(want[key]) + 1e-3, (key, e[key], want[key])
+    assert abs(e["direct_group"] - want["direct_group"]) <= 1e-4 * abs(want["direct_group"])
+    assert abs(e["reciprocal_group"] - want["reciprocal_group"]) <= 1e-5 * abs(want["reciprocal_group"])
+    assert abs(e["exceptions"] - want["exceptions"]) <= 1e-5 * abs(want["exceptions"])
+    assert e["pairs_within_cutoff"] == want["pairs_within_cutoff"]
+    assert 200.0 < e["temperature"] < 400.0
+    loop.destroy()

@@ -146,3 +146,27 @@ def test_ions_for_concentration():
 
     assert synth.ions_for(125.0, 0.15) == 11
     assert synth.ions_for(1000.0, 0.15) == 90
+
+
+def test_octahedron_workload_matches_the_configuration(oracle):
+    """60-residue (AGKE)15 coil, truncated octahedron at 1.0 nm padding, ~27k atoms."""
+    from mdb200 import peptide, synth
+
+    solute, x = peptide.coil()
+    radius = peptide.bounding_radius(x)
+    assert 2.95 <= radius <= 3.1
+    system, state = synth.config_octahedron_27k()
+    box = np.asarray(state.box)
+    width = 2 * radius + 1.0  # solvate.ts:390
+    assert np.allclose(box, synth.box_vectors("octahedron", width))
+    assert 25000 <= system.particle_count <= 29000
+    assert abs(system.nonbonded.charge.sum()) < 1e-9
+    names = [a[2] for a in peptide.build_chain(peptide.AGKE60, 0.0, 0.0)]
+    assert solute.particle_count == len(names) == 822
+    # no clashes: every solute pair at least two residues apart keeps its distance
+    res = np.array([a[0] for a in peptide.build_chain(peptide.AGKE60, 0.0, 0.0)])
+    d = np.linalg.norm(x[:, None] - x[None], axis=-1)
+    assert d[np.abs(res[:, None] - res[None]) >= 2].min() >= 0.2
+    status, (settle, iterative, largest_atoms, largest_constraints) = oracle.split_counts(system)
+    assert status == 0 and iterative > 0
+    assert largest_atoms <= 4 and largest_constraints <= 3
