@@ -43,6 +43,9 @@ NS_PER_DAY_PER_STEP_PER_S = TIME_STEP_PS * 86400 / 1000.0
 # functions = 1), the tally written down with the roofline in DESIGN.md.
 FLOP_PER_PAIR = 74.0
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate at max SM clock
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_nonbonded launch, from
+# the ncu capture summarised in profiles/nonbonded_peptide12k.md
+NB_TRAFFIC = {"peptide-12k": 4344832}
 
 
 def workload(name: str, seed: int):
@@ -150,10 +153,32 @@ def cpu_time_oracle(system, state, steps_hint: int, budget_s: float, threads: in
     return n / elapsed, n, elapsed
 
 
+def cpu_rate(config: str, steps_hint: int, budget_s: float, threads: int):
+    """ns/day of the oracle on the workload, and a description of the sample.
+    For the ensemble: one step of every system, summed into one ensemble step."""
+    if config == "ensemble-64":
+        from mdb200 import synth
+        from oracle import oracle as orc
+
+        members = synth.config_ensemble_64(seed=1)
+        elapsed = 0.0
+        for system, state, _ in members:
+            t = time.perf_counter()
+            orc.run(system, state, 1, seed=1, threads=threads)
+            elapsed += time.perf_counter() - t
+        value = len(members) / elapsed * NS_PER_DAY_PER_STEP_PER_S
+        return value, 1, elapsed, (f"one MD step of each of the {len(members)} systems ({elapsed:.1f} s), "
+                                   "system-ns/day summed")
+    system, state, _ = workload(config, seed=1)
+    sps, n, elapsed = cpu_time_oracle(system, state, steps_hint, budget_s, threads)
+    return sps * NS_PER_DAY_PER_STEP_PER_S, n, elapsed, f"{n} MD steps of the same workload in {elapsed:.1f} s"
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=12000)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps; default 12000 (about 2 s on one system), 400 for the ensemble")
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--stride", type=int, default=100)
     ap.add_argument("--config", default=None)
@@ -163,6 +188,8 @@ def main() -> None:
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     config = args.config or default_config()
+    if args.steps is None:
+        args.steps = 400 if config == "ensemble-64" else 12000
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -171,18 +198,17 @@ def main() -> None:
     if args.impl == "reference":
         if rank != 0:
             return
-        system, state, cfg = workload(config, seed=1)
         threads = os.cpu_count() or 1
-        sps, n, elapsed = cpu_time_oracle(system, state, args.steps, min(args.cpu_budget * 6, 240.0), threads)
-        value = sps * NS_PER_DAY_PER_STEP_PER_S
+        value, n, elapsed, sample = cpu_rate(config, args.steps, min(args.cpu_budget * 6, 240.0), threads)
+        cfg = {"workload": config} if config == "ensemble-64" else workload(config, seed=1)[2]
         print(json.dumps({
             "impl": "reference", "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": args.gpus,
-            "steps": n, "warmup": 1, "ms_per_step": 1000.0 / sps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "steps": n, "warmup": 1, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {**cfg, "parallelism": "host threads", "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port",
-                             "sample": f"{n} full MD steps of the same workload (f64 C++ restatement of "
-                                       f"src/reference; the TypeScript original needs Node, absent here)"},
+                             "sample": sample + " (f64 C++ restatement of src/reference; the TypeScript "
+                                                "original needs Node, absent here)"},
             "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
         return
@@ -198,21 +224,6 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from mdb200 import steploop
 
-    system, state, cfg = workload(config, seed=1 + rank)
-    opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride)
-    loop = steploop.StepLoop.from_parsed(system, state, opts)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    # clocks are sampled from before the warm-up, so nvidia-smi is running when
-    # the timed region starts; only samples inside that region are reported
-    clocks = ClockSampler(local).__enter__()
-    # warm-up: graphs for the stride and the remainder, lists, clocks
-    loop.run(args.warmup)
-    stride = min(args.stride, args.steps)
-    strides = [stride] * (args.steps // stride) + ([args.steps % stride] if args.steps % stride else [])
-    for s in set(strides):
-        loop.run(s)
-
     def barrier():
         if world > 1:
             import torch.distributed as dist
@@ -220,78 +231,150 @@ def main() -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    barrier()
-    device_ms = 0.0
-    timed_start = time.perf_counter()
-    for s in strides:
-        flush_l2(flush)
-        torch.cuda.synchronize()
-        device_ms += loop.run_timed(s)
-    barrier()
-    timed_end = time.perf_counter()
-    time.sleep(0.3)  # let the sampler flush the last line of the region
-    clocks.__exit__(None, None, None)
-    total_s = device_ms / 1000.0
-    if world > 1:
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
         import torch.distributed as dist
 
-        t = torch.tensor([total_s], device=f"cuda:{local}", dtype=torch.float64)
+        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
-    steps_per_s = args.steps / total_s
-    value = steps_per_s * NS_PER_DAY_PER_STEP_PER_S * world
+        return float(t.item())
 
-    # end to end through the public API, host buffers in and out
-    n = system.particle_count
-    host_pos = np.ascontiguousarray(state.positions, dtype=np.float64)
-    host_vel = np.ascontiguousarray(state.velocities, dtype=np.float64)
-    barrier()
-    t0 = time.perf_counter()
-    loop.set_positions(host_pos)
-    loop.set_velocities(host_vel)
-    readbacks = 0
-    for s in strides:
-        loop.run(s)
-        out = loop.positions()
-        readbacks += 1
-    e2e_s = time.perf_counter() - t0
-    barrier()
-    if world > 1:
-        import torch.distributed as dist
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    stride = min(args.stride, args.steps)
+    strides = [stride] * (args.steps // stride) + ([args.steps % stride] if args.steps % stride else [])
 
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = args.steps / e2e_s * NS_PER_DAY_PER_STEP_PER_S * world
-    assert np.isfinite(out).all()
+    def timed(loop) -> tuple[float, dict]:
+        """Warm-up, then exactly args.steps steps as timed strides; device seconds."""
+        # clocks are sampled from before the warm-up, so nvidia-smi is running when
+        # the timed region starts; only samples inside that region are reported
+        clocks = ClockSampler(local).__enter__()
+        loop.run(args.warmup)
+        for s in set(strides):
+            loop.run(s)
+        barrier()
+        device_ms = 0.0
+        t0 = time.perf_counter()
+        for s in strides:
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            device_ms += loop.run_timed(s)
+        barrier()
+        t1 = time.perf_counter()
+        time.sleep(0.3)  # let the sampler flush the last line of the region
+        clocks.__exit__(None, None, None)
+        return max_over_ranks(device_ms / 1000.0), clocks.summary(t0, t1)
 
-    # stage profile for the roofline (advances the replica; done after timing)
-    prof = loop.profile_step(repeats=20)
-    pairs = prof["pairs_within_cutoff"]
-    nb_s = prof["ms_nonbonded"] / 1000.0
-    achieved = FLOP_PER_PAIR * pairs / nb_s / 1e12
-    peaks = {}
-    peaks_path = ROOT / "MEASURED_PEAKS.json"
-    if peaks_path.exists():
-        peaks = json.loads(peaks_path.read_text())
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    mesh = prof["mesh_points"]
-    atoms = prof["atoms"]
-    spread_bytes = 28 * atoms + 8 * mesh
-    gather_bytes = 4 * mesh + 52 * atoms
-    integ_bytes = 124 * atoms
-    stages = {
-        "nonbonded_ms": prof["ms_nonbonded"], "listed_ms": prof["ms_listed"], "pme_ms": prof["ms_pme"],
-        "pme_spread_ms": prof["ms_pme_spread"], "pme_fft_ms": prof["ms_pme_fft"],
-        "pme_gather_ms": prof["ms_pme_gather"], "integrate_ms": prof["ms_integrate"],
-        "list_check_ms": prof["ms_list_check"], "list_rebuild_ms": prof["ms_list_rebuild"],
-        "step_ms": prof["ms_step"], "pairs_within_cutoff": pairs, "tiles": prof["tiles"],
-        "pair_fraction_in_tiles": pairs / max(1, prof["tiles"] * 1024),
-        "spread_GBs": spread_bytes / (prof["ms_pme_spread"] / 1000) / 1e9,
-        "gather_GBs": gather_bytes / (prof["ms_pme_gather"] / 1000) / 1e9,
-        "integrate_GBs": integ_bytes / (prof["ms_integrate"] / 1000) / 1e9,
-    }
+    def end_to_end(loop, states) -> tuple[float, int, int]:
+        """The same steps through the public API with host buffers: upload every
+        system's state, run the strides, read every system's positions back after
+        each; wall-clock seconds and the bytes moved."""
+        host = [(np.ascontiguousarray(st.positions, dtype=np.float64),
+                 np.ascontiguousarray(st.velocities, dtype=np.float64)) for st in states]
+        barrier()
+        t0 = time.perf_counter()
+        h2d = d2h = 0
+        for k, (p, v) in enumerate(host):
+            loop.set_positions(p, k)
+            loop.set_velocities(v, k)
+            h2d += p.nbytes + v.nbytes
+        for s in strides:
+            loop.run(s)
+            for k in range(len(host)):
+                out = loop.positions(k)
+                d2h += out.nbytes
+            assert np.isfinite(out).all()
+        elapsed = time.perf_counter() - t0
+        barrier()
+        return max_over_ranks(elapsed), h2d, d2h
 
+    def roofline(loop) -> dict:
+        # stage profile (advances the replica; done after timing)
+        prof = loop.profile_step(repeats=20)
+        pairs = prof["pairs_within_cutoff"]
+        achieved = FLOP_PER_PAIR * pairs / (prof["ms_nonbonded"] / 1000.0) / 1e12
+        peaks = {}
+        peaks_path = ROOT / "MEASURED_PEAKS.json"
+        if peaks_path.exists():
+            peaks = json.loads(peaks_path.read_text())
+        mesh, atoms = prof["mesh_points"], prof["atoms"]
+        spread_bytes = 28 * atoms + 8 * mesh
+        gather_bytes = 4 * mesh + 52 * atoms
+        integ_bytes = 124 * atoms
+        stages = {
+            "nonbonded_ms": prof["ms_nonbonded"], "listed_ms": prof["ms_listed"], "pme_ms": prof["ms_pme"],
+            "pme_spread_ms": prof["ms_pme_spread"], "pme_fft_ms": prof["ms_pme_fft"],
+            "pme_gather_ms": prof["ms_pme_gather"], "integrate_ms": prof["ms_integrate"],
+            "list_check_ms": prof["ms_list_check"], "list_rebuild_ms": prof["ms_list_rebuild"],
+            "step_ms": prof["ms_step"], "pairs_within_cutoff": pairs, "tiles": prof["tiles"],
+            "pair_fraction_in_tiles": pairs / max(1, prof["tiles"] * 1024),
+            "spread_GBs": spread_bytes / (prof["ms_pme_spread"] / 1000) / 1e9,
+            "gather_GBs": gather_bytes / (prof["ms_pme_gather"] / 1000) / 1e9,
+            "integrate_GBs": integ_bytes / (prof["ms_integrate"] / 1000) / 1e9,
+        }
+        return {"bound": "fp32", "kernel": "k_nonbonded", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
+                "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": NB_TRAFFIC.get(config),
+                "peak_source": "nominal FP32 issue rate, 148 SM x 128 lanes x 2 flop x 1.965 GHz",
+                "algorithmic": f"{FLOP_PER_PAIR:.0f} flop x {pairs} in-cutoff pairs per launch",
+                "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0), "hbm_peak_source":
+                    "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback", "stages": stages,
+                "launches_per_step": prof["launches_per_step"]}
+
+    if config == "ensemble-64":
+        from mdb200 import synth
+
+        members = synth.config_ensemble_64(seed=1 + rank)
+        systems = [m[0] for m in members]
+        states = [m[1] for m in members]
+        # plain engine: every system alone, default tuning, timed the same way
+        plain_ms = 0.0
+        plain_steps = max(100, min(args.steps, 500))
+        for s, st in zip(systems, states):
+            one = steploop.StepLoop.from_parsed(s, st, steploop.RunOptions(seed=7 + rank, device=local,
+                                                                          max_batch=args.stride))
+            one.run(args.warmup)
+            one.run(min(args.stride, plain_steps))
+            ms = 0.0
+            for _ in range(max(1, plain_steps // args.stride)):
+                flush_l2(flush)
+                torch.cuda.synchronize()
+                ms += one.run_timed(min(args.stride, plain_steps))
+            plain_ms += ms / (max(1, plain_steps // args.stride) * min(args.stride, plain_steps))
+            one.destroy()
+        plain_ms = max_over_ranks(plain_ms)
+        # autotuner per size bucket (untimed), then one batched engine
+        tuning, buckets = steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local))
+        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride, tuning=tuning)
+        loop = steploop.StepLoop.batch(systems, states, opts)
+        total_s, clock_summary = timed(loop)
+        steps_per_s = args.steps / total_s
+        n_sys = len(systems)
+        value = steps_per_s * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
+        plain_value = 1000.0 / plain_ms * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
+        e2e_s, h2d, d2h = end_to_end(loop, states)
+        cfg = {"workload": f"{n_sys} independent systems, 2,000-30,000 atoms log-uniform, cubic or rhombic "
+                           "dodecahedral TIP3P, half with an Ala helix of 10-40 residues where it fits",
+               "systems": n_sys, "atoms": sum(s.particle_count for s in systems),
+               "aggregate": "system-ns/day summed over the systems",
+               "plain_engine_ns_per_day": plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
+               "batched_over_plain": value / plain_value,
+               "autotuner": {str(b): {k: round(v, 4) if isinstance(v, float) else v for k, v in r.items()}
+                             for b, r in buckets.items()}}
+        result_loop, n_atoms = loop, cfg["atoms"]
+        e2e_value = args.steps / e2e_s * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
+        system, state = systems[0], states[0]
+    else:
+        system, state, cfg = workload(config, seed=1 + rank)
+        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride)
+        loop = steploop.StepLoop.from_parsed(system, state, opts)
+        total_s, clock_summary = timed(loop)
+        steps_per_s = args.steps / total_s
+        value = steps_per_s * NS_PER_DAY_PER_STEP_PER_S * world
+        e2e_s, h2d, d2h = end_to_end(loop, [state])
+        e2e_value = args.steps / e2e_s * NS_PER_DAY_PER_STEP_PER_S * world
+        result_loop, n_atoms = loop, system.particle_count
+
+    roof = roofline(result_loop)
     result = {
         "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_s * 1000.0 / args.steps, "higher_is_better": True,
@@ -300,23 +383,18 @@ def main() -> None:
         "config": {**cfg, "time_step_ps": TIME_STEP_PS, "steps_per_s": steps_per_s * world,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"flushed (256 MB write) between timed strides of {stride} steps"},
-        "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": 48 * n / args.steps,
-                "d2h_bytes_per_step": 24 * n * readbacks / args.steps},
-        "gpu_launches": int(prof["launches_per_step"]) * args.steps,
-        "roofline": {"bound": "fp32", "kernel": "k_nonbonded", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
-                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": None,
-                     "peak_source": "nominal FP32 issue rate, 148 SM x 128 lanes x 2 flop x 1.965 GHz",
-                     "algorithmic": f"{FLOP_PER_PAIR:.0f} flop x {pairs} in-cutoff pairs per launch",
-                     "hbm_peak_gbs": hbm_peak, "stages": stages},
-        "clocks": clocks.summary(timed_start, timed_end),
+        "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps},
+        "gpu_launches": int(roof.pop("launches_per_step")) * args.steps,
+        "roofline": roof,
+        "clocks": clock_summary,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sps, nsteps, elapsed = cpu_time_oracle(system, state, 1000, args.cpu_budget, threads)
+        cpu_value, _, _, sample = cpu_rate(config, 1000, args.cpu_budget, threads)
         result["cpu_baseline"] = {
-            "value": sps * NS_PER_DAY_PER_STEP_PER_S, "unit": "ns/day", "cores": threads, "kind": "port",
-            "sample": f"{nsteps} MD steps of the same workload in {elapsed:.1f} s (f64 C++ restatement of "
-                      "src/reference, OpenMP over all host threads)"}
+            "value": cpu_value, "unit": "ns/day", "cores": threads, "kind": "port",
+            "sample": sample + " (f64 C++ restatement of src/reference, OpenMP over all host threads)"}
     loop.destroy()
     if rank == 0:
         print(json.dumps(result))

@@ -153,6 +153,16 @@ typedef struct mdb_state_desc {
 } mdb_state_desc;
 
 /* Mirrors `RunOptions`, src/gpu/loop.ts:117-168. */
+/*
+ * Per-system tuning of the neighbour machinery (no reference counterpart):
+ * chosen per size bucket by mdb_autotune, passed one per system through
+ * mdb_run_options.tuning.  Zero or negative fields keep the defaults.
+ */
+typedef struct mdb_tuning {
+  double verlet_skin;  /* nm; list radius = cutoff + skin; default 0.15 (nonbonded.ts:227) */
+  double sort_cell;    /* nm; width of the fractional cells of the spatial sort; default 0.25 */
+} mdb_tuning;
+
 typedef struct mdb_run_options {
   double time_step;            /* ps */
   double temperature;          /* K */
@@ -165,6 +175,7 @@ typedef struct mdb_run_options {
   int32_t mesh[3];             /* PME mesh override; 0 = from the box */
   int32_t device;              /* CUDA device ordinal */
   int32_t flags;               /* MDB_FLAG_* */
+  const mdb_tuning* tuning;    /* NULL, or one entry per system of the engine (no reference counterpart) */
 } mdb_run_options;
 
 /*
@@ -367,6 +378,17 @@ int mdb_get_neighbour_stats(mdb_engine* engine, int32_t system,
 int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* charges,
                            const double box[9], double alpha, const int32_t mesh[3],
                            double* forces, double* energy, void* stream);
+
+/*
+ * Autotuner (no reference counterpart).  Times every candidate of a fixed grid
+ * of (verlet_skin, sort_cell) on the device -- a temporary engine per
+ * candidate, `steps` graph-replayed steps after a warm-up of the same length,
+ * CUDA-event timed -- and returns the fastest in `best` and its ms per step.
+ * `tried` (may be NULL) receives the number of candidates.  The state the
+ * candidates start from is `state`; nothing else is changed.
+ */
+int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
+                 int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried);
 
 /* Per-stage device timing (see mdb_profile).  Replaces `StepLoop.profileStep`, loop.ts:705. */
 int mdb_profile_step(mdb_engine* engine, int32_t repeats, mdb_profile* out);

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -71,6 +72,8 @@ struct mdb_engine {
   int n_mesh_items = 0;
   std::vector<int> fft_x_sys;  // system of each x-pass work item
   bool coop_list = false;      // the list kernels run as one cooperative launch
+  std::vector<double> skin;        // per system, nm
+  std::vector<double> sort_cell;   // per system, nm
 };
 
 namespace {
@@ -269,7 +272,16 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   e->opt = *options;
   if (e->opt.max_batch <= 0) e->opt.max_batch = 100;
   if (!(e->opt.time_step > 0)) return fail(e, MDB_ERR_INVALID_ARGUMENT, "time_step must be positive");
-  const double skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
+  const double default_skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
+  e->skin.assign(n, default_skin);
+  e->sort_cell.assign(n, kCellWidth);
+  if (e->opt.tuning) {
+    for (int s = 0; s < n; ++s) {
+      if (e->opt.tuning[s].verlet_skin > 0) e->skin[s] = e->opt.tuning[s].verlet_skin;
+      if (e->opt.tuning[s].sort_cell > 0) e->sort_cell[s] = e->opt.tuning[s].sort_cell;
+    }
+    e->opt.tuning = nullptr;  // the caller's array is not kept
+  }
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
     return fail(e, MDB_ERR_NO_DEVICE, "no CUDA device is visible");
@@ -329,7 +341,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     S.block_off = blocks;
     double widths[3];
     perpendicular_widths(h.box.data(), widths);
-    for (int k = 0; k < 3; ++k) S.cdim[k] = std::max(1, int(std::floor(widths[k] / kCellWidth)));
+    for (int k = 0; k < 3; ++k) S.cdim[k] = std::max(1, int(std::floor(widths[k] / e->sort_cell[s])));
     S.n_cells = S.cdim[0] * S.cdim[1] * S.cdim[2];
     S.cell_off = cells;
     const long long all_pairs = (long long)S.n_blocks * (S.n_blocks + 1) / 2;
@@ -337,6 +349,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     S.tile_off = tiles;
     S.energy_base = s * kECount;
     S.cut2 = float(h.cutoff * h.cutoff);
+    const double skin = e->skin[s];
     S.list2 = float((h.cutoff + skin) * (h.cutoff + skin));
     S.half_skin2 = float(0.25 * skin * skin);
     S.alpha = float(h.alpha);
@@ -1013,6 +1026,41 @@ int mdb_system_count(const mdb_engine* e, int32_t* out) {
   return MDB_OK;
 }
 
+// The candidate grid: list skin (rebuild frequency against tile count) and
+// spatial-sort cell width (how compact a 32-atom block is).
+int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
+                 int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried) {
+  if (!system || !state || !options || !best || steps <= 0) return MDB_ERR_INVALID_ARGUMENT;
+  static const double kSkins[] = {0.10, 0.15, 0.20};
+  static const double kCells[] = {0.20, 0.25, 0.35};
+  double best_ms = std::numeric_limits<double>::infinity();
+  int count = 0, last = MDB_OK;
+  for (double skin : kSkins)
+    for (double cell : kCells) {
+      mdb_tuning t{skin, cell};
+      mdb_run_options o = *options;
+      o.tuning = &t;
+      mdb_engine* e = nullptr;
+      int st = mdb_batch_create(1, system, state, &o, &e);
+      double ms = 0;
+      if (st == MDB_OK) st = mdb_run(e, steps);  // warm-up: lists, graph capture
+      if (st == MDB_OK) st = mdb_run_timed(e, steps, &ms);
+      if (e) mdb_destroy(e, nullptr);
+      ++count;
+      if (st != MDB_OK) {  // a candidate may overflow a table; the others still count
+        last = st;
+        continue;
+      }
+      if (ms / steps < best_ms) {
+        best_ms = ms / steps;
+        *best = t;
+      }
+    }
+  if (tried) *tried = count;
+  if (best_ms_per_step) *best_ms_per_step = best_ms;
+  return std::isfinite(best_ms) ? MDB_OK : last;
+}
+
 int mdb_run(mdb_engine* e, int64_t steps) {
   if (!e || steps < 0) return MDB_ERR_INVALID_ARGUMENT;
   return run(e, steps);
@@ -1146,7 +1194,7 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   out->tile_capacity = e->sd[s].tile_cap;
   out->blocks = e->sd[s].n_blocks;
   out->overflowed = (err & kErrTileCapacity) ? 1 : 0;
-  out->skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
+  out->skin = e->skin[s];
   return MDB_OK;
 }
 

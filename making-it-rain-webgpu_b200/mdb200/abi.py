@@ -110,6 +110,12 @@ class StateDesc(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    """`mdb_tuning` (no reference counterpart)."""
+
+    _fields_ = [("verlet_skin", C.c_double), ("sort_cell", C.c_double)]
+
+
 class RunOptions(C.Structure):
     """`mdb_run_options`."""
 
@@ -125,6 +131,7 @@ class RunOptions(C.Structure):
         ("mesh", C.c_int32 * 3),
         ("device", C.c_int32),
         ("flags", C.c_int32),
+        ("tuning", C.POINTER(Tuning)),
     ]
 
 
@@ -238,6 +245,8 @@ EXPORTS = {
     "mdb_get_neighbour_stats": (C.c_int, [_E, C.c_int32, C.POINTER(NeighbourStats)]),
     "mdb_memory_report": (C.c_int, [_E, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "mdb_profile_step": (C.c_int, [_E, C.c_int32, C.POINTER(Profile)]),
+    "mdb_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunOptions), C.c_int32, C.POINTER(Tuning),
+                               C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mdb_reciprocal_noalloc": (
         C.c_int,
         [C.c_int32, C.c_void_p, C.c_void_p, _dp, C.c_double, _ip, C.c_void_p, C.c_void_p, C.c_void_p],

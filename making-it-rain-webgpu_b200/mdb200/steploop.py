@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import math
 from typing import Optional, Sequence
 
 import numpy as np
@@ -74,6 +75,8 @@ class RunOptions:
     device: int = 0
     graphs: bool = True
     always_rebuild: bool = False
+    # per-system (verlet_skin, sort_cell) pairs from `autotune`; None = defaults
+    tuning: Optional[Sequence[tuple]] = None
 
     def to_c(self) -> abi.RunOptions:
         o = abi.RunOptions()
@@ -88,6 +91,10 @@ class RunOptions:
         o.mesh[:] = list(self.mesh) if self.mesh is not None else [0, 0, 0]
         o.device = int(self.device)
         o.flags = (0 if self.graphs else abi.FLAG_NO_GRAPH) | (abi.FLAG_ALWAYS_REBUILD if self.always_rebuild else 0)
+        if self.tuning is not None:
+            arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(a), float(b)) for a, b in self.tuning])
+            o.tuning = C.cast(arr, C.POINTER(abi.Tuning))
+            o._keep = arr  # the array must outlive the create call
         return o
 
 
@@ -294,3 +301,49 @@ class StepLoop:
 
 __all__ = ["StepLoop", "RunOptions", "Report", "EngineError", "CutoffTooLargeForBox", "ClusterTooLarge",
            "NotSmooth", "NoDevice", "UnsupportedForce"]
+
+
+# ---- autotuner (no reference counterpart) -------------------------------------
+def autotune(system: System, state: State, options: RunOptions | None = None, steps: int = 200) -> dict:
+    """Time the library's candidate grid of (verlet_skin, sort_cell) for one
+    system on the device (`mdb_autotune`) and return the fastest."""
+    options = options or RunOptions()
+    lib = abi.load()
+    sh, th = system.desc(), state.desc()
+    opts = dataclasses.replace(options, tuning=None).to_c()
+    best = abi.Tuning()
+    ms = C.c_double()
+    tried = C.c_int32()
+    status = lib.mdb_autotune(C.byref(sh.desc), C.byref(th.desc), C.byref(opts), int(steps), C.byref(best),
+                              C.byref(ms), C.byref(tried))
+    if status != abi.OK:
+        raise _ERRORS.get(status, EngineError)(status, lib.mdb_status_string(status).decode())
+    return {"verlet_skin": best.verlet_skin, "sort_cell": best.sort_cell, "ms_per_step": ms.value,
+            "candidates": tried.value}
+
+
+def size_bucket(atoms: int) -> int:
+    """Size buckets of the autotuner: powers of two of the atom count."""
+    return int(math.floor(math.log2(max(1, atoms))))
+
+
+def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: RunOptions | None = None,
+                   steps: int = 200, cache: dict | None = None) -> tuple[list, dict]:
+    """One `autotune` per size bucket, on the bucket's median-sized system;
+    every system of the bucket takes its result.  Returns the per-system
+    (verlet_skin, sort_cell) list for `RunOptions.tuning` and the per-bucket
+    results.  `cache` (bucket -> result) skips buckets already tuned."""
+    cache = {} if cache is None else cache
+    buckets: dict[int, list[int]] = {}
+    for k, s in enumerate(systems):
+        buckets.setdefault(size_bucket(s.particle_count), []).append(k)
+    for b, members in sorted(buckets.items()):
+        if b in cache:
+            continue
+        members = sorted(members, key=lambda k: systems[k].particle_count)
+        rep = members[len(members) // 2]
+        cache[b] = autotune(systems[rep], states[rep], options, steps)
+    tuning = [(cache[size_bucket(s.particle_count)]["verlet_skin"], cache[size_bucket(s.particle_count)]["sort_cell"])
+              for s in systems]
+    return tuning, cache
+

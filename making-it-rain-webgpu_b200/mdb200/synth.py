@@ -256,3 +256,51 @@ def config_octahedron_27k(seed: int = 1):
     solute, positions = peptide.coil()
     width = max(2.0 * peptide.bounding_radius(positions) + 1.0, 2.0)
     return solvated(solute, positions, width=width, shape="octahedron", seed=seed)
+
+
+def _perpendicular_min(box: np.ndarray) -> float:
+    a, b, c = box
+    v = abs(np.linalg.det(box))
+    return float(min(v / np.linalg.norm(np.cross(b, c)), v / np.linalg.norm(np.cross(c, a)),
+                     v / np.linalg.norm(np.cross(a, b))))
+
+
+def ensemble_member(rng: np.random.Generator, seed: int, cutoff: float = 1.0):
+    """One system of the batched ensemble: a target atom count drawn
+    log-uniformly from 2,000 to 30,000, a cubic or rhombic-dodecahedral cell of
+    TIP3P sized to it, and, half the time, an Ala helix of 10-40 residues when
+    one fits the cell at OpenMM's 1.0 nm padding (otherwise the longest that
+    fits, or none).  Returns (system, state, description)."""
+    from . import peptide
+
+    target = math.exp(rng.uniform(math.log(2000), math.log(30000)))
+    shape = "cube" if rng.random() < 0.5 else "dodecahedron"
+    volume = target / (3 * WATER_DENSITY_PER_NM3)
+    unit = abs(np.linalg.det(box_vectors(shape, 1.0)))
+    width = (volume / unit) ** (1 / 3)
+    # the cutoff must stay below half the narrowest perpendicular width
+    width = max(width, 2.02 * cutoff / _perpendicular_min(box_vectors(shape, 1.0)))
+    residues = int(rng.integers(10, 41)) if rng.random() < 0.5 else 0
+    room = _perpendicular_min(box_vectors(shape, width))
+    while residues >= 10:
+        solute, x = peptide.helix(["ALA"] * residues)
+        if 2 * peptide.bounding_radius(x) + 1.0 <= room:
+            break
+        residues -= 5
+    if residues < 10:
+        residues = 0
+    if residues:
+        system, state = solvated(solute, x, width=width, shape=shape, seed=seed)
+    else:
+        system, state = water_box(width=width, shape=shape, seed=seed)
+    return system, state, {"shape": shape, "width": width, "helix_residues": residues,
+                           "atoms": system.particle_count}
+
+
+def config_ensemble_64(seed: int = 1, count: int = 64):
+    """The batched ensemble: `count` independent systems of uneven sizes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        out.append(ensemble_member(rng, seed=seed * 1000 + k))
+    return out
