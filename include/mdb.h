@@ -176,6 +176,9 @@ typedef struct mdb_run_options {
   int32_t device;              /* CUDA device ordinal */
   int32_t flags;               /* MDB_FLAG_* */
   const mdb_tuning* tuning;    /* NULL, or one entry per system of the engine (no reference counterpart) */
+  int32_t surrogate_attempts;  /* > 0: each barostat learns a screening network from that many exact
+                                  attempts, then screens proposals by delayed acceptance; 0 = plain
+                                  barostat (no reference counterpart) */
 } mdb_run_options;
 
 /*
@@ -208,6 +211,9 @@ typedef struct mdb_energies {
                                   dispersion and net-charge corrections (not restraints); kJ/mol.
                                   No reference counterpart. */
   double pairs_within_cutoff;  /* non-excluded pairs inside the cutoff (count) */
+  double molecular_virial[9];  /* -dU/d eps under scaling of molecule centres (the plain mean of a
+                                  molecule's positions, as the barostat moves them): the virial
+                                  minus sum_i (r_i - R_mol(i)) (x) F_i.  No reference counterpart. */
 } mdb_energies;
 
 /* Mirrors `StepLoop.barostatStatistics`, src/gpu/loop.ts:572. */
@@ -216,8 +222,13 @@ typedef struct mdb_barostat_stats {
   int64_t accepted;
   double volume_scale;     /* nm^3 */
   /* delayed-acceptance screening (no reference counterpart) */
-  int64_t screened;        /* proposals decided by the surrogate stage alone */
-  int64_t exact_evaluations;
+  int64_t screened;          /* proposals rejected by the network stage alone */
+  int64_t exact_evaluations; /* exact potential evaluations the attempts made */
+  int64_t training_samples;  /* exact attempts the network learned from */
+  int32_t surrogate_active;  /* 1 while proposals are screened */
+  int32_t surrogate_disabled;/* 1 when the exact stage found the network too inaccurate */
+  double surrogate_rms;      /* running RMS of (predicted - exact) potential change, kJ/mol */
+  double training_loss;      /* final mean squared training loss (standardised units) */
 } mdb_barostat_stats;
 
 /*
@@ -389,6 +400,24 @@ int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* cha
  */
 int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
                  int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried);
+
+/*
+ * The barostat screening network's kernels on their own (no reference
+ * counterpart), for checking them against a CPU restatement.  Layout of
+ * `params` (kMlpParams = 5313 floats): W1[64][16], b1[64], W2[64][64], b2[64],
+ * w3[64], b3.  Inputs x[n][16], targets t[n], host arrays; these entry points
+ * allocate device memory.
+ *   mdb_mlp_gradient: the weights are rounded to BF16 as the kernels use them;
+ *     writes the mean-squared-error gradient of the first min(n, 128) samples
+ *     (FP32, accumulated in FP32) and that loss.
+ *   mdb_mlp_fit: seeded Glorot start, `epochs` epochs of Adam (lr 2e-3,
+ *     minibatch 128); writes the final FP32 master weights and, per epoch, the
+ *     mean minibatch loss.
+ */
+int mdb_mlp_gradient(const float* params, const float* x, const float* t, int32_t n, float* grad, float* loss);
+int mdb_mlp_fit(const float* x, const float* t, int32_t n, int32_t epochs, uint32_t seed, float* params,
+                float* epoch_loss);
+int mdb_mlp_predict(const float* params, const float* x, int32_t n, float* y);
 
 /* Per-stage device timing (see mdb_profile).  Replaces `StepLoop.profileStep`, loop.ts:705. */
 int mdb_profile_step(mdb_engine* engine, int32_t repeats, mdb_profile* out);

@@ -32,6 +32,9 @@ struct Dev {
   int* rank;      // slot of an atom within its system's sorted order
   int* cell_of;   // global cell
   long long *refx, *refy, *refz;
+  long long *bx, *by, *bz;         // positions before a Monte Carlo volume move
+  const int* mol_off;              // molecule m's atoms: mol_atoms[mol_off[m] .. mol_off[m+1])
+  const int* mol_atoms;            // global atom indices, molecule by molecule, system by system
   const float4* prm_atom;  // q*sqrt(ONE_4PI_EPS0), sigma/2, sqrt(eps), q
 
   // slots, sorted order
@@ -124,5 +127,10 @@ void launch_pme_fft(const Dev& d, bool energy, cudaStream_t s);
 void launch_pme_gather(const Dev& d, cudaStream_t s);
 void launch_integrate(const Dev& d, cudaStream_t s);
 void launch_momentum(const Dev& d, cudaStream_t s);
+void launch_scale_molecules(const Dev& d, int first_mol, int n_mol, double scale, cudaStream_t st);
+void launch_restore_positions(const Dev& d, int atom_off, int n, cudaStream_t st);
+int molecular_offset_blocks(int n_mol);
+void launch_molecular_offsets(const Dev& d, int first_mol, int n_mol, int slot_off, double* partials,
+                              cudaStream_t st);
 
 }  // namespace mdb

@@ -16,18 +16,21 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
 #include <map>
 #include <memory>
+#include <numeric>
 #include <sstream>
 #include <string>
 #include <vector>
 
 #include "../../include/mdb.h"
 #include "device_state.h"
+#include "mlp.h"
 #include "prep.h"
 
 namespace mdb {
@@ -47,10 +50,30 @@ struct Allocation {
   size_t bytes;
 };
 
+// The barostat's screening network for one system (no reference counterpart).
+struct Surrogate {
+  int target = 0;                 // exact attempts to learn from before screening; 0 = off
+  bool active = false;            // trained: proposals go through the two-stage test
+  bool disabled = false;          // the exact stage judged it too inaccurate: plain barostat
+  std::vector<float> feats;       // raw features of every exact attempt, kMlpIn each
+  std::vector<double> delta_u;    // exact potential change of those attempts per atom, kJ/mol
+  double mu[kMlpIn] = {}, sd[kMlpIn] = {}, mu_t = 0, sd_t = 1;
+  double err2 = 0;                // running mean square of (predicted - exact) change
+  int64_t judged = 0;
+  MlpDev dev{};
+  float* x = nullptr;             // device: normalised training inputs, then inference inputs
+  float* t = nullptr;             // device: normalised targets
+  float* y = nullptr;             // device: inference outputs
+  float* loss = nullptr;          // device: per-minibatch losses of the last epoch
+  double final_loss = 0;
+};
+
 struct BarostatState {
   double volume_scale = 0;
   int64_t attempts = 0, accepted = 0, step = 0, draw = 0;
+  int64_t screened = 0, exact = 0;
   int window_attempts = 0, window_accepted = 0;
+  Surrogate net;
 };
 
 }  // namespace
@@ -73,6 +96,8 @@ struct mdb_engine {
   std::vector<int> fft_x_sys;  // system of each x-pass work item
   bool coop_list = false;      // the list kernels run as one cooperative launch
   std::vector<double> skin;        // per system, nm
+  std::vector<int> mol_first, mol_count;  // per system: its molecules in d.mol_off
+  double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel
   std::vector<double> sort_cell;   // per system, nm
 };
 
@@ -523,6 +548,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     tiles += S.tile_cap;
     e->baro[s].volume_scale = 0.01 * box_volume(h.box.data());
     e->baro[s].step = 0;
+    e->baro[s].net.target = std::max(0, e->opt.surrogate_attempts);
   }
 
   // ---- device tables ----
@@ -556,6 +582,9 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "list reference.x", d.refx, atoms));
   TRY(alloc(e, "list reference.y", d.refy, atoms));
   TRY(alloc(e, "list reference.z", d.refz, atoms));
+  TRY(alloc(e, "volume move backup.x", d.bx, atoms));
+  TRY(alloc(e, "volume move backup.y", d.by, atoms));
+  TRY(alloc(e, "volume move backup.z", d.bz, atoms));
   float4* prm_atom_dev = nullptr;
   TRY(upload(e, "pair parameters by atom", prm_atom_dev, prm_atom));
   d.prm_atom = prm_atom_dev;
@@ -634,6 +663,29 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.fft_x = w_dev; d.n_fft_x = int(wx.size());
   e->n_mesh_items = int(wx.size());
   TRY(alloc(e, "energies", d.energy, size_t(n) * kECount));
+  {
+    std::vector<int> mol_off{0}, mol_atoms;
+    e->mol_first.assign(n, 0);
+    e->mol_count.assign(n, 0);
+    int base = 0;
+    for (int s = 0; s < n; ++s) {
+      e->mol_first[s] = int(mol_off.size()) - 1;
+      e->mol_count[s] = int(e->hs[s].molecules.size());
+      for (const auto& m : e->hs[s].molecules) {
+        for (int a : m) mol_atoms.push_back(base + a);
+        mol_off.push_back(int(mol_atoms.size()));
+      }
+      base += e->hs[s].n;
+    }
+    int* tmp = nullptr;
+    TRY(upload(e, "molecule offsets", tmp, mol_off));
+    d.mol_off = tmp;
+    TRY(upload(e, "molecule atoms", tmp, mol_atoms));
+    d.mol_atoms = tmp;
+    int most = 1;
+    for (int s = 0; s < n; ++s) most = std::max(most, molecular_offset_blocks(e->mol_count[s]));
+    TRY(alloc(e, "molecular virial partials", e->mol_partials, size_t(most) * 9));
+  }
   UnitDev* u_dev = nullptr;
   TRY(upload(e, "integration units", u_dev, units));
   d.units = u_dev;
@@ -699,7 +751,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   return MDB_OK;
 }
 
-int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
+int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinetic = true) {
   const Dev& d = e->d;
   const HostSystem& h = e->hs[s];
   const SysDev& S = e->sd[s];
@@ -711,6 +763,14 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
   CUDA_TRY(e, cudaGetLastError());
   int st = check_device_status(e);
   if (st) return st;
+  std::vector<double> mol_part;
+  if (out) {
+    launch_molecular_offsets(d, e->mol_first[s], e->mol_count[s], S.slot_off, e->mol_partials, e->s0);
+    CUDA_TRY(e, cudaGetLastError());
+    mol_part.resize(size_t(molecular_offset_blocks(e->mol_count[s])) * 9);
+    CUDA_TRY(e, cudaStreamSynchronize(e->s0));  // s0 does not order with the legacy stream
+    CUDA_TRY(e, cudaMemcpy(mol_part.data(), e->mol_partials, sizeof(double) * mol_part.size(), cudaMemcpyDeviceToHost));
+  }
   if (forces) {
     std::vector<unsigned long long> f[3];
     std::vector<int> order(S.n_slots);
@@ -767,21 +827,29 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out) {
       if (sym[c][1] != sym[c][0]) out->virial[sym[c][1]] += wm[c];
     }
     for (int a = 0; a < 3; ++a) out->virial[4 * a] += out->dispersion + out->net_charge;
+    // the molecular virial: minus the atoms' offsets from their molecule's centre
+    for (int c = 0; c < 9; ++c) {
+      double corr = 0;
+      for (size_t b = 0; b < mol_part.size() / 9; ++b) corr += mol_part[b * 9 + c];
+      out->molecular_virial[c] = out->virial[c] - corr;
+    }
     out->potential = out->bond + out->angle + out->torsion + out->restraint + out->direct_group +
                      out->reciprocal_group;
     // kinetic energy from the velocities as they are (kinetic.ts:31)
-    std::vector<float> v[3];
-    for (auto& x : v) x.resize(h.n);
-    cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
-    cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
-    cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
-    double ke = 0;
-    for (int a = 0; a < h.n; ++a)
-      if (h.mass[a] > 0)
-        ke += h.mass[a] * (double(v[0][a]) * v[0][a] + double(v[1][a]) * v[1][a] + double(v[2][a]) * v[2][a]);
-    out->kinetic = 0.5 * ke;
-    out->degrees_of_freedom = h.dof;
-    out->temperature = h.dof > 0 ? 2 * out->kinetic / (h.dof * kBoltzmann) : 0;
+    if (kinetic) {
+      std::vector<float> v[3];
+      for (auto& x : v) x.resize(h.n);
+      cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+      cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+      cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+      double ke = 0;
+      for (int a = 0; a < h.n; ++a)
+        if (h.mass[a] > 0)
+          ke += h.mass[a] * (double(v[0][a]) * v[0][a] + double(v[1][a]) * v[1][a] + double(v[2][a]) * v[2][a]);
+      out->kinetic = 0.5 * ke;
+      out->degrees_of_freedom = h.dof;
+      out->temperature = h.dof > 0 ? 2 * out->kinetic / (h.dof * kBoltzmann) : 0;
+    }
   }
   // the step loop expects cleared accumulators
   CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, e->s0));
@@ -846,16 +914,142 @@ int set_box(mdb_engine* e, int s, const double* box) {
   return MDB_OK;
 }
 
+// ---- the barostat's screening network (no reference counterpart) ----------
+// Inputs: dlnV, the energy components and the molecular virial's diagonal per
+// atom, the box diagonal, and the first-order change -tr(W_mol) dlnV / 3 per
+// atom; the target is the potential change per atom.
+void surrogate_features(const mdb_energies& en, const HostSystem& h, const double* box, double dlnv,
+                        double* f) {
+  const double n = std::max(1, h.n);
+  const double raw[kMlpIn] = {dlnv,
+                              en.bond / n,
+                              en.angle / n,
+                              en.torsion / n,
+                              en.direct_coulomb / n,
+                              en.direct_lj / n,
+                              (en.exclusion_correction + en.exceptions) / n,
+                              en.reciprocal_mesh / n,
+                              en.dispersion / n,
+                              en.molecular_virial[0] / n,
+                              en.molecular_virial[4] / n,
+                              en.molecular_virial[8] / n,
+                              box[0],
+                              box[4],
+                              box[8],
+                              // the first-order change under molecular scaling, -tr(W_mol) dlnV / 3
+                              -(en.molecular_virial[0] + en.molecular_virial[4] + en.molecular_virial[8]) * dlnv /
+                                  (3 * n)};
+  for (int k = 0; k < kMlpIn; ++k) f[k] = raw[k];
+}
+
+int surrogate_alloc(mdb_engine* e, Surrogate& net, int samples) {
+#define TRY(x)              \
+  do {                      \
+    const int st_ = (x);    \
+    if (st_) return st_;    \
+  } while (0)
+  TRY(alloc(e, "surrogate weights", net.dev.w, kMlpParams));
+  TRY(alloc(e, "surrogate adam m", net.dev.m, kMlpParams));
+  TRY(alloc(e, "surrogate adam v", net.dev.v, kMlpParams));
+  TRY(alloc(e, "surrogate weights bf16", net.dev.w_bf16, kMlpParams));
+  TRY(alloc(e, "surrogate adam step", net.dev.step_count, 1));
+  TRY(alloc(e, "surrogate inputs", net.x, size_t(std::max(samples, 2)) * kMlpIn));
+  TRY(alloc(e, "surrogate targets", net.t, std::max(samples, 2)));
+  TRY(alloc(e, "surrogate outputs", net.y, 2));
+  TRY(alloc(e, "surrogate losses", net.loss, samples / kMlpBatch + 2));
+#undef TRY
+  return MDB_OK;
+}
+
+// Standardise the collected attempts, then train on the device from a seeded
+// start (mlp_train).
+int surrogate_train(mdb_engine* e, Surrogate& net, uint32_t seed, int epochs) {
+  const int n = int(net.delta_u.size());
+  if (n < kMlpBatch) return MDB_OK;
+  for (int k = 0; k < kMlpIn; ++k) {
+    double m = 0, v = 0;
+    for (int i = 0; i < n; ++i) m += net.feats[size_t(i) * kMlpIn + k];
+    m /= n;
+    for (int i = 0; i < n; ++i) v += (net.feats[size_t(i) * kMlpIn + k] - m) * (net.feats[size_t(i) * kMlpIn + k] - m);
+    net.mu[k] = m;
+    net.sd[k] = std::sqrt(v / n) > 1e-12 ? std::sqrt(v / n) : 1.0;
+  }
+  {
+    double m = 0, v = 0;
+    for (double t : net.delta_u) m += t;
+    m /= n;
+    for (double t : net.delta_u) v += (t - m) * (t - m);
+    net.mu_t = m;
+    net.sd_t = std::sqrt(v / n) > 1e-12 ? std::sqrt(v / n) : 1.0;
+  }
+  int st = surrogate_alloc(e, net, n);
+  if (st) return st;
+  std::vector<float> x(size_t(n) * kMlpIn), t(n);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < kMlpIn; ++k)
+      x[size_t(i) * kMlpIn + k] = float((net.feats[size_t(i) * kMlpIn + k] - net.mu[k]) / net.sd[k]);
+    t[i] = float((net.delta_u[i] - net.mu_t) / net.sd_t);
+  }
+  CUDA_TRY(e, cudaMemcpy(net.x, x.data(), sizeof(float) * x.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(net.t, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
+  net.dev.lr = 2e-3f;
+  net.dev.beta1 = 0.9f;
+  net.dev.beta2 = 0.999f;
+  net.dev.eps = 1e-8f;
+  std::vector<double> losses;
+  CUDA_TRY(e, mlp_train(net.dev, net.x, net.t, n, epochs, seed, net.loss, &losses, e->s0));
+  net.final_loss = losses.empty() ? 0.0 : losses.back();
+  net.active = true;
+  return MDB_OK;
+}
+
+// Predicted potential change (kJ/mol) of a move dlnV from a state with these
+// energies and box, by one device forward pass.
+int surrogate_predict(mdb_engine* e, Surrogate& net, const HostSystem& h, const mdb_energies& en,
+                      const double* box, double dlnv, double* out) {
+  double f[kMlpIn];
+  surrogate_features(en, h, box, dlnv, f);
+  float x[kMlpIn];
+  for (int k = 0; k < kMlpIn; ++k) x[k] = float((f[k] - net.mu[k]) / net.sd[k]);
+  CUDA_TRY(e, cudaMemcpyAsync(net.x, x, sizeof(x), cudaMemcpyHostToDevice, e->s0));
+  launch_mlp_forward(net.dev.w_bf16, net.x, 1, net.y, e->s0);
+  float y = 0;
+  CUDA_TRY(e, cudaMemcpyAsync(&y, net.y, sizeof(float), cudaMemcpyDeviceToHost, e->s0));
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  *out = (double(y) * net.sd_t + net.mu_t) * std::max(1, h.n);
+  return MDB_OK;
+}
+
+// Box and positions of a volume move, on the device: back up, scale every
+// molecule's centre, set the box (which requests the list rebuild).
+int apply_volume_move(mdb_engine* e, int s, double scale) {
+  launch_scale_molecules(e->d, e->mol_first[s], e->mol_count[s], scale, e->s0);
+  CUDA_TRY(e, cudaGetLastError());
+  double nb[9];
+  for (int i = 0; i < 9; ++i) nb[i] = e->hs[s].box[i] * scale;
+  return set_box(e, s, nb);
+}
+
+int undo_volume_move(mdb_engine* e, int s, const std::array<double, 9>& old_box) {
+  launch_restore_positions(e->d, e->sd[s].atom_off, e->sd[s].n_atoms, e->s0);
+  CUDA_TRY(e, cudaGetLastError());
+  return set_box(e, s, old_box.data());
+}
+
 // One Monte Carlo volume move (src/gpu/loop.ts:602-641, src/reference/barostat.ts:210-274).
+// With a trained screening network the move goes through delayed acceptance
+// (Christen & Fox 2005): stage 1 accepts with a1 = min(1, exp(-w~/kT)) from
+// the network's predicted change, and only then is the exact energy of the
+// proposal computed; stage 2 accepts with min(1, exp(-w/kT) a1(y->x)/a1(x->y)),
+// the reverse move's stage-1 probability evaluated with the network at the
+// proposal, so the chain keeps the exact NPT distribution.
 int barostat_attempt(mdb_engine* e, int s) {
   HostSystem& h = e->hs[s];
   BarostatState& b = e->baro[s];
-  const int n = h.n;
-  std::vector<double> pos(3 * n);
-  int st = get_positions(e, s, pos.data());
-  if (st) return st;
+  Surrogate& net = b.net;
   mdb_energies e0{};
-  if ((st = evaluate(e, s, nullptr, &e0))) return st;
+  int st = evaluate(e, s, nullptr, &e0, false);
+  if (st) return st;
   auto uniform = [&]() {
     // threefry2x32([draw, seed], [BAROSTAT_DOMAIN, 0]) (loop.ts:614-622)
     uint32_t c0 = uint32_t(b.draw++), c1 = e->opt.seed, k0 = 0x6a09e667u, k1 = 0;
@@ -873,40 +1067,60 @@ int barostat_attempt(mdb_engine* e, int s) {
     }
     return (double(x0 >> 9) + 0.5) * std::ldexp(1.0, -23);
   };
+  const std::array<double, 9> old_box = h.box;
   const double volume = box_volume(h.box.data());
   const double dv = b.volume_scale * 2 * (uniform() - 0.5);
   const double nv = volume + dv;
   const double scale = std::cbrt(nv / volume);
-  std::vector<double> trial(pos);
-  for (const auto& mol : h.molecules) {
-    double c[3] = {0, 0, 0};
-    for (int a : mol)
-      for (int k = 0; k < 3; ++k) c[k] += pos[3 * a + k];
-    for (int k = 0; k < 3; ++k) {
-      const double mean = c[k] / double(mol.size());
-      const double off = scale * mean - mean;
-      for (int a : mol) trial[3 * a + k] += off;
-    }
-  }
-  const std::array<double, 9> old_box = h.box;
-  double new_box[9];
-  for (int i = 0; i < 9; ++i) new_box[i] = old_box[i] * scale;
-  if ((st = set_box(e, s, new_box))) return st;
-  if ((st = set_positions(e, s, trial.data(), false))) return st;
-  mdb_energies e1{};
-  if ((st = evaluate(e, s, nullptr, &e1))) return st;
+  const double dlnv = std::log(nv / volume);
   const double pressure = h.barostat_pressure * 0.06022140762081242;
   const double kT = kBoltzmann * h.barostat_temperature;
-  const double w = e1.potential - e0.potential + pressure * dv - double(h.molecules.size()) * kT * std::log(nv / volume);
-  const bool accepted = !(w > 0 && uniform() > std::exp(-w / kT));
+  const double volume_term = pressure * dv - double(h.molecules.size()) * kT * dlnv;
+  const bool screen = net.active && !net.disabled;
+  double a1 = 1.0, du_pred = 0.0;
+  if (screen) {
+    if ((st = surrogate_predict(e, net, h, e0, old_box.data(), dlnv, &du_pred))) return st;
+    a1 = std::min(1.0, std::exp(-(du_pred + volume_term) / kT));
+  }
   b.attempts++;
   b.window_attempts++;
+  bool accepted = false;
+  if (screen && !(uniform() < a1)) {
+    b.screened++;  // rejected by the network alone: no exact evaluation
+  } else {
+    if ((st = apply_volume_move(e, s, scale))) return st;
+    mdb_energies e1{};
+    if ((st = evaluate(e, s, nullptr, &e1, false))) return st;
+    b.exact++;
+    const double du = e1.potential - e0.potential;
+    const double w = du + volume_term;
+    if (screen) {
+      double du_rev = 0.0;
+      if ((st = surrogate_predict(e, net, h, e1, h.box.data(), -dlnv, &du_rev))) return st;
+      const double a1_rev = std::min(1.0, std::exp(-(du_rev - volume_term) / kT));
+      const double a2 = std::min(1.0, std::exp(-w / kT) * a1_rev / a1);
+      accepted = uniform() < a2;
+      // the exact stage judges the network
+      const double err = du_pred - du;
+      net.err2 = net.judged == 0 ? err * err : 0.98 * net.err2 + 0.02 * err * err;
+      if (++net.judged >= 50 && std::sqrt(net.err2) > 3.0 * kT) net.disabled = true;
+    } else {
+      accepted = !(w > 0 && uniform() > std::exp(-w / kT));
+      if (net.target > 0 && !net.active) {
+        double f[kMlpIn];
+        surrogate_features(e0, h, old_box.data(), dlnv, f);
+        for (double v : f) net.feats.push_back(float(v));
+        net.delta_u.push_back(du / std::max(1, h.n));  // per atom, like the energy features
+        if (int(net.delta_u.size()) >= net.target) {
+          if ((st = surrogate_train(e, net, e->opt.seed, 300))) return st;
+        }
+      }
+    }
+    if (!accepted && (st = undo_volume_move(e, s, old_box))) return st;
+  }
   if (accepted) {
     b.accepted++;
     b.window_accepted++;
-  } else {
-    if ((st = set_box(e, s, old_box.data()))) return st;
-    if ((st = set_positions(e, s, pos.data(), false))) return st;
   }
   if (b.window_attempts >= 10) {
     if (b.window_accepted < 0.25 * b.window_attempts) {
@@ -1177,7 +1391,15 @@ int mdb_get_barostat_stats(const mdb_engine* e, int32_t s, mdb_barostat_stats* o
   out->attempts = e->baro[s].attempts;
   out->accepted = e->baro[s].accepted;
   out->volume_scale = e->baro[s].volume_scale;
-  out->exact_evaluations = 2 * e->baro[s].attempts;
+  // the current state's energy every attempt, the proposal's when not screened
+  out->exact_evaluations = e->baro[s].attempts + e->baro[s].exact;
+  out->screened = e->baro[s].screened;
+  const Surrogate& net = e->baro[s].net;
+  out->surrogate_active = net.active && !net.disabled ? 1 : 0;
+  out->surrogate_disabled = net.disabled ? 1 : 0;
+  out->training_samples = int64_t(net.delta_u.size());
+  out->surrogate_rms = std::sqrt(net.err2);
+  out->training_loss = net.final_loss;
   return MDB_OK;
 }
 

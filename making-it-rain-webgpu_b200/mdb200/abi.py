@@ -132,6 +132,7 @@ class RunOptions(C.Structure):
         ("device", C.c_int32),
         ("flags", C.c_int32),
         ("tuning", C.POINTER(Tuning)),
+        ("surrogate_attempts", C.c_int32),
     ]
 
 
@@ -159,11 +160,13 @@ class Energies(C.Structure):
         ("degrees_of_freedom", C.c_double),
         ("virial", C.c_double * 9),
         ("pairs_within_cutoff", C.c_double),
+        ("molecular_virial", C.c_double * 9),
     ]
 
     def as_dict(self) -> dict:
-        out = {name: getattr(self, name) for name, _ in self._fields_ if name != "virial"}
+        out = {name: getattr(self, name) for name, _ in self._fields_ if name not in ("virial", "molecular_virial")}
         out["virial"] = list(self.virial)
+        out["molecular_virial"] = list(self.molecular_virial)
         return out
 
 
@@ -174,6 +177,11 @@ class BarostatStats(C.Structure):
         ("volume_scale", C.c_double),
         ("screened", C.c_int64),
         ("exact_evaluations", C.c_int64),
+        ("training_samples", C.c_int64),
+        ("surrogate_active", C.c_int32),
+        ("surrogate_disabled", C.c_int32),
+        ("surrogate_rms", C.c_double),
+        ("training_loss", C.c_double),
     ]
 
 
@@ -245,6 +253,10 @@ EXPORTS = {
     "mdb_get_neighbour_stats": (C.c_int, [_E, C.c_int32, C.POINTER(NeighbourStats)]),
     "mdb_memory_report": (C.c_int, [_E, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "mdb_profile_step": (C.c_int, [_E, C.c_int32, C.POINTER(Profile)]),
+    "mdb_mlp_gradient": (C.c_int, [C.POINTER(C.c_float)] * 3 + [C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mdb_mlp_fit": (C.c_int, [C.POINTER(C.c_float)] * 2 + [C.c_int32, C.c_int32, C.c_uint32, C.POINTER(C.c_float),
+                                                        C.POINTER(C.c_float)]),
+    "mdb_mlp_predict": (C.c_int, [C.POINTER(C.c_float)] * 2 + [C.c_int32, C.POINTER(C.c_float)]),
     "mdb_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunOptions), C.c_int32, C.POINTER(Tuning),
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mdb_reciprocal_noalloc": (

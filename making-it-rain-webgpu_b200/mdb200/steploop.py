@@ -77,6 +77,9 @@ class RunOptions:
     always_rebuild: bool = False
     # per-system (verlet_skin, sort_cell) pairs from `autotune`; None = defaults
     tuning: Optional[Sequence[tuple]] = None
+    # > 0: each barostat learns a screening network from that many exact
+    # attempts, then screens proposals by delayed acceptance
+    surrogate_attempts: int = 0
 
     def to_c(self) -> abi.RunOptions:
         o = abi.RunOptions()
@@ -91,6 +94,7 @@ class RunOptions:
         o.mesh[:] = list(self.mesh) if self.mesh is not None else [0, 0, 0]
         o.device = int(self.device)
         o.flags = (0 if self.graphs else abi.FLAG_NO_GRAPH) | (abi.FLAG_ALWAYS_REBUILD if self.always_rebuild else 0)
+        o.surrogate_attempts = int(self.surrogate_attempts)
         if self.tuning is not None:
             arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(a), float(b)) for a, b in self.tuning])
             o.tuning = C.cast(arr, C.POINTER(abi.Tuning))
@@ -256,7 +260,10 @@ class StepLoop:
         s = abi.BarostatStats()
         self._check(self._lib.mdb_get_barostat_stats(self._handle, system, C.byref(s)))
         return {"attempts": s.attempts, "accepted": s.accepted, "volumeScale": s.volume_scale,
-                "screened": s.screened, "exactEvaluations": s.exact_evaluations}
+                "screened": s.screened, "exactEvaluations": s.exact_evaluations,
+                "trainingSamples": s.training_samples, "surrogateActive": bool(s.surrogate_active),
+                "surrogateDisabled": bool(s.surrogate_disabled), "surrogateRms": s.surrogate_rms,
+                "trainingLoss": s.training_loss}
 
     def verlet_flags(self, system: int = 0) -> dict:
         """`StepLoop.verletFlags`, loop.ts:941."""
@@ -346,4 +353,49 @@ def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: 
     tuning = [(cache[size_bucket(s.particle_count)]["verlet_skin"], cache[size_bucket(s.particle_count)]["sort_cell"])
               for s in systems]
     return tuning, cache
+
+
+# ---- the barostat screening network's kernels on their own ---------------------
+MLP_IN, MLP_HIDDEN = 16, 64
+MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def mlp_gradient(params, x, t) -> tuple[float, np.ndarray]:
+    """Loss and gradient of the first min(n, 128) samples, by the CUDA kernel."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    tt = np.ascontiguousarray(t, dtype=np.float32)
+    g = np.zeros(MLP_PARAMS, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    status = abi.load().mdb_mlp_gradient(_fptr(p), _fptr(xx), _fptr(tt), int(tt.size), _fptr(g), _fptr(loss))
+    if status != abi.OK:
+        raise EngineError(status, abi.load().mdb_status_string(status).decode())
+    return float(loss[0]), g
+
+
+def mlp_fit(x, t, epochs: int, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Train the network on the device; (FP32 master weights, per-epoch loss)."""
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    tt = np.ascontiguousarray(t, dtype=np.float32)
+    params = np.zeros(MLP_PARAMS, dtype=np.float32)
+    losses = np.zeros(epochs, dtype=np.float32)
+    status = abi.load().mdb_mlp_fit(_fptr(xx), _fptr(tt), int(tt.size), int(epochs), int(seed) & 0xFFFFFFFF,
+                                    _fptr(params), _fptr(losses))
+    if status != abi.OK:
+        raise EngineError(status, abi.load().mdb_status_string(status).decode())
+    return params, losses
+
+
+def mlp_predict(params, x) -> np.ndarray:
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.zeros(xx.shape[0], dtype=np.float32)
+    status = abi.load().mdb_mlp_predict(_fptr(p), _fptr(xx), int(xx.shape[0]), _fptr(y))
+    if status != abi.OK:
+        raise EngineError(status, abi.load().mdb_status_string(status).decode())
+    return y
 

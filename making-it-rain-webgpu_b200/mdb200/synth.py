@@ -304,3 +304,9 @@ def config_ensemble_64(seed: int = 1, count: int = 64):
     for k in range(count):
         out.append(ensemble_member(rng, seed=seed * 1000 + k))
     return out
+
+
+def config_npt_100k(seed: int = 1, width: float = 10.0, frequency: int = 25):
+    """NPT: a cubic 10 nm TIP3P box (about 100,000 atoms) at 300 K and 1 bar,
+    Monte Carlo volume moves every 25 steps; mesh by the reference's rule."""
+    return water_box(width=width, seed=seed, barostat=(1.0, 300.0, frequency))

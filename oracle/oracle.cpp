@@ -1397,6 +1397,59 @@ int32_t orc_potential_virial(const mdb_system_desc* sys, const double* positions
   return p.status;
 }
 
+// The barostat screening network (no reference counterpart): inputs -> 64
+// tanh -> 64 tanh -> 1, parameters W1[64][16], b1[64], W2[64][64], b2[64],
+// w3[64], b3, in f64; the mean-squared-error loss over the first min(n, 128)
+// samples and its gradient by reverse accumulation.
+int32_t orc_mlp_gradient(const float* params, const float* x, const float* t, int32_t n, double* grad,
+                         double* loss) {
+  constexpr int I = 16, H = 64;
+  constexpr int oB1 = H * I, oW2 = oB1 + H, oB2 = oW2 + H * H, oW3 = oB2 + H, oB3 = oW3 + H, P = oB3 + 1;
+  if (!params || !x || !t || !grad || !loss || n <= 0) return MDB_ERR_INVALID_ARGUMENT;
+  const int B = std::min(n, 128);
+  std::vector<double> w(params, params + P);
+  std::fill(grad, grad + P, 0.0);
+  double l = 0;
+  for (int b = 0; b < B; ++b) {
+    const float* in = x + size_t(b) * I;
+    double h1[H], h2[H];
+    for (int j = 0; j < H; ++j) {
+      double a = w[oB1 + j];
+      for (int k = 0; k < I; ++k) a += w[j * I + k] * in[k];
+      h1[j] = std::tanh(a);
+    }
+    for (int j = 0; j < H; ++j) {
+      double a = w[oB2 + j];
+      for (int k = 0; k < H; ++k) a += w[oW2 + j * H + k] * h1[k];
+      h2[j] = std::tanh(a);
+    }
+    double y = w[oB3];
+    for (int j = 0; j < H; ++j) y += w[oW3 + j] * h2[j];
+    const double e = y - t[b];
+    l += e * e;
+    const double dy = 2 * e / B;
+    double d2[H], d1[H];
+    for (int j = 0; j < H; ++j) {
+      grad[oW3 + j] += dy * h2[j];
+      d2[j] = dy * w[oW3 + j] * (1 - h2[j] * h2[j]);
+    }
+    grad[oB3] += dy;
+    for (int k = 0; k < H; ++k) {
+      double a = 0;
+      for (int j = 0; j < H; ++j) a += w[oW2 + j * H + k] * d2[j];
+      d1[k] = a * (1 - h1[k] * h1[k]);
+    }
+    for (int j = 0; j < H; ++j) {
+      for (int k = 0; k < H; ++k) grad[oW2 + j * H + k] += d2[j] * h1[k];
+      grad[oB2 + j] += d2[j];
+      for (int k = 0; k < I; ++k) grad[j * I + k] += d1[j] * in[k];
+      grad[oB1 + j] += d1[j];
+    }
+  }
+  *loss = l / B;
+  return MDB_OK;
+}
+
 // ewald.ts:82 -- half the lattice, doubled; k-space only.
 int32_t orc_ewald_reciprocal(const mdb_system_desc* s, const double* pos, const double box[9],
                              double alpha, int32_t kmax, double* forces, double* energy) {

@@ -88,6 +88,12 @@ int32_t orc_potential(const mdb_system_desc* sys, const double* positions,
  * box), pairs, exceptions, bonded terms, the PME mesh sum and the 1/V
  * dispersion and net-charge corrections; restraints excluded.  No reference
  * counterpart.  Not thread-safe (a module-level accumulator). */
+/* The barostat screening network's mean-squared-error gradient over the
+ * first min(n, 128) samples, in f64 (the CUDA kernel's checker).  No reference
+ * counterpart. */
+int32_t orc_mlp_gradient(const float* params, const float* x, const float* t, int32_t n, double* grad,
+                         double* loss);
+
 int32_t orc_potential_virial(const mdb_system_desc* sys, const double* positions, const double box[9],
                              const int32_t* grid, int32_t threads, double* forces, orc_energies* out,
                              double virial[9]);

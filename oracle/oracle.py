@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
         "orc_bspline_moduli": (None, [C.c_int32, _dp]),
         "orc_potential": (C.c_int32, [_SD, _dp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, _dp,
                                       C.POINTER(Energies)]),
+        "orc_mlp_gradient": (C.c_int32, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                         C.c_int32, _dp, _dp]),
         "orc_potential_virial": (C.c_int32, [_SD, _dp, _dp, C.POINTER(C.c_int32), C.c_int32, _dp,
                                              C.POINTER(Energies), _dp]),
         "orc_ewald_reciprocal": (C.c_int32, [_SD, _dp, _dp, C.c_double, C.c_int32, _dp, _dp]),
@@ -141,6 +143,21 @@ def potential_virial(system: System, positions, box=None, grid=None, threads: in
     if status != 0:
         raise RuntimeError(f"oracle potential failed with status {status}")
     return e.as_dict(), f.reshape(-1, 3), w.reshape(3, 3)
+
+
+def mlp_gradient(params, x, t):
+    """f64 loss and gradient of the screening network (first min(n, 128) samples)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    tt = np.ascontiguousarray(t, dtype=np.float32)
+    g = np.zeros(p.size)
+    loss = C.c_double()
+    fp = C.POINTER(C.c_float)
+    status = lib().orc_mlp_gradient(p.ctypes.data_as(fp), xx.ctypes.data_as(fp), tt.ctypes.data_as(fp),
+                                    int(tt.size), _p(g), C.byref(loss))
+    if status != 0:
+        raise RuntimeError(f"oracle mlp gradient failed with status {status}")
+    return loss.value, g
 
 
 def ewald_reciprocal(system: System, positions, alpha: float, kmax: int, box=None):

@@ -63,7 +63,7 @@ def test_struct_layouts_match_the_header():
     """Field offsets the C compiler would give, checked by ctypes arithmetic."""
     from mdb200 import abi
 
-    assert C.sizeof(abi.Energies) == 8 * (18 + 9 + 1)
+    assert C.sizeof(abi.Energies) == 8 * (18 + 9 + 1 + 9)
     assert abi.SystemDesc.box.offset == 16
     assert abi.StateDesc.box.offset == 16
     assert abi.RunOptions.seed.offset == 32

@@ -72,3 +72,27 @@ def test_engine_virial_matches_oracle(oracle, workload):
     err = np.abs(got - want).max() / np.abs(want).max()
     print(workload, "virial\n", got, "\noracle\n", want, "\nmax rel", err)
     assert err < 2e-5, err
+
+
+@pytest.mark.gpu
+def test_engine_molecular_virial_is_the_molecular_scaling_derivative(oracle):
+    """tr(W_mol) = -dU/d ln s under scaling of molecule centres by s (the
+    barostat's move), by central differences of the oracle's energy."""
+    from mdb200 import steploop, synth
+
+    system, state = synth.water_box(n_waters=700, width=2.8, seed=5, grid=(28, 28, 28))
+    loop = steploop.StepLoop.from_parsed(system, state, steploop.RunOptions(mesh=(28, 28, 28)))
+    e, _ = loop.evaluate()
+    loop.destroy()
+    w_mol = np.array(e["molecular_virial"]).reshape(3, 3)
+    box = np.asarray(state.box)
+    h = 1e-7
+    u = []
+    for sgn in (1.0, -1.0):
+        s = np.exp(sgn * h)
+        p = oracle.scale_molecules(system, state.positions, s).reshape(-1, 3)
+        en, _ = oracle.potential(system, p, box=box * s, grid=(28, 28, 28), threads=8, forces=False)
+        u.append(en["potential"])
+    fd = -(u[0] - u[1]) / (2 * h)
+    print("tr W_mol", np.trace(w_mol), "finite difference", fd, "tr W (atomic)", sum(e["virial"][::4]))
+    assert abs(np.trace(w_mol) - fd) < 2e-5 * abs(fd) + 0.5
