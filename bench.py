@@ -169,7 +169,12 @@ def cpu_rate(config: str, steps_hint: int, budget_s: float, threads: int):
         value = len(members) / elapsed * NS_PER_DAY_PER_STEP_PER_S
         return value, 1, elapsed, (f"one MD step of each of the {len(members)} systems ({elapsed:.1f} s), "
                                    "system-ns/day summed")
-    system, state, _ = workload(config, seed=1)
+    if config == "npt-100k":
+        from mdb200 import synth
+
+        system, state = synth.config_npt_100k(seed=1)
+    else:
+        system, state, _ = workload(config, seed=1)
     sps, n, elapsed = cpu_time_oracle(system, state, steps_hint, budget_s, threads)
     return sps * NS_PER_DAY_PER_STEP_PER_S, n, elapsed, f"{n} MD steps of the same workload in {elapsed:.1f} s"
 
@@ -185,11 +190,13 @@ def main() -> None:
     ap.add_argument("--impl", default="mdb", choices=("mdb", "reference"))
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--surrogate-attempts", type=int, default=2000,
+                    help="npt-100k: exact attempts the screening network learns from (2,000 = 50,000 steps)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     config = args.config or default_config()
     if args.steps is None:
-        args.steps = 400 if config == "ensemble-64" else 12000
+        args.steps = {"ensemble-64": 400, "npt-100k": 2000}.get(config, 12000)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -200,7 +207,7 @@ def main() -> None:
             return
         threads = os.cpu_count() or 1
         value, n, elapsed, sample = cpu_rate(config, args.steps, min(args.cpu_budget * 6, 240.0), threads)
-        cfg = {"workload": config} if config == "ensemble-64" else workload(config, seed=1)[2]
+        cfg = {"workload": config} if config in ("ensemble-64", "npt-100k") else workload(config, seed=1)[2]
         print(json.dumps({
             "impl": "reference", "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": args.gpus,
             "steps": n, "warmup": 1, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
@@ -363,6 +370,46 @@ def main() -> None:
         result_loop, n_atoms = loop, cfg["atoms"]
         e2e_value = args.steps / e2e_s * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
         system, state = systems[0], states[0]
+    elif config == "npt-100k":
+        from mdb200 import synth
+
+        system, state = synth.config_npt_100k(seed=1 + rank)
+        frequency = system.barostat[2]
+        # the plain Monte Carlo barostat on the same box, timed the same way
+        plain = steploop.StepLoop.from_parsed(system, state, steploop.RunOptions(seed=7 + rank, device=local,
+                                                                                max_batch=args.stride))
+        plain_s, _ = timed(plain)
+        plain_stats = plain.barostat_statistics()
+        plain.destroy()
+        # the screened barostat: learn from the first attempts (untimed), then time
+        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
+                                   surrogate_attempts=args.surrogate_attempts)
+        loop = steploop.StepLoop.from_parsed(system, state, opts)
+        t_train = time.perf_counter()
+        loop.run(args.surrogate_attempts * frequency)
+        t_train = time.perf_counter() - t_train
+        before = loop.barostat_statistics()
+        total_s, clock_summary = timed(loop)
+        after = loop.barostat_statistics()
+        steps_per_s = args.steps / total_s
+        value = steps_per_s * NS_PER_DAY_PER_STEP_PER_S * world
+        plain_value = args.steps / plain_s * NS_PER_DAY_PER_STEP_PER_S * world
+        attempts = after["attempts"] - before["attempts"]
+        cfg = {"workload": "NPT TIP3P cube 10 nm, 1 bar, 300 K, Monte Carlo volume move every "
+                           f"{frequency} steps, screened by the device-trained network",
+               "atoms": system.particle_count,
+               "plain_barostat_ns_per_day": plain_value, "screened_over_plain": value / plain_value,
+               "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
+                             "active": after["surrogateActive"], "rms_kj_mol": after["surrogateRms"],
+                             "attempts_timed": attempts,
+                             "exact_per_attempt": (after["exactEvaluations"] - before["exactEvaluations"])
+                                                  / max(1, attempts),
+                             "screened_timed": after["screened"] - before["screened"],
+                             "plain_exact_per_attempt": plain_stats["exactEvaluations"]
+                                                        / max(1, plain_stats["attempts"])}}
+        e2e_s, h2d, d2h = end_to_end(loop, [state])
+        e2e_value = args.steps / e2e_s * NS_PER_DAY_PER_STEP_PER_S * world
+        result_loop, n_atoms = loop, system.particle_count
     else:
         system, state, cfg = workload(config, seed=1 + rank)
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride)

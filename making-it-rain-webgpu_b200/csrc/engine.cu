@@ -56,7 +56,7 @@ struct Surrogate {
   bool active = false;            // trained: proposals go through the two-stage test
   bool disabled = false;          // the exact stage judged it too inaccurate: plain barostat
   std::vector<float> feats;       // raw features of every exact attempt, kMlpIn each
-  std::vector<double> delta_u;    // exact potential change of those attempts per atom, kJ/mol
+  std::vector<double> delta_u;    // exact change minus its first-order term, per atom, kJ/mol
   double mu[kMlpIn] = {}, sd[kMlpIn] = {}, mu_t = 0, sd_t = 1;
   double err2 = 0;                // running mean square of (predicted - exact) change
   int64_t judged = 0;
@@ -917,7 +917,13 @@ int set_box(mdb_engine* e, int s, const double* box) {
 // ---- the barostat's screening network (no reference counterpart) ----------
 // Inputs: dlnV, the energy components and the molecular virial's diagonal per
 // atom, the box diagonal, and the first-order change -tr(W_mol) dlnV / 3 per
-// atom; the target is the potential change per atom.
+// atom.  The network learns what the first-order term misses: its target is
+// (dU - first order) per atom, so its error stays on the kT scale however
+// large the system (the first-order term itself grows with it).
+double first_order_change(const mdb_energies& en, double dlnv) {
+  return -(en.molecular_virial[0] + en.molecular_virial[4] + en.molecular_virial[8]) * dlnv / 3.0;
+}
+
 void surrogate_features(const mdb_energies& en, const HostSystem& h, const double* box, double dlnv,
                         double* f) {
   const double n = std::max(1, h.n);
@@ -1016,7 +1022,7 @@ int surrogate_predict(mdb_engine* e, Surrogate& net, const HostSystem& h, const 
   float y = 0;
   CUDA_TRY(e, cudaMemcpyAsync(&y, net.y, sizeof(float), cudaMemcpyDeviceToHost, e->s0));
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  *out = (double(y) * net.sd_t + net.mu_t) * std::max(1, h.n);
+  *out = first_order_change(en, dlnv) + (double(y) * net.sd_t + net.mu_t) * std::max(1, h.n);
   return MDB_OK;
 }
 
@@ -1110,7 +1116,8 @@ int barostat_attempt(mdb_engine* e, int s) {
         double f[kMlpIn];
         surrogate_features(e0, h, old_box.data(), dlnv, f);
         for (double v : f) net.feats.push_back(float(v));
-        net.delta_u.push_back(du / std::max(1, h.n));  // per atom, like the energy features
+        // what the first-order term misses, per atom like the energy features
+        net.delta_u.push_back((du - first_order_change(e0, dlnv)) / std::max(1, h.n));
         if (int(net.delta_u.size()) >= net.target) {
           if ((st = surrogate_train(e, net, e->opt.seed, 300))) return st;
         }
