@@ -66,7 +66,10 @@ enum {
   /* Launch every kernel directly instead of replaying captured CUDA graphs. */
   MDB_FLAG_NO_GRAPH = 1,
   /* Rebuild the tile list every step, whatever the displacement. */
-  MDB_FLAG_ALWAYS_REBUILD = 2
+  MDB_FLAG_ALWAYS_REBUILD = 2,
+  /* Run the list build's phases as separate kernel launches instead of one
+     cooperative launch (each phase then shows up on its own in a profiler). */
+  MDB_FLAG_PHASE_LAUNCHES = 4
 };
 
 /*
@@ -161,6 +164,8 @@ typedef struct mdb_state_desc {
 typedef struct mdb_tuning {
   double verlet_skin;  /* nm; list radius = cutoff + skin; default 0.15 (nonbonded.ts:227) */
   double sort_cell;    /* nm; width of the fractional cells of the spatial sort; default 0.25 */
+  int32_t tile_atoms;  /* atoms per cluster of the pair tiles, 8 or 32; default 8.  One shape per
+                          engine: a batch takes the first system's that sets one */
 } mdb_tuning;
 
 typedef struct mdb_run_options {
@@ -392,7 +397,7 @@ int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* cha
 
 /*
  * Autotuner (no reference counterpart).  Times every candidate of a fixed grid
- * of (verlet_skin, sort_cell) on the device -- a temporary engine per
+ * of (tile_atoms, verlet_skin, sort_cell) on the device -- a temporary engine per
  * candidate, `steps` graph-replayed steps after a warm-up of the same length,
  * CUDA-event timed -- and returns the fastest in `best` and its ms per step.
  * `tried` (may be NULL) receives the number of candidates.  The state the

@@ -189,6 +189,31 @@ __device__ __forceinline__ int find_system(const int* prefix, int count, int ind
   return lo;
 }
 
+// Minimum image of a pair-coordinate difference (int32 at 2^pc_shift per nm).
+template <bool TRICLINIC>
+__device__ __forceinline__ void min_image(const SysDev& S, int& dx, int& dy, int& dz) {
+  if (!TRICLINIC) {
+    if (dx > S.pc_half[0]) dx -= S.pc_box[0];
+    if (dx < -S.pc_half[0]) dx += S.pc_box[0];
+    if (dy > S.pc_half[1]) dy -= S.pc_box[4];
+    if (dy < -S.pc_half[1]) dy += S.pc_box[4];
+    if (dz > S.pc_half[2]) dz -= S.pc_box[8];
+    if (dz < -S.pc_half[2]) dz += S.pc_box[8];
+  } else {
+    // Sequential reduction against c, b, a (nonbonded.ts:241), the count
+    // estimated in f32 and applied in integers.
+    const int kc = __float2int_rn(dz * S.pc_inv_diag[2]);
+    dz -= kc * S.pc_box[8];
+    dy -= kc * S.pc_box[7];
+    dx -= kc * S.pc_box[6];
+    const int kb = __float2int_rn(dy * S.pc_inv_diag[1]);
+    dy -= kb * S.pc_box[4];
+    dx -= kb * S.pc_box[3];
+    const int ka = __float2int_rn(dx * S.pc_inv_diag[0]);
+    dx -= ka * S.pc_box[0];
+  }
+}
+
 // u = r . M on the mesh, exactly in 2^32 fixed point, for the spline argument
 // of the PME spread and gather.  r is the 2^32 fixed-point position.
 __device__ __forceinline__ long long fixed_mul(long long a, long long b) {

@@ -22,6 +22,8 @@ struct Dev {
   const SysDev* sys;
   RunDev run;
   int n_atoms, n_slots, n_blocks, n_cells, n_units, n_iblk;
+  int cluster;        // atoms per cluster of the tile list: 8 or 32 (n_blocks counts clusters)
+  int any_triclinic;  // some system's box is triclinic: the pair kernel takes the general minimum image
 
   // atoms, original order
   long long *px, *py, *pz;
@@ -46,7 +48,8 @@ struct Dev {
   const int* slot_sys;
 
   // blocks
-  float4 *bb_lo, *bb_hi;
+  float4 *bb_lo, *bb_hi;  // per cluster
+  float4 *sb_lo, *sb_hi;  // per 32-slot super-cluster (the cluster boxes themselves when clusters are 32)
   int* tile_cnt;
   int* tile_start;
   const int* block_sys;

@@ -42,6 +42,10 @@ using namespace mdb;
 namespace {
 
 constexpr double kCellWidth = 0.25;  // nm, fractional cells of the spatial sort
+constexpr int kDefaultCluster = 8;   // atoms per cluster of the tile list
+// Capacity of the dense tile list, per cluster: about three times the mean
+// row at a 0.2 nm skin in water (~120 tiles for 8-atom clusters, ~90 for 32).
+int row_cap_for(int cluster) { return cluster == 8 ? 384 : 192; }
 constexpr int kFftTile = 8;  // kz columns per y- and x-pass CTA
 
 struct Allocation {
@@ -95,6 +99,7 @@ struct mdb_engine {
   int n_mesh_items = 0;
   std::vector<int> fft_x_sys;  // system of each x-pass work item
   bool coop_list = false;      // the list kernels run as one cooperative launch
+  int cluster = 8;                 // atoms per cluster of the tile list (8 or 32), per engine
   std::vector<double> skin;        // per system, nm
   std::vector<int> mol_first, mol_count;  // per system: its molecules in d.mol_off
   double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel
@@ -300,10 +305,19 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   const double default_skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
   e->skin.assign(n, default_skin);
   e->sort_cell.assign(n, kCellWidth);
+  e->cluster = kDefaultCluster;
   if (e->opt.tuning) {
+    bool shape_set = false;
     for (int s = 0; s < n; ++s) {
       if (e->opt.tuning[s].verlet_skin > 0) e->skin[s] = e->opt.tuning[s].verlet_skin;
       if (e->opt.tuning[s].sort_cell > 0) e->sort_cell[s] = e->opt.tuning[s].sort_cell;
+      const int shape = e->opt.tuning[s].tile_atoms;
+      if (shape != 0 && shape != 8 && shape != 32)
+        return fail(e, MDB_ERR_INVALID_ARGUMENT, "tile_atoms must be 8 or 32");
+      if (shape && !shape_set) {  // one tile shape per engine: the first system's that names one
+        e->cluster = shape;
+        shape_set = true;
+      }
     }
     e->opt.tuning = nullptr;  // the caller's array is not kept
   }
@@ -360,8 +374,11 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     std::memset(&S, 0, sizeof(S));
     S.n_atoms = h.n;
     S.atom_off = atoms;
-    S.n_blocks = (h.n + 31) / 32;
-    S.n_slots = S.n_blocks * 32;
+    S.n_slots = (h.n + 31) / 32 * 32;
+    // clusters of the tile list; trailing ones may be empty so that cluster I
+    // of every system starts at slot I * cluster (their bounding boxes are
+    // inverted, so no tile ever includes them)
+    S.n_blocks = S.n_slots / e->cluster;
     S.slot_off = slots;
     S.block_off = blocks;
     double widths[3];
@@ -370,7 +387,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     S.n_cells = S.cdim[0] * S.cdim[1] * S.cdim[2];
     S.cell_off = cells;
     const long long all_pairs = (long long)S.n_blocks * (S.n_blocks + 1) / 2;
-    S.tile_cap = int(std::min<long long>(all_pairs, (long long)S.n_blocks * 192));
+    S.tile_cap = int(std::min<long long>(all_pairs, (long long)S.n_blocks * row_cap_for(e->cluster)));
     S.tile_off = tiles;
     S.energy_base = s * kECount;
     S.cut2 = float(h.cutoff * h.cutoff);
@@ -558,6 +575,9 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.n_atoms = atoms;
   d.n_slots = slots;
   d.n_blocks = blocks;
+  d.cluster = e->cluster;
+  d.any_triclinic = 0;
+  for (int s = 0; s < n; ++s) d.any_triclinic |= e->sd[s].triclinic ? 1 : 0;
   d.n_cells = cells;
   d.n_units = units_n;
   d.n_iblk = iblk;
@@ -600,6 +620,14 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.slot_sys = tmp_i;
   TRY(alloc(e, "block bounds lo", d.bb_lo, blocks));
   TRY(alloc(e, "block bounds hi", d.bb_hi, blocks));
+  if (e->cluster < 32) {
+    TRY(alloc(e, "super-cluster bounds lo", d.sb_lo, blocks / (32 / e->cluster)));
+    TRY(alloc(e, "super-cluster bounds hi", d.sb_hi, blocks / (32 / e->cluster)));
+  } else {
+    d.sb_lo = d.bb_lo;
+    d.sb_hi = d.bb_hi;
+  }
+
   TRY(alloc(e, "tile row count", d.tile_cnt, blocks));
   TRY(alloc(e, "tile row start", d.tile_start, blocks));
   TRY(upload(e, "block system", tmp_i, block_sys));
@@ -612,13 +640,14 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(upload(e, "cell order map", tmp_i, cell_map));
   d.cell_map = tmp_i;
   TRY(alloc(e, "tiles", d.tiles, tiles));
-  TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * 32));
+  TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
   TRY(alloc(e, "tile count", d.tile_count, n));
   TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
   TRY(alloc(e, "rebuild flag", d.rebuild_flag, n));
   TRY(alloc(e, "rebuild now", d.rebuild_now, n));
   TRY(alloc(e, "any rebuild", d.any_rebuild, 1));
   TRY(alloc(e, "status", d.err, n));
+
   TRY(alloc(e, "rebuild count", d.rebuild_count, n));
   TRY(alloc(e, "launch ticket", d.global_ticket, 1));
   TRY(alloc(e, "list grid barrier", d.list_barrier, 2));
@@ -748,6 +777,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   } else if (prepare_list_kernel(e->device) > 0) {
     e->coop_list = true;
   }
+  if (e->opt.flags & MDB_FLAG_PHASE_LAUNCHES) e->coop_list = false;
   return MDB_OK;
 }
 
@@ -1247,18 +1277,21 @@ int mdb_system_count(const mdb_engine* e, int32_t* out) {
   return MDB_OK;
 }
 
-// The candidate grid: list skin (rebuild frequency against tile count) and
-// spatial-sort cell width (how compact a 32-atom block is).
+// The candidate grid: tile shape (8x8 or 32x32 clusters), list skin (rebuild
+// frequency against tile count) and spatial-sort cell width (how compact a
+// cluster is).
 int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
                  int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried) {
   if (!system || !state || !options || !best || steps <= 0) return MDB_ERR_INVALID_ARGUMENT;
   static const double kSkins[] = {0.10, 0.15, 0.20};
   static const double kCells[] = {0.20, 0.25, 0.35};
+  static const int kShapes[] = {8, 32};
   double best_ms = std::numeric_limits<double>::infinity();
   int count = 0, last = MDB_OK;
+  for (int shape : kShapes)
   for (double skin : kSkins)
     for (double cell : kCells) {
-      mdb_tuning t{skin, cell};
+      mdb_tuning t{skin, cell, shape};
       mdb_run_options o = *options;
       o.tuning = &t;
       mdb_engine* e = nullptr;

@@ -84,41 +84,45 @@ __device__ void phase_cells_assign(const Dev& d) {
   }
 }
 
-// Exclusive scan of `in[0..n)` into `out`, one block, in order.  Returns total.
+// Exclusive scan of `in[0..n)` into `out`, one block, in order.  Returns the
+// total.  Each warp owns a contiguous segment: pass one sums the segments
+// (coalesced), the block adds up the warps before each, pass two scans every
+// segment 32 elements at a time from its carry.
 __device__ int block_exclusive_scan(const int* in, int* out, int n) {
-  __shared__ int warp_sums[kThreads / 32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
+  __shared__ int warp_total[kThreads / 32];
+  __shared__ int total;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int per = ((n + nw - 1) / nw + 31) / 32 * 32;
+  const int lo = min(n, warp * per), hi = min(n, lo + per);
+  int sum = 0;
+  for (int i = lo + lane; i < hi; i += 32) sum += in[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0) warp_total[warp] = sum;
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int base = 0; base < n; base += blockDim.x) {
-    const int i = base + threadIdx.x;
-    const int v = i < n ? in[i] : 0;
+  int carry = 0;
+  for (int w = 0; w < warp; ++w) carry += warp_total[w];
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < nw; ++w) t += warp_total[w];
+    total = t;
+  }
+  for (int base = lo; base < hi; base += 32) {
+    const int i = base + lane;
+    const int v = i < hi ? in[i] : 0;
     int x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += y;
     }
-    if (lane == 31) warp_sums[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      int w = lane < (kThreads / 32) ? warp_sums[lane] : 0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, w, o);
-        if (lane >= o) w += y;
-      }
-      if (lane < (kThreads / 32)) warp_sums[lane] = w;
-    }
-    __syncthreads();
-    const int before = (warp > 0 ? warp_sums[warp - 1] : 0) + carry;
-    if (i < n) out[i] = before + x - v;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = before + x;
-    __syncthreads();
+    if (i < hi) out[i] = carry + x - v;
+    carry += __shfl_sync(0xffffffffu, x, 31);
   }
-  return carry;
+  __syncthreads();
+  const int t = total;
+  __syncthreads();  // the shared words are free for the next call
+  return t;
 }
 
 __device__ void phase_cells_scan(const Dev& d) {
@@ -178,48 +182,71 @@ __device__ void phase_wrap(const Dev& d) {
   }
 }
 
-// Warp per block: parameters in slot order, bounding box, and the reference
-// positions the displacement test measures against.
+// A group of C lanes per cluster (32/C clusters per warp): parameters in slot
+// order, the cluster's bounding box, and the reference positions the
+// displacement test measures against.  Every lane takes part in every
+// shuffle; only the writes depend on whether the cluster's system rebuilds.
+template <int C>
 __device__ void phase_tiles_blocks(const Dev& d) {
-  const int lane = threadIdx.x & 31;
+  constexpr int G = 32 / C;
+  const int lane = threadIdx.x & 31, g = lane / C, l = lane & (C - 1);
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < d.n_blocks; b += warps) {
-    const int s = d.block_sys[b];
-    if (!d.rebuild_now[s]) continue;
+  for (int wb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wb * G < d.n_blocks; wb += warps) {
+    const int b = wb * G + g;
+    const bool valid = b < d.n_blocks;
+    const int s = valid ? d.block_sys[b] : 0;
+    const bool work = valid && d.rebuild_now[s];
     const SysDev& S = d.sys[s];
-    const int gs = b * 32 + lane;
-    const int a = d.order[gs];
+    const int gs = b * C + l;
+    const int a = work ? d.order[gs] : -1;
     float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
-    if (a >= 0) {
-      d.prm[gs] = d.prm_atom[a];
-      d.refx[a] = d.px[a];
-      d.refy[a] = d.py[a];
-      d.refz[a] = d.pz[a];
-      const int4 p = d.pc[gs];
-      lo[0] = hi[0] = p.x * S.pc_inv;
-      lo[1] = hi[1] = p.y * S.pc_inv;
-      lo[2] = hi[2] = p.z * S.pc_inv;
-    } else {
-      d.prm[gs] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (work) {
+      if (a >= 0) {
+        d.prm[gs] = d.prm_atom[a];
+        d.refx[a] = d.px[a];
+        d.refy[a] = d.py[a];
+        d.refz[a] = d.pz[a];
+        const int4 p = d.pc[gs];
+        lo[0] = hi[0] = p.x * S.pc_inv;
+        lo[1] = hi[1] = p.y * S.pc_inv;
+        lo[2] = hi[2] = p.z * S.pc_inv;
+      } else {
+        d.prm[gs] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
-        hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+      for (int o = C / 2; o > 0; o >>= 1) {
+        lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o, C));
+        hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o, C));
       }
-    if (lane == 0) {
+    if (work && l == 0) {
       d.bb_lo[b] = make_float4(lo[0], lo[1], lo[2], 0.f);
       d.bb_hi[b] = make_float4(hi[0], hi[1], hi[2], 0.f);
+    }
+    if (C < 32) {
+      // the warp's 32/C clusters form one super-cluster (a system's clusters
+      // start at a multiple of 32 slots, so it never straddles two systems)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int o = C; o < 32; o <<= 1) {
+          lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+          hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+      if (work && lane == 0) {
+        d.sb_lo[wb] = make_float4(lo[0], lo[1], lo[2], 0.f);
+        d.sb_hi[wb] = make_float4(hi[0], hi[1], hi[2], 0.f);
+      }
     }
   }
 }
 
-// Do blocks I and J of one system come within cutoff + skin under some
-// periodic image?  Box-to-box gap distance, minimised over images.
-__device__ __forceinline__ bool blocks_near(const SysDev& S, const Dev& d, int I, int J) {
-  const float4 li = d.bb_lo[I], hi_ = d.bb_hi[I], lj = d.bb_lo[J], hj = d.bb_hi[J];
+// Do two boxes of one system come within cutoff + skin under some periodic
+// image?  Box-to-box gap distance, minimised over images.  An empty
+// cluster's box is inverted (lo = +3e38, hi = -3e38): its gap is infinite.
+__device__ __forceinline__ bool boxes_near(const SysDev& S, float4 li, float4 hi_, float4 lj, float4 hj) {
   const float hx = 0.5f * (hi_.x - li.x) + 0.5f * (hj.x - lj.x);
   const float hy = 0.5f * (hi_.y - li.y) + 0.5f * (hj.y - lj.y);
   const float hz = 0.5f * (hi_.z - li.z) + 0.5f * (hj.z - lj.z);
@@ -250,21 +277,102 @@ __device__ __forceinline__ bool blocks_near(const SysDev& S, const Dev& d, int I
   return best < S.list2;
 }
 
-__device__ void phase_tiles_count(const Dev& d) {
+__device__ __forceinline__ bool blocks_near(const SysDev& S, const Dev& d, int I, int J) {
+  return boxes_near(S, d.bb_lo[I], d.bb_hi[I], d.bb_lo[J], d.bb_hi[J]);
+}
+
+// Position of the k-th (from 0) set bit of m, or -1.
+__device__ __forceinline__ int nth_set_bit(unsigned int m, int k) {
+  for (int i = 0; i < k && m; ++i) m &= m - 1;
+  return m ? __ffs(m) - 1 : -1;
+}
+
+// Tiles of row I, in ascending J.  The search is two-level: the 32-slot
+// super-cluster of J (kSub = 32 / C clusters) must come near I's cluster
+// before the clusters inside it are tested, 32 / kSub super-clusters to a
+// pass of the warp, and every near tile is written by its own lane.  The
+// count pass (WRITE false) sizes the rows; after the scan the fill pass
+// (WRITE true) writes them at their place in the dense list.  Rows vary a lot:
+// a cluster that straddles a jump of the space-filling curve (where it leaves
+// the sort grid and comes back) has a large box and a long row.
+template <int C, bool WRITE>
+__device__ void phase_tiles_find(const Dev& d) {
+  constexpr int kSub = 32 / C;         // clusters per super-cluster
+  constexpr int kBatch = 32 / kSub;    // super-clusters per pass
+  constexpr int kWords = C * C / 32;   // mask words per tile
+  constexpr unsigned kRowAll = C == 32 ? 0xffffffffu : ((1u << C) - 1u);
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  const unsigned below = (1u << lane) - 1u;
   for (int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < d.n_blocks; I += warps) {
     const int s = d.block_sys[I];
     if (!d.rebuild_now[s]) continue;
     const SysDev& S = d.sys[s];
-    const int end = S.block_off + S.n_blocks;
+    // the row's tiles go to [base, base + cap) of the dense list
+    const long long base = static_cast<long long>(S.tile_off) + (WRITE ? d.tile_start[I] : 0);
+    const int cap = WRITE ? min(d.tile_cnt[I], S.tile_cap - d.tile_start[I]) : 0;
+    const int sI = I / kSub, sEnd = (S.block_off + S.n_blocks) / kSub;
+    const float4 li = d.bb_lo[I], hi_ = d.bb_hi[I];
+    const int Il = I - S.block_off;
     int count = 0;
-    for (int J0 = I; J0 < end; J0 += 32) {
-      const int J = J0 + lane;
-      const bool near = J < end && blocks_near(S, d, I, J);
-      count += __popc(__ballot_sync(0xffffffffu, near));
+    for (int J0 = sI; J0 < sEnd; J0 += 32) {
+      const int SJ = J0 + lane;
+      const bool near = SJ < sEnd && boxes_near(S, li, hi_, d.sb_lo[SJ], d.sb_hi[SJ]);
+      const unsigned int supers = __ballot_sync(0xffffffffu, near);
+      if (C == 32) {
+        // no super level: the boxes tested are the clusters themselves, and a
+        // 32x32 tile's mask is one word per row, so every lane writes its row
+        const unsigned int found = __ballot_sync(0xffffffffu, near && SJ >= I);
+        unsigned int f = found;
+        while (f) {
+          const int src = __ffs(f) - 1;
+          f &= f - 1;
+          const int Jt = J0 + src;
+          const int pos = count + __popc(found & ((1u << src) - 1u));
+          if (WRITE && pos < cap) {
+            if (lane == 0) d.tiles[base + pos] = make_int2(I, Jt);
+            const int Jl = Jt - S.block_off;
+            const int nj = max(0, min(C, S.n_atoms - Jl * C));
+            unsigned int valid = nj >= C ? kRowAll : ((1u << nj) - 1u);
+            if (Jt == I) valid &= lane == C - 1 ? 0u : (kRowAll << (lane + 1));
+            if (Il * C + lane >= S.n_atoms) valid = 0u;
+            d.masks[(base + pos) * kWords + lane] = valid;
+          }
+        }
+        count += __popc(found);
+        continue;
+      }
+      unsigned int rest = supers;
+      while (rest) {
+        // lanes k * kSub .. k * kSub + kSub - 1 take the k-th remaining near super-cluster
+        const int k = lane / kSub, sub = lane % kSub;
+        const int nth = nth_set_bit(rest, k);
+        const int J = nth >= 0 ? (J0 + nth) * kSub + sub : -1;
+        const bool tile = J >= I && boxes_near(S, li, hi_, d.bb_lo[J], d.bb_hi[J]);
+        const unsigned int found = __ballot_sync(0xffffffffu, tile);
+        const int at = count + __popc(found & below);
+        if (WRITE && tile && at < cap) {
+          d.tiles[base + at] = make_int2(I, J);
+          const int Jl = J - S.block_off;
+          const int nj = max(0, min(C, S.n_atoms - Jl * C));
+          const unsigned int cols = nj >= C ? kRowAll : ((1u << nj) - 1u);
+          unsigned int words[kWords];
+#pragma unroll
+          for (int w = 0; w < kWords; ++w) words[w] = 0u;
+#pragma unroll
+          for (int r = 0; r < C; ++r) {
+            unsigned int row = Il * C + r < S.n_atoms ? cols : 0u;
+            if (J == I) row &= r == C - 1 ? 0u : ((kRowAll << (r + 1)) & kRowAll);
+            words[(r * C) >> 5] |= row << ((r * C) & 31);
+          }
+#pragma unroll
+          for (int w = 0; w < kWords; ++w) d.masks[(base + at) * kWords + w] = words[w];
+        }
+        count += __popc(found);
+        for (int b = 0; b < kBatch && rest; ++b) rest &= rest - 1;  // the super-clusters this pass took
+      }
     }
-    if (lane == 0) d.tile_cnt[I] = count;
+    if (!WRITE && lane == 0) d.tile_cnt[I] = count;
   }
 }
 
@@ -280,41 +388,8 @@ __device__ void phase_tiles_scan(const Dev& d) {
   }
 }
 
-__device__ void phase_tiles_fill(const Dev& d) {
-  const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < d.n_blocks; I += warps) {
-    const int s = d.block_sys[I];
-    if (!d.rebuild_now[s]) continue;
-    const SysDev& S = d.sys[s];
-    const int end = S.block_off + S.n_blocks;
-    const int Il = I - S.block_off;
-    const bool row_valid = Il * 32 + lane < S.n_atoms;
-    int at = d.tile_start[I];
-    for (int J0 = I; J0 < end; J0 += 32) {
-      const int J = J0 + lane;
-      const bool near = J < end && blocks_near(S, d, I, J);
-      unsigned int bits = __ballot_sync(0xffffffffu, near);
-      while (bits) {
-        const int k = __ffs(bits) - 1;
-        bits &= bits - 1;
-        const int Jk = J0 + k;
-        if (at < S.tile_cap) {
-          const int t = S.tile_off + at;
-          if (lane == 0) d.tiles[t] = make_int2(I, Jk);
-          const int Jl = Jk - S.block_off;
-          const int nj = min(32, S.n_atoms - Jl * 32);
-          unsigned int valid = nj >= 32 ? 0xffffffffu : ((1u << nj) - 1u);
-          if (Jk == I) valid &= lane == 31 ? 0u : (0xffffffffu << (lane + 1));
-          d.masks[static_cast<long long>(t) * 32 + lane] = row_valid ? valid : 0u;
-        }
-        ++at;
-      }
-    }
-  }
-}
-
 // Clear the mask bit of every excluded pair in the tile that holds it.
+template <int C>
 __device__ void phase_tiles_exclusions(const Dev& d) {
   for (int e = grid_stride_start(); e < d.n_excl; e += grid_stride()) {
     const int s = d.excl_sys[e];
@@ -323,8 +398,8 @@ __device__ void phase_tiles_exclusions(const Dev& d) {
     const int2 pr = d.excl[e];
     int sa = d.rank[pr.x], sb = d.rank[pr.y];
     if (sa > sb) { const int t = sa; sa = sb; sb = t; }
-    const int I = S.block_off + (sa >> 5), J = S.block_off + (sb >> 5);
-    const int lane = sa & 31, bit = sb & 31;
+    const int I = S.block_off + sa / C, J = S.block_off + sb / C;
+    const int row = sa % C, bit = sb % C;
     int lo = d.tile_start[I];
     int hi = lo + d.tile_cnt[I];
     if (hi > S.tile_cap) hi = S.tile_cap;
@@ -335,8 +410,11 @@ __device__ void phase_tiles_exclusions(const Dev& d) {
       if (Jm < J) lo = mid + 1;
       else hi = mid;
     }
-    if (lo < d.tile_start[I] + d.tile_cnt[I] && lo < S.tile_cap && d.tiles[S.tile_off + lo].y == J)
-      atomicAnd(&d.masks[static_cast<long long>(S.tile_off + lo) * 32 + lane], ~(1u << bit));
+    if (lo < d.tile_start[I] + d.tile_cnt[I] && lo < S.tile_cap && d.tiles[S.tile_off + lo].y == J) {
+      const long long t = static_cast<long long>(S.tile_off) + lo;
+      if (C == 32) atomicAnd(&d.masks[t * 32 + row], ~(1u << bit));
+      else atomicAnd(&d.masks[t * (C * C / 32) + (row >> 2)], ~(1u << ((row & 3) * 8 + bit)));
+    }
   }
 }
 
@@ -390,6 +468,7 @@ __device__ bool grid_barrier(unsigned int* bar, int* err) {
 // One launch per step.  With no rebuild requested it only folds the pair
 // coordinates; otherwise it runs the sort and tile-list phases with a grid
 // barrier between them.
+template <int C>
 __global__ void __launch_bounds__(kThreads) k_list(Dev d) {
   const bool rebuild = *d.any_rebuild != 0;
   if (!rebuild) {
@@ -409,15 +488,15 @@ __global__ void __launch_bounds__(kThreads) k_list(Dev d) {
   if (!grid_barrier(d.list_barrier, err)) return;
   phase_wrap(d);
   if (!grid_barrier(d.list_barrier, err)) return;
-  phase_tiles_blocks(d);
+  phase_tiles_blocks<C>(d);
   if (!grid_barrier(d.list_barrier, err)) return;
-  phase_tiles_count(d);
+  phase_tiles_find<C, false>(d);
   if (!grid_barrier(d.list_barrier, err)) return;
   phase_tiles_scan(d);
   if (!grid_barrier(d.list_barrier, err)) return;
-  phase_tiles_fill(d);
+  phase_tiles_find<C, true>(d);
   if (!grid_barrier(d.list_barrier, err)) return;
-  phase_tiles_exclusions(d);
+  phase_tiles_exclusions<C>(d);
   if (!grid_barrier(d.list_barrier, err)) return;
   phase_tiles_finish(d);
 }
@@ -435,13 +514,28 @@ MDB_PHASE_KERNEL(cells_scan, true)
 MDB_PHASE_KERNEL(cells_scatter, true)
 MDB_PHASE_KERNEL(cells_order, true)
 MDB_PHASE_KERNEL(wrap, false)
-MDB_PHASE_KERNEL(tiles_blocks, true)
-MDB_PHASE_KERNEL(tiles_count, true)
 MDB_PHASE_KERNEL(tiles_scan, true)
-MDB_PHASE_KERNEL(tiles_fill, true)
-MDB_PHASE_KERNEL(tiles_exclusions, true)
 MDB_PHASE_KERNEL(tiles_finish, true)
 #undef MDB_PHASE_KERNEL
+#define MDB_PHASE_KERNEL_C(name)                                   \
+  template <int C>                                                 \
+  __global__ void __launch_bounds__(kThreads) k_##name(Dev d) {   \
+    if (!*d.any_rebuild) return;                                   \
+    phase_##name<C>(d);                                            \
+  }
+MDB_PHASE_KERNEL_C(tiles_blocks)
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_tiles_count(Dev d) {
+  if (!*d.any_rebuild) return;
+  phase_tiles_find<C, false>(d);
+}
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_tiles_fill(Dev d) {
+  if (!*d.any_rebuild) return;
+  phase_tiles_find<C, true>(d);
+}
+MDB_PHASE_KERNEL_C(tiles_exclusions)
+#undef MDB_PHASE_KERNEL_C
 
 int blocks_for(int n, int threads, int cap = 148 * 8) {
   const int b = (n + threads - 1) / threads;
@@ -455,7 +549,10 @@ int g_list_grid = 0;
 // Size the cooperative grid once: every block resident at the same time.
 int prepare_list_kernel(int device) {
   int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list, kThreads, 0) != cudaSuccess) return 0;
+  int per_sm8 = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list<32>, kThreads, 0) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm8, k_list<8>, kThreads, 0) != cudaSuccess) return 0;
+  per_sm = std::min(per_sm, per_sm8);
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
   int coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
@@ -475,7 +572,8 @@ bool launch_list(const Dev& d, cudaStream_t st) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_list, d) == cudaSuccess;
+  if (d.cluster == 8) return cudaLaunchKernelEx(&cfg, k_list<8>, d) == cudaSuccess;
+  return cudaLaunchKernelEx(&cfg, k_list<32>, d) == cudaSuccess;
 }
 
 void launch_rebuild_sort(const Dev& d, cudaStream_t st) {
@@ -490,14 +588,20 @@ void launch_wrap(const Dev& d, cudaStream_t st) {
   k_wrap<<<blocks_for(d.n_slots, kThreads), kThreads, 0, st>>>(d);
 }
 
-void launch_rebuild_tiles(const Dev& d, cudaStream_t st) {
+template <int C>
+void rebuild_tiles(const Dev& d, cudaStream_t st) {
   const int warp_blocks = blocks_for(d.n_blocks * 32, kThreads);
-  k_tiles_blocks<<<warp_blocks, kThreads, 0, st>>>(d);
-  k_tiles_count<<<warp_blocks, kThreads, 0, st>>>(d);
+  k_tiles_blocks<C><<<warp_blocks, kThreads, 0, st>>>(d);
+  k_tiles_count<C><<<warp_blocks, kThreads, 0, st>>>(d);
   k_tiles_scan<<<d.S < 148 ? d.S : 148, kThreads, 0, st>>>(d);
-  k_tiles_fill<<<warp_blocks, kThreads, 0, st>>>(d);
-  k_tiles_exclusions<<<blocks_for(d.n_excl, kThreads), kThreads, 0, st>>>(d);
+  k_tiles_fill<C><<<warp_blocks, kThreads, 0, st>>>(d);
+  k_tiles_exclusions<C><<<blocks_for(d.n_excl, kThreads), kThreads, 0, st>>>(d);
   k_tiles_finish<<<1, 32, 0, st>>>(d);
+}
+
+void launch_rebuild_tiles(const Dev& d, cudaStream_t st) {
+  if (d.cluster == 8) rebuild_tiles<8>(d, st);
+  else rebuild_tiles<32>(d, st);
 }
 
 }  // namespace mdb

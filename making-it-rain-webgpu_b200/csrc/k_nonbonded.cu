@@ -6,16 +6,20 @@
 // evaluated in f32 on the exact fixed-point pair vector, excluded pairs
 // skipped (the exceptions kernel takes their reciprocal part back out).
 //
-// The B200 shape is different: one warp owns one 32x32 tile of the list.  Lane
-// l keeps atom i of block I in registers and holds atom j of block J; after
-// every pair the j data and the j-force accumulator rotate one lane down with
-// `__shfl_sync`, so each pair is evaluated exactly once (Newton's third law,
-// half the arithmetic of the reference's gather) and no shared memory or
-// atomics are needed inside the tile.  Per tile the f32 partial sums become
-// int64 fixed point: the j side with one atomic per component, the i side in
-// registers across the consecutive tiles of its row.  Integer addition makes
-// the totals independent of the order tiles finish in, so repeat runs are
-// bit-identical.
+// The B200 shape is different.  Atoms are sorted into clusters of C (8 or 32)
+// consecutive slots along a space-filling curve and the list holds cluster
+// pairs (tiles).  A warp runs 32/C tiles at once, one per group of C lanes:
+// lane l of a group keeps atom i of cluster I in registers and holds atom j of
+// cluster J; after every pair the j data and the j-force accumulator rotate
+// one lane down inside the group (`__shfl_sync` of width C), so each pair is
+// evaluated exactly once (Newton's third law, half the arithmetic of the
+// reference's gather) with no shared memory and no atomics inside a tile.
+// Smaller clusters are tighter, so 8x8 tiles cover the cutoff sphere with
+// about half the pair slots of 32x32 ones at the price of more j-force
+// atomics per slot.  Per tile the f32 partial sums become int64 fixed point:
+// the j side with one atomic per component, the i side in registers across
+// the consecutive tiles of its row.  Integer addition makes the totals
+// independent of the order tiles finish in, so repeat runs are bit-identical.
 #include "device_state.h"
 
 namespace mdb {
@@ -23,36 +27,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ long long warp_sum64(long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-
-template <bool TRICLINIC>
-__device__ __forceinline__ void min_image(const SysDev& S, int& dx, int& dy, int& dz) {
-  if (!TRICLINIC) {
-    if (dx > S.pc_half[0]) dx -= S.pc_box[0];
-    if (dx < -S.pc_half[0]) dx += S.pc_box[0];
-    if (dy > S.pc_half[1]) dy -= S.pc_box[4];
-    if (dy < -S.pc_half[1]) dy += S.pc_box[4];
-    if (dz > S.pc_half[2]) dz -= S.pc_box[8];
-    if (dz < -S.pc_half[2]) dz += S.pc_box[8];
-  } else {
-    // Sequential reduction against c, b, a (nonbonded.ts:241), the count
-    // estimated in f32 and applied in integers.
-    const int kc = __float2int_rn(dz * S.pc_inv_diag[2]);
-    dz -= kc * S.pc_box[8];
-    dy -= kc * S.pc_box[7];
-    dx -= kc * S.pc_box[6];
-    const int kb = __float2int_rn(dy * S.pc_inv_diag[1]);
-    dy -= kb * S.pc_box[4];
-    dx -= kb * S.pc_box[3];
-    const int ka = __float2int_rn(dx * S.pc_inv_diag[0]);
-    dx -= ka * S.pc_box[0];
-  }
-}
 
 // erfc(x) = exp(-x^2) P(u): P fits erfcx on x in [0, 3.6] as a degree-7
 // polynomial in u = 3.111 t - 2.111, t = 1/(1 + x/2) (fit_erfcx.py in this
@@ -72,15 +46,36 @@ __device__ __forceinline__ float erfcx_poly(float x) {
   return p;
 }
 
-template <bool ENERGY, bool TRICLINIC>
+// Lanes of the group that holds `lane`, as a shuffle mask.
+template <int C>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+  return C == 32 ? kFull : (((1u << C) - 1u) << (lane & ~(C - 1)));
+}
+
+template <int C>
+__device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
+#pragma unroll
+  for (int o = C / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, C);
+  return v;
+}
+
+// The mask bits of row l (one bit per j of the tile).
+template <int C>
+__device__ __forceinline__ unsigned int row_bits(const unsigned int* masks, long long ti, int l) {
+  if (C == 32) return masks[ti * 32 + l];
+  return (masks[ti * (C * C / 32) + (l >> 2)] >> ((l & 3) * 8)) & 0xFFu;
+}
+
+template <int C, bool ENERGY, bool TRICLINIC>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
-                                           unsigned int mask, int lane, float& fix, float& fiy,
-                                           float& fiz, float& fjx, float& fjy, float& fjz,
-                                           float& ecoul, float& elj, int& pairs, float* vir) {
+                                           unsigned int mask, int l, float& fix, float& fiy, float& fiz,
+                                           float& fjx, float& fjy, float& fjz, float& ecoul, float& elj,
+                                           int& pairs, float* vir) {
   const float alpha = S.alpha, a2sp = S.alpha_2_sqrtpi, cut2 = S.cut2, inv = S.pc_inv;
+  const int src = (l + 1) & (C - 1);
 #pragma unroll 4
-  for (int k = 0; k < 32; ++k) {
-    const int jl = (lane + k) & 31;
+  for (int k = 0; k < C; ++k) {
+    const int jl = (l + k) & (C - 1);
     int dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
     min_image<TRICLINIC>(S, dx, dy, dz);
     const float rx = dx * inv, ry = dy * inv, rz = dz * inv;
@@ -120,30 +115,35 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
         vir[5] -= fs * ry * rz;
       }
     }
-    const int src = (lane + 1) & 31;
-    pj.x = __shfl_sync(kFull, pj.x, src);
-    pj.y = __shfl_sync(kFull, pj.y, src);
-    pj.z = __shfl_sync(kFull, pj.z, src);
-    qj.x = __shfl_sync(kFull, qj.x, src);
-    qj.y = __shfl_sync(kFull, qj.y, src);
-    qj.z = __shfl_sync(kFull, qj.z, src);
-    fjx = __shfl_sync(kFull, fjx, src);
-    fjy = __shfl_sync(kFull, fjy, src);
-    fjz = __shfl_sync(kFull, fjz, src);
+    pj.x = __shfl_sync(kFull, pj.x, src, C);
+    pj.y = __shfl_sync(kFull, pj.y, src, C);
+    pj.z = __shfl_sync(kFull, pj.z, src, C);
+    qj.x = __shfl_sync(kFull, qj.x, src, C);
+    qj.y = __shfl_sync(kFull, qj.y, src, C);
+    qj.z = __shfl_sync(kFull, qj.z, src, C);
+    fjx = __shfl_sync(kFull, fjx, src, C);
+    fjy = __shfl_sync(kFull, fjy, src, C);
+    fjz = __shfl_sync(kFull, fjz, src, C);
   }
 }
 
-template <bool ENERGY>
+// A warp takes a contiguous run of the list and walks it 32/C tiles at a
+// time; group g of the warp runs tile t + g.  Every lane keeps its own row
+// and system, because the groups of one warp may be at different ones.
+template <int C, bool ENERGY, bool TRICLINIC>
 __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
+  constexpr int G = 32 / C;
   const int lane = threadIdx.x & 31;
+  const int g = lane / C, l = lane & (C - 1);
+  const unsigned gmask = group_mask<C>(lane);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int total = d.tile_prefix[d.S];
-  const int per = (total + nwarps - 1) / nwarps;
-  int t = warp * per;
-  const int tend = min(total, t + per);
-  if (t >= tend) return;
-  int s = find_system(d.tile_prefix, d.S, t);
+  const int per = ((total + nwarps - 1) / nwarps + G - 1) / G * G;
+  const int t0 = warp * per;
+  const int tend = min(total, t0 + per);
+  if (t0 >= tend) return;
+  int s = find_system(d.tile_prefix, d.S, min(t0 + g, tend - 1));
 
   long long aix = 0, aiy = 0, aiz = 0;
   int cur_row = -1;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
 
   auto flush_row = [&]() {
     if (cur_row >= 0) {
-      const int gi = cur_row * 32 + lane;
+      const int gi = cur_row * C + l;
       if (aix | aiy | aiz) {
         add_fixed64(&d.fx[gi], aix);
         add_fixed64(&d.fy[gi], aiy);
@@ -161,56 +161,68 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
     }
     aix = aiy = aiz = 0;
   };
-  auto base_of = [&](int sys) { return d.sys[sys].energy_base; };
+  // energies of the group's tiles so far, into system `sys` (every lane of the
+  // group calls it together)
   auto flush_energy = [&](int sys) {
     if (ENERGY) {
-      const long long c = warp_sum64(ecoul64), l = warp_sum64(elj64), p = warp_sum64(pairs64);
-      if (lane == 0) {
-        const int base = d.sys[sys].energy_base;
-        add_fixed64(&d.energy[base + kECoulomb], c);
-        add_fixed64(&d.energy[base + kELj], l);
-        add_fixed64(&d.energy[base + kEPairs], p);
-      }
-      // slots: row-major 3x3, the symmetric pair tensor written to both halves
-      const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
+      const long long c = group_sum64<C>(ecoul64, gmask), lj = group_sum64<C>(elj64, gmask),
+                      p = group_sum64<C>(pairs64, gmask);
+      long long v[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const long long v = warp_sum64(vir64[k]);
-        if (lane == 0) {
-          add_fixed64(&d.energy[base_of(sys) + kEVirial0 + slot[k]], v);
-          if (mirror[k] >= 0) add_fixed64(&d.energy[base_of(sys) + kEVirial0 + mirror[k]], v);
+      for (int k = 0; k < 6; ++k) v[k] = group_sum64<C>(vir64[k], gmask);
+      if (l == 0) {
+        unsigned long long* e = &d.energy[d.sys[sys].energy_base];
+        if (c) add_fixed64(&e[kECoulomb], c);
+        if (lj) add_fixed64(&e[kELj], lj);
+        if (p) add_fixed64(&e[kEPairs], p);
+        // slots: row-major 3x3, the symmetric pair tensor written to both halves
+        const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          if (!v[k]) continue;
+          add_fixed64(&e[kEVirial0 + slot[k]], v[k]);
+          if (mirror[k] >= 0) add_fixed64(&e[kEVirial0 + mirror[k]], v[k]);
         }
-        vir64[k] = 0;
       }
       ecoul64 = elj64 = pairs64 = 0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) vir64[k] = 0;
     }
   };
 
-  for (; t < tend; ++t) {
-    while (t >= d.tile_prefix[s + 1]) {
-      flush_energy(s);
-      ++s;
+  for (int base = t0; base < tend; base += G) {
+    const int t = base + g;
+    const bool active = t < tend;  // the same for every lane of a group
+    unsigned int mask = 0u;
+    int4 pi = make_int4(0, 0, 0, 0), pj = pi;
+    float4 qi = make_float4(0.f, 0.f, 0.f, 0.f), qj = qi;
+    int gj = -1;
+    if (active) {
+      while (t >= d.tile_prefix[s + 1]) {
+        flush_energy(s);
+        ++s;
+      }
+      const SysDev& S = d.sys[s];
+      const long long ti = S.tile_off + (t - d.tile_prefix[s]);
+      mask = row_bits<C>(d.masks, ti, l);
+      const int2 tile = d.tiles[ti];
+      if (tile.x != cur_row) {
+        flush_row();
+        cur_row = tile.x;
+      }
+      const int gi = tile.x * C + l;
+      gj = tile.y * C + l;
+      pi = d.pc[gi];
+      qi = d.prm[gi];
+      pj = d.pc[gj];
+      qj = d.prm[gj];
     }
-    const SysDev& S = d.sys[s];
-    const long long ti = S.tile_off + (t - d.tile_prefix[s]);
-    const int2 tile = d.tiles[ti];
-    if (tile.x != cur_row) {
-      flush_row();
-      cur_row = tile.x;
-    }
-    const int gi = tile.x * 32 + lane, gj = tile.y * 32 + lane;
-    const int4 pi = d.pc[gi];
-    const float4 qi = d.prm[gi];
-    const int4 pj = d.pc[gj];
-    const float4 qj = d.prm[gj];
-    const unsigned int mask = d.masks[ti * 32 + lane];
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
     float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int np = 0;
-    if (S.triclinic)
-      tile_pairs<ENERGY, true>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np, vir);
-    else
-      tile_pairs<ENERGY, false>(S, pi, qi, pj, qj, mask, lane, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np, vir);
+    tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, l, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np,
+                                     vir);
+    if (!active) continue;
     aix += to_fixed(fix);
     aiy += to_fixed(fiy);
     aiz += to_fixed(fiz);
@@ -231,14 +243,25 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   flush_energy(s);
 }
 
-}  // namespace
-
-void launch_nonbonded(const Dev& d, bool energy, cudaStream_t st) {
+template <int C>
+void launch_shape(const Dev& d, bool energy, bool triclinic, cudaStream_t st) {
   // Persistent-style: a fixed grid of 148 SMs x 8 blocks of 8 warps, each warp
   // taking a contiguous run of tiles so consecutive tiles of a row share i.
   const int blocks = 148 * 8;
-  if (energy) k_nonbonded<true><<<blocks, kThreads, 0, st>>>(d);
-  else k_nonbonded<false><<<blocks, kThreads, 0, st>>>(d);
+  if (energy) {
+    if (triclinic) k_nonbonded<C, true, true><<<blocks, kThreads, 0, st>>>(d);
+    else k_nonbonded<C, true, false><<<blocks, kThreads, 0, st>>>(d);
+  } else {
+    if (triclinic) k_nonbonded<C, false, true><<<blocks, kThreads, 0, st>>>(d);
+    else k_nonbonded<C, false, false><<<blocks, kThreads, 0, st>>>(d);
+  }
+}
+
+}  // namespace
+
+void launch_nonbonded(const Dev& d, bool energy, cudaStream_t st) {
+  if (d.cluster == 8) launch_shape<8>(d, energy, d.any_triclinic != 0, st);
+  else launch_shape<32>(d, energy, d.any_triclinic != 0, st);
 }
 
 }  // namespace mdb

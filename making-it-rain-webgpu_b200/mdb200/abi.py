@@ -36,6 +36,7 @@ INTEGRATOR_VERLET = 1
 
 FLAG_NO_GRAPH = 1
 FLAG_ALWAYS_REBUILD = 2
+FLAG_PHASE_LAUNCHES = 4
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -113,7 +114,7 @@ class StateDesc(C.Structure):
 class Tuning(C.Structure):
     """`mdb_tuning` (no reference counterpart)."""
 
-    _fields_ = [("verlet_skin", C.c_double), ("sort_cell", C.c_double)]
+    _fields_ = [("verlet_skin", C.c_double), ("sort_cell", C.c_double), ("tile_atoms", C.c_int32)]
 
 
 class RunOptions(C.Structure):

@@ -75,7 +75,8 @@ class RunOptions:
     device: int = 0
     graphs: bool = True
     always_rebuild: bool = False
-    # per-system (verlet_skin, sort_cell) pairs from `autotune`; None = defaults
+    phase_launches: bool = False  # list build as separate launches (profiling)
+    # per-system (verlet_skin, sort_cell[, tile_atoms]) from `autotune`; None = defaults
     tuning: Optional[Sequence[tuple]] = None
     # > 0: each barostat learns a screening network from that many exact
     # attempts, then screens proposals by delayed acceptance
@@ -93,10 +94,12 @@ class RunOptions:
         o.max_batch = int(self.max_batch)
         o.mesh[:] = list(self.mesh) if self.mesh is not None else [0, 0, 0]
         o.device = int(self.device)
-        o.flags = (0 if self.graphs else abi.FLAG_NO_GRAPH) | (abi.FLAG_ALWAYS_REBUILD if self.always_rebuild else 0)
+        o.flags = ((0 if self.graphs else abi.FLAG_NO_GRAPH) | (abi.FLAG_ALWAYS_REBUILD if self.always_rebuild else 0)
+                   | (abi.FLAG_PHASE_LAUNCHES if self.phase_launches else 0))
         o.surrogate_attempts = int(self.surrogate_attempts)
         if self.tuning is not None:
-            arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(a), float(b)) for a, b in self.tuning])
+            arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(t[0]), float(t[1]), int(t[2]) if len(t) > 2 else 0)
+                                                    for t in self.tuning])
             o.tuning = C.cast(arr, C.POINTER(abi.Tuning))
             o._keep = arr  # the array must outlive the create call
         return o
@@ -325,8 +328,8 @@ def autotune(system: System, state: State, options: RunOptions | None = None, st
                               C.byref(ms), C.byref(tried))
     if status != abi.OK:
         raise _ERRORS.get(status, EngineError)(status, lib.mdb_status_string(status).decode())
-    return {"verlet_skin": best.verlet_skin, "sort_cell": best.sort_cell, "ms_per_step": ms.value,
-            "candidates": tried.value}
+    return {"verlet_skin": best.verlet_skin, "sort_cell": best.sort_cell, "tile_atoms": best.tile_atoms,
+            "ms_per_step": ms.value, "candidates": tried.value}
 
 
 def size_bucket(atoms: int) -> int:
@@ -350,7 +353,7 @@ def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: 
         members = sorted(members, key=lambda k: systems[k].particle_count)
         rep = members[len(members) // 2]
         cache[b] = autotune(systems[rep], states[rep], options, steps)
-    tuning = [(cache[size_bucket(s.particle_count)]["verlet_skin"], cache[size_bucket(s.particle_count)]["sort_cell"])
+    tuning = [tuple(cache[size_bucket(s.particle_count)][k] for k in ("verlet_skin", "sort_cell", "tile_atoms"))
               for s in systems]
     return tuning, cache
 

@@ -257,18 +257,22 @@ def test_octahedron_10k_steps_then_groups_match_oracle(mdb, oracle, octahedron):
 
 def test_autotune_picks_a_candidate_and_tuned_batch_equals_tuned_single(mdb):
     """The autotuner returns one of its candidates; a tuning passed per system
-    to a batch gives the same trajectory as the same tuning on a single engine."""
+    to a batch gives the same trajectory as the same tuning on a single engine
+    (the batch takes the first system's tile shape, so the single engines get
+    it too)."""
     from mdb200 import synth
 
     a = synth.water_box(n_waters=700, width=2.8, seed=3, grid=(28, 28, 28))
     b = synth.water_box(n_waters=900, width=3.1, seed=4, grid=(32, 32, 32))
     best = mdb.autotune(*a, steps=50)
     print("autotune", best)
-    assert best["candidates"] == 9
+    assert best["candidates"] == 18
     assert best["verlet_skin"] in (0.10, 0.15, 0.20) and best["sort_cell"] in (0.20, 0.25, 0.35)
-    tuning = [(best["verlet_skin"], best["sort_cell"]), (0.20, 0.35)]
+    assert best["tile_atoms"] in (8, 32)
+    tuning = [(best["verlet_skin"], best["sort_cell"], best["tile_atoms"]), (0.20, 0.35, 0)]
     single = []
     for (s, st), t in zip((a, b), tuning):
+        t = (t[0], t[1], tuning[0][2])
         loop = mdb.StepLoop.from_parsed(s, st, mdb.RunOptions(seed=5, tuning=[t]))
         loop.run(30)
         single.append(loop.positions())
