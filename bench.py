@@ -412,7 +412,12 @@ def main() -> None:
         result_loop, n_atoms = loop, system.particle_count
     else:
         system, state, cfg = workload(config, seed=1 + rank)
-        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride)
+        # the library's autotuner picks tile shape, skin and sort cell for this
+        # system (untimed, like graph capture); the timed run uses its choice
+        best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=200)
+        cfg["autotuner"] = {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}
+        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
+                                   tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"])])
         loop = steploop.StepLoop.from_parsed(system, state, opts)
         total_s, clock_summary = timed(loop)
         steps_per_s = args.steps / total_s

@@ -87,6 +87,7 @@ struct SysDev {
   int energy_base;
   // box, row-major a b c, reduced form; inverse M with f = r . M (M[v*3+u])
   float box_f[9];
+  float min_width;   // narrowest perpendicular width of the cell, nm
   float inv_f[9];
   long long box_fx[9];  // lattice vectors, 2^32 fixed point
   long long inv_fx[9];  // M, 2^32 fixed point (fold and cells)

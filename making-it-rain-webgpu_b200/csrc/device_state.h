@@ -50,6 +50,8 @@ struct Dev {
   // blocks
   float4 *bb_lo, *bb_hi;  // per cluster
   float4 *sb_lo, *sb_hi;  // per 32-slot super-cluster (the cluster boxes themselves when clusters are 32)
+  int* fold;              // per slot: the lattice translation of the last rebuild's fold (3 x 10 bits)
+  int4* tile_shift;       // per tile: lattice shift of J in pair-coordinate units; w = 1: per-pair minimum image
   int* tile_cnt;
   int* tile_start;
   const int* block_sys;

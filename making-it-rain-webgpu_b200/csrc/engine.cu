@@ -204,6 +204,9 @@ void fill_box(const HostSystem& h, SysDev& S, bool keep_shift) {
     S.inv_fx[i] = to_fixed_host(M[i]);
   }
   S.triclinic = (B[3] != 0 || B[6] != 0 || B[7] != 0) ? 1 : 0;
+  double widths[3];
+  perpendicular_widths(B, widths);
+  S.min_width = float(std::min({widths[0], widths[1], widths[2]}));
   // Pair coordinates: the folded extent plus one box stays below 2^31.
   const double ext = std::max({B[0] + std::fabs(B[3]) + std::fabs(B[6]), B[4] + std::fabs(B[7]), B[8]});
   int shift = int(std::floor(std::log2(std::ldexp(1.0, 30) / ext)));
@@ -641,6 +644,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.cell_map = tmp_i;
   TRY(alloc(e, "tiles", d.tiles, tiles));
   TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
+  TRY(alloc(e, "tile image shifts", d.tile_shift, tiles));
+  TRY(alloc(e, "fold translations", d.fold, slots));
   TRY(alloc(e, "tile count", d.tile_count, n));
   TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
   TRY(alloc(e, "rebuild flag", d.rebuild_flag, n));

@@ -32,6 +32,7 @@ __device__ __forceinline__ int grid_stride() { return gridDim.x * blockDim.x; }
 struct Folded {
   long long x, y, z;           // folded position, 2^32 fixed
   unsigned int fa, fb, fc;     // fractional parts, 2^-32 units
+  long long na, nb, nc;        // lattice translation taken off
 };
 
 __device__ __forceinline__ Folded fold(const SysDev& S, long long x, long long y, long long z) {
@@ -46,6 +47,9 @@ __device__ __forceinline__ Folded fold(const SysDev& S, long long x, long long y
   f.fa = static_cast<unsigned int>(fa & 0xffffffffll);
   f.fb = static_cast<unsigned int>(fb & 0xffffffffll);
   f.fc = static_cast<unsigned int>(fc & 0xffffffffll);
+  f.na = na;
+  f.nb = nb;
+  f.nc = nc;
   return f;
 }
 
@@ -166,8 +170,12 @@ __device__ void phase_cells_order(const Dev& d) {
   }
 }
 
-// Every step, every system: pair coordinates of each slot, folded into the
-// cell, as int32 at 2^pc_shift per nm (cell-list.wgsl:140 `wrap`).
+// Every step, every system: pair coordinates of each slot as int32 at
+// 2^pc_shift per nm (cell-list.wgsl:140 `wrap`).  A rebuild folds each atom
+// into the cell and records the lattice translation it took (three signed
+// 10-bit counts); between rebuilds the same translation is applied, so the
+// coordinates move continuously (an atom leaves the cell by at most half the
+// skin before the next rebuild) and the tiles' lattice shifts stay valid.
 __device__ void phase_wrap(const Dev& d) {
   for (int gs = grid_stride_start(); gs < d.n_slots; gs += grid_stride()) {
     const int a = d.order[gs];
@@ -175,10 +183,26 @@ __device__ void phase_wrap(const Dev& d) {
       d.pc[gs] = make_int4(0, 0, 0, 0);
       continue;
     }
-    const SysDev& S = d.sys[d.slot_sys[gs]];
-    const Folded f = fold(S, d.px[a], d.py[a], d.pz[a]);
-    d.pc[gs] = make_int4(to_pair_coordinate(f.x, S.pc_shift), to_pair_coordinate(f.y, S.pc_shift),
-                         to_pair_coordinate(f.z, S.pc_shift), 0);
+    const int s = d.slot_sys[gs];
+    const SysDev& S = d.sys[s];
+    long long na, nb, nc;
+    if (d.rebuild_now[s]) {
+      const Folded f = fold(S, d.px[a], d.py[a], d.pz[a]);
+      na = f.na;
+      nb = f.nb;
+      nc = f.nc;
+      d.fold[gs] = int((na & 1023) | ((nb & 1023) << 10) | ((nc & 1023) << 20));
+    } else {
+      const int w = d.fold[gs];
+      na = (w << 22) >> 22;
+      nb = (w << 12) >> 22;
+      nc = (w << 2) >> 22;
+    }
+    const long long x = d.px[a] - na * S.box_fx[0] - nb * S.box_fx[3] - nc * S.box_fx[6];
+    const long long y = d.py[a] - nb * S.box_fx[4] - nc * S.box_fx[7];
+    const long long z = d.pz[a] - nc * S.box_fx[8];
+    d.pc[gs] = make_int4(to_pair_coordinate(x, S.pc_shift), to_pair_coordinate(y, S.pc_shift),
+                         to_pair_coordinate(z, S.pc_shift), 0);
   }
 }
 
@@ -277,6 +301,63 @@ __device__ __forceinline__ bool boxes_near(const SysDev& S, float4 li, float4 hi
   return best < S.list2;
 }
 
+// The lattice shift (in pair-coordinate units, applied to J) of the image
+// that brings box J nearest box I, as boxes_near finds it.  w = 1 when that
+// one image might not hold every pair of the tile within the cutoff: when
+// 2 (|h_I| + |h_J|) + list + cutoff reaches the cell's narrowest width (h the
+// half-diagonals), another image of some pair could come inside the cutoff,
+// and the pair kernel takes the minimum image per pair instead.
+__device__ __forceinline__ int4 tile_image(const SysDev& S, float4 li, float4 hi_, float4 lj, float4 hj) {
+  float dx = 0.5f * (lj.x + hj.x) - 0.5f * (li.x + hi_.x);
+  float dy = 0.5f * (lj.y + hj.y) - 0.5f * (li.y + hi_.y);
+  float dz = 0.5f * (lj.z + hj.z) - 0.5f * (li.z + hi_.z);
+  const float* B = S.box_f;
+  const float kc = rintf(dz / B[8]);
+  dx -= kc * B[6]; dy -= kc * B[7]; dz -= kc * B[8];
+  const float kb = rintf(dy / B[4]);
+  dx -= kb * B[3]; dy -= kb * B[4];
+  const float ka = rintf(dx / B[0]);
+  dx -= ka * B[0];
+  int na = -int(ka), nb = -int(kb), nc = -int(kc);
+  if (S.triclinic) {
+    const float hx = 0.5f * (hi_.x - li.x) + 0.5f * (hj.x - lj.x);
+    const float hy = 0.5f * (hi_.y - li.y) + 0.5f * (hj.y - lj.y);
+    const float hz = 0.5f * (hi_.z - li.z) + 0.5f * (hj.z - lj.z);
+    float best = 3.0e38f;
+    int bi = 0, bj = 0, bk = 0;
+    for (int k = -1; k <= 1; ++k)
+      for (int j = -1; j <= 1; ++j)
+        for (int i = -1; i <= 1; ++i) {
+          const float x = dx + i * B[0] + j * B[3] + k * B[6];
+          const float y = dy + j * B[4] + k * B[7];
+          const float z = dz + k * B[8];
+          const float gx = fmaxf(fabsf(x) - hx, 0.f), gy = fmaxf(fabsf(y) - hy, 0.f), gz = fmaxf(fabsf(z) - hz, 0.f);
+          const float g = gx * gx + gy * gy + gz * gz;
+          if (g < best) {
+            best = g;
+            bi = i;
+            bj = j;
+            bk = k;
+          }
+        }
+    na += bi;
+    nb += bj;
+    nc += bk;
+  }
+  // wrapping 32-bit arithmetic: the pair kernel adds this to a coordinate and
+  // subtracts another; the result, a separation inside the cutoff, fits
+  const unsigned int sx = unsigned(na) * unsigned(S.pc_box[0]) + unsigned(nb) * unsigned(S.pc_box[3]) +
+                          unsigned(nc) * unsigned(S.pc_box[6]);
+  const unsigned int sy = unsigned(nb) * unsigned(S.pc_box[4]) + unsigned(nc) * unsigned(S.pc_box[7]);
+  const unsigned int sz = unsigned(nc) * unsigned(S.pc_box[8]);
+  const float ei = 0.5f * sqrtf((hi_.x - li.x) * (hi_.x - li.x) + (hi_.y - li.y) * (hi_.y - li.y) +
+                                (hi_.z - li.z) * (hi_.z - li.z));
+  const float ej = 0.5f * sqrtf((hj.x - lj.x) * (hj.x - lj.x) + (hj.y - lj.y) * (hj.y - lj.y) +
+                                (hj.z - lj.z) * (hj.z - lj.z));
+  const bool per_pair = 2.f * (ei + ej) + sqrtf(S.list2) + sqrtf(S.cut2) >= S.min_width;
+  return make_int4(int(sx), int(sy), int(sz), per_pair ? 1 : 0);
+}
+
 __device__ __forceinline__ bool blocks_near(const SysDev& S, const Dev& d, int I, int J) {
   return boxes_near(S, d.bb_lo[I], d.bb_hi[I], d.bb_lo[J], d.bb_hi[J]);
 }
@@ -330,7 +411,10 @@ __device__ void phase_tiles_find(const Dev& d) {
           const int Jt = J0 + src;
           const int pos = count + __popc(found & ((1u << src) - 1u));
           if (WRITE && pos < cap) {
-            if (lane == 0) d.tiles[base + pos] = make_int2(I, Jt);
+            if (lane == 0) {
+              d.tiles[base + pos] = make_int2(I, Jt);
+              d.tile_shift[base + pos] = tile_image(S, li, hi_, d.bb_lo[Jt], d.bb_hi[Jt]);
+            }
             const int Jl = Jt - S.block_off;
             const int nj = max(0, min(C, S.n_atoms - Jl * C));
             unsigned int valid = nj >= C ? kRowAll : ((1u << nj) - 1u);
@@ -353,6 +437,7 @@ __device__ void phase_tiles_find(const Dev& d) {
         const int at = count + __popc(found & below);
         if (WRITE && tile && at < cap) {
           d.tiles[base + at] = make_int2(I, J);
+          d.tile_shift[base + at] = tile_image(S, li, hi_, d.bb_lo[J], d.bb_hi[J]);
           const int Jl = J - S.block_off;
           const int nj = max(0, min(C, S.n_atoms - Jl * C));
           const unsigned int cols = nj >= C ? kRowAll : ((1u << nj) - 1u);

@@ -66,9 +66,12 @@ __device__ __forceinline__ unsigned int row_bits(const unsigned int* masks, long
   return (masks[ti * (C * C / 32) + (l >> 2)] >> ((l & 3) * 8)) & 0xFFu;
 }
 
+// `per_pair`: take the minimum image of every pair; otherwise pj already
+// carries the tile's lattice shift and the plain difference is the separation.
 template <int C, bool ENERGY, bool TRICLINIC>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
-                                           unsigned int mask, int l, float& fix, float& fiy, float& fiz,
+                                           unsigned int mask, bool per_pair, int l, float& fix, float& fiy,
+                                           float& fiz,
                                            float& fjx, float& fjy, float& fjz, float& ecoul, float& elj,
                                            int& pairs, float* vir) {
   const float alpha = S.alpha, a2sp = S.alpha_2_sqrtpi, cut2 = S.cut2, inv = S.pc_inv;
@@ -76,8 +79,9 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
 #pragma unroll 4
   for (int k = 0; k < C; ++k) {
     const int jl = (l + k) & (C - 1);
-    int dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-    min_image<TRICLINIC>(S, dx, dy, dz);
+    int dx = int(unsigned(pj.x) - unsigned(pi.x)), dy = int(unsigned(pj.y) - unsigned(pi.y)),
+        dz = int(unsigned(pj.z) - unsigned(pi.z));
+    if (per_pair) min_image<TRICLINIC>(S, dx, dy, dz);
     const float rx = dx * inv, ry = dy * inv, rz = dz * inv;
     const float r2 = rx * rx + ry * ry + rz * rz;
     if (((mask >> jl) & 1u) && r2 < cut2) {
@@ -197,6 +201,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
     int4 pi = make_int4(0, 0, 0, 0), pj = pi;
     float4 qi = make_float4(0.f, 0.f, 0.f, 0.f), qj = qi;
     int gj = -1;
+    bool per_pair = false;
     if (active) {
       while (t >= d.tile_prefix[s + 1]) {
         flush_energy(s);
@@ -216,12 +221,19 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
       qi = d.prm[gi];
       pj = d.pc[gj];
       qj = d.prm[gj];
+      const int4 sh = d.tile_shift[ti];
+      per_pair = sh.w != 0;
+      if (!per_pair) {
+        pj.x = int(unsigned(pj.x) + unsigned(sh.x));
+        pj.y = int(unsigned(pj.y) + unsigned(sh.y));
+        pj.z = int(unsigned(pj.z) + unsigned(sh.z));
+      }
     }
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
     float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int np = 0;
-    tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, l, fix, fiy, fiz, fjx, fjy, fjz, ec, el, np,
-                                     vir);
+    tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy, fjz, ec,
+                                     el, np, vir);
     if (!active) continue;
     aix += to_fixed(fix);
     aiy += to_fixed(fiy);
