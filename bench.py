@@ -417,7 +417,8 @@ def main() -> None:
         best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=200)
         cfg["autotuner"] = {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
-                                   tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"])])
+                                   tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"],
+                                            best["prune_tiles"])])
         loop = steploop.StepLoop.from_parsed(system, state, opts)
         total_s, clock_summary = timed(loop)
         steps_per_s = args.steps / total_s

@@ -166,6 +166,8 @@ typedef struct mdb_tuning {
   double sort_cell;    /* nm; width of the fractional cells of the spatial sort; default 0.25 */
   int32_t tile_atoms;  /* atoms per cluster of the pair tiles, 8 or 32; default 8.  One shape per
                           engine: a batch takes the first system's that sets one */
+  int32_t prune_tiles; /* 1: each rebuild drops the tiles with no pair inside cutoff + skin;
+                          2: keeps them; 0: default (1).  Per engine, like tile_atoms */
 } mdb_tuning;
 
 typedef struct mdb_run_options {
@@ -397,7 +399,7 @@ int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* cha
 
 /*
  * Autotuner (no reference counterpart).  Times every candidate of a fixed grid
- * of (tile_atoms, verlet_skin, sort_cell) on the device -- a temporary engine per
+ * of (tile_atoms, prune_tiles, verlet_skin, sort_cell) on the device -- a temporary engine per
  * candidate, `steps` graph-replayed steps after a warm-up of the same length,
  * CUDA-event timed -- and returns the fastest in `best` and its ms per step.
  * `tried` (may be NULL) receives the number of candidates.  The state the

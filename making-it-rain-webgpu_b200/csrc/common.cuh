@@ -190,6 +190,14 @@ __device__ __forceinline__ int find_system(const int* prefix, int count, int ind
   return lo;
 }
 
+// The interaction-mask bits of row l of tile ti (one bit per j): a word per
+// row for 32x32 tiles, a byte per row (four to a word) for 8x8 tiles.
+template <int C>
+__device__ __forceinline__ unsigned int row_bits(const unsigned int* masks, long long ti, int l) {
+  if (C == 32) return masks[ti * 32 + l];
+  return (masks[ti * (C * C / 32) + (l >> 2)] >> ((l & 3) * 8)) & 0xFFu;
+}
+
 // Minimum image of a pair-coordinate difference (int32 at 2^pc_shift per nm).
 template <bool TRICLINIC>
 __device__ __forceinline__ void min_image(const SysDev& S, int& dx, int& dy, int& dz) {

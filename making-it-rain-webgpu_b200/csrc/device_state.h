@@ -23,6 +23,7 @@ struct Dev {
   RunDev run;
   int n_atoms, n_slots, n_blocks, n_cells, n_units, n_iblk;
   int cluster;        // atoms per cluster of the tile list: 8 or 32 (n_blocks counts clusters)
+  int prune;          // rebuilds drop tiles with no pair inside cutoff + skin
   int any_triclinic;  // some system's box is triclinic: the pair kernel takes the general minimum image
 
   // atoms, original order
@@ -51,7 +52,13 @@ struct Dev {
   float4 *bb_lo, *bb_hi;  // per cluster
   float4 *sb_lo, *sb_hi;  // per 32-slot super-cluster (the cluster boxes themselves when clusters are 32)
   int* fold;              // per slot: the lattice translation of the last rebuild's fold (3 x 10 bits)
-  int4* tile_shift;       // per tile: lattice shift of J in pair-coordinate units; w = 1: per-pair minimum image
+  int4* tile_shift;
+  int2* raw_tiles;        // the fill pass's list, before pruning
+  unsigned int* raw_masks;
+  int4* raw_shift;
+  unsigned char* tile_alive;  // per raw tile: some pair within cutoff + skin
+  int* row_alive;         // per cluster: surviving tiles of its row
+  int* alive_start;       // per cluster: their start after pruning       // per tile: lattice shift of J in pair-coordinate units; w = 1: per-pair minimum image
   int* tile_cnt;
   int* tile_start;
   const int* block_sys;

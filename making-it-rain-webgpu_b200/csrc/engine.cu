@@ -100,6 +100,7 @@ struct mdb_engine {
   std::vector<int> fft_x_sys;  // system of each x-pass work item
   bool coop_list = false;      // the list kernels run as one cooperative launch
   int cluster = 8;                 // atoms per cluster of the tile list (8 or 32), per engine
+  bool prune = true;               // rebuilds drop tiles with no pair inside cutoff + skin
   std::vector<double> skin;        // per system, nm
   std::vector<int> mol_first, mol_count;  // per system: its molecules in d.mol_off
   double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel
@@ -310,7 +311,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   e->sort_cell.assign(n, kCellWidth);
   e->cluster = kDefaultCluster;
   if (e->opt.tuning) {
-    bool shape_set = false;
+    bool shape_set = false, prune_set = false;
     for (int s = 0; s < n; ++s) {
       if (e->opt.tuning[s].verlet_skin > 0) e->skin[s] = e->opt.tuning[s].verlet_skin;
       if (e->opt.tuning[s].sort_cell > 0) e->sort_cell[s] = e->opt.tuning[s].sort_cell;
@@ -320,6 +321,12 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
       if (shape && !shape_set) {  // one tile shape per engine: the first system's that names one
         e->cluster = shape;
         shape_set = true;
+      }
+      const int prune = e->opt.tuning[s].prune_tiles;
+      if (prune < 0 || prune > 2) return fail(e, MDB_ERR_INVALID_ARGUMENT, "prune_tiles must be 0, 1 or 2");
+      if (prune && !prune_set) {
+        e->prune = prune == 1;
+        prune_set = true;
       }
     }
     e->opt.tuning = nullptr;  // the caller's array is not kept
@@ -579,6 +586,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.n_slots = slots;
   d.n_blocks = blocks;
   d.cluster = e->cluster;
+  d.prune = e->prune ? 1 : 0;
   d.any_triclinic = 0;
   for (int s = 0; s < n; ++s) d.any_triclinic |= e->sd[s].triclinic ? 1 : 0;
   d.n_cells = cells;
@@ -645,6 +653,12 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "tiles", d.tiles, tiles));
   TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
   TRY(alloc(e, "tile image shifts", d.tile_shift, tiles));
+  TRY(alloc(e, "raw tiles", d.raw_tiles, tiles));
+  TRY(alloc(e, "raw tile masks", d.raw_masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
+  TRY(alloc(e, "raw tile shifts", d.raw_shift, tiles));
+  TRY(alloc(e, "tile survives", d.tile_alive, tiles));
+  TRY(alloc(e, "surviving tiles per row", d.row_alive, blocks));
+  TRY(alloc(e, "surviving tiles start", d.alive_start, blocks));
   TRY(alloc(e, "fold translations", d.fold, slots));
   TRY(alloc(e, "tile count", d.tile_count, n));
   TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
@@ -1282,21 +1296,23 @@ int mdb_system_count(const mdb_engine* e, int32_t* out) {
   return MDB_OK;
 }
 
-// The candidate grid: tile shape (8x8 or 32x32 clusters), list skin (rebuild
-// frequency against tile count) and spatial-sort cell width (how compact a
-// cluster is).
+// The candidate grid: tile shape (8x8 or 32x32 clusters), tile pruning (a
+// cheaper pair kernel against a longer rebuild), list skin (rebuild frequency
+// against tile count) and spatial-sort cell width (how compact a cluster is).
 int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
                  int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried) {
   if (!system || !state || !options || !best || steps <= 0) return MDB_ERR_INVALID_ARGUMENT;
-  static const double kSkins[] = {0.10, 0.15, 0.20};
+  static const double kSkins[] = {0.15, 0.20};
   static const double kCells[] = {0.20, 0.25, 0.35};
   static const int kShapes[] = {8, 32};
+  static const int kPrune[] = {1, 2};
   double best_ms = std::numeric_limits<double>::infinity();
   int count = 0, last = MDB_OK;
   for (int shape : kShapes)
+  for (int prune : kPrune)
   for (double skin : kSkins)
     for (double cell : kCells) {
-      mdb_tuning t{skin, cell, shape};
+      mdb_tuning t{skin, cell, shape, prune};
       mdb_run_options o = *options;
       o.tuning = &t;
       mdb_engine* e = nullptr;

@@ -284,7 +284,11 @@ __device__ __forceinline__ bool boxes_near(const SysDev& S, float4 li, float4 hi
   const float kb = rintf(dy / B[4]);
   dx -= kb * B[3]; dy -= kb * B[4];
   dx -= rintf(dx / B[0]) * B[0];
-  if (!S.triclinic) {
+  // When every centre distance that could pass (list + both half-diagonals)
+  // is below half the cell's narrowest width, the sequential reduction above
+  // already gives the minimum image, as it does for the reference's cutoff.
+  const bool one_image = !S.triclinic || sqrtf(S.list2) + sqrtf(hx * hx + hy * hy + hz * hz) < 0.5f * S.min_width;
+  if (one_image) {
     const float gx = fmaxf(fabsf(dx) - hx, 0.f), gy = fmaxf(fabsf(dy) - hy, 0.f), gz = fmaxf(fabsf(dz) - hz, 0.f);
     return gx * gx + gy * gy + gz * gz < S.list2;
   }
@@ -319,10 +323,10 @@ __device__ __forceinline__ int4 tile_image(const SysDev& S, float4 li, float4 hi
   const float ka = rintf(dx / B[0]);
   dx -= ka * B[0];
   int na = -int(ka), nb = -int(kb), nc = -int(kc);
-  if (S.triclinic) {
-    const float hx = 0.5f * (hi_.x - li.x) + 0.5f * (hj.x - lj.x);
-    const float hy = 0.5f * (hi_.y - li.y) + 0.5f * (hj.y - lj.y);
-    const float hz = 0.5f * (hi_.z - li.z) + 0.5f * (hj.z - lj.z);
+  const float hx = 0.5f * (hi_.x - li.x) + 0.5f * (hj.x - lj.x);
+  const float hy = 0.5f * (hi_.y - li.y) + 0.5f * (hj.y - lj.y);
+  const float hz = 0.5f * (hi_.z - li.z) + 0.5f * (hj.z - lj.z);
+  if (S.triclinic && sqrtf(S.list2) + sqrtf(hx * hx + hy * hy + hz * hz) >= 0.5f * S.min_width) {
     float best = 3.0e38f;
     int bi = 0, bj = 0, bk = 0;
     for (int k = -1; k <= 1; ++k)
@@ -412,15 +416,15 @@ __device__ void phase_tiles_find(const Dev& d) {
           const int pos = count + __popc(found & ((1u << src) - 1u));
           if (WRITE && pos < cap) {
             if (lane == 0) {
-              d.tiles[base + pos] = make_int2(I, Jt);
-              d.tile_shift[base + pos] = tile_image(S, li, hi_, d.bb_lo[Jt], d.bb_hi[Jt]);
+              (d.prune ? d.raw_tiles : d.tiles)[base + pos] = make_int2(I, Jt);
+              (d.prune ? d.raw_shift : d.tile_shift)[base + pos] = tile_image(S, li, hi_, d.bb_lo[Jt], d.bb_hi[Jt]);
             }
             const int Jl = Jt - S.block_off;
             const int nj = max(0, min(C, S.n_atoms - Jl * C));
             unsigned int valid = nj >= C ? kRowAll : ((1u << nj) - 1u);
             if (Jt == I) valid &= lane == C - 1 ? 0u : (kRowAll << (lane + 1));
             if (Il * C + lane >= S.n_atoms) valid = 0u;
-            d.masks[(base + pos) * kWords + lane] = valid;
+            (d.prune ? d.raw_masks : d.masks)[(base + pos) * kWords + lane] = valid;
           }
         }
         count += __popc(found);
@@ -436,8 +440,8 @@ __device__ void phase_tiles_find(const Dev& d) {
         const unsigned int found = __ballot_sync(0xffffffffu, tile);
         const int at = count + __popc(found & below);
         if (WRITE && tile && at < cap) {
-          d.tiles[base + at] = make_int2(I, J);
-          d.tile_shift[base + at] = tile_image(S, li, hi_, d.bb_lo[J], d.bb_hi[J]);
+          (d.prune ? d.raw_tiles : d.tiles)[base + at] = make_int2(I, J);
+          (d.prune ? d.raw_shift : d.tile_shift)[base + at] = tile_image(S, li, hi_, d.bb_lo[J], d.bb_hi[J]);
           const int Jl = J - S.block_off;
           const int nj = max(0, min(C, S.n_atoms - Jl * C));
           const unsigned int cols = nj >= C ? kRowAll : ((1u << nj) - 1u);
@@ -451,13 +455,18 @@ __device__ void phase_tiles_find(const Dev& d) {
             words[(r * C) >> 5] |= row << ((r * C) & 31);
           }
 #pragma unroll
-          for (int w = 0; w < kWords; ++w) d.masks[(base + at) * kWords + w] = words[w];
+          unsigned int* masks = d.prune ? d.raw_masks : d.masks;
+#pragma unroll
+          for (int w = 0; w < kWords; ++w) masks[(base + at) * kWords + w] = words[w];
         }
         count += __popc(found);
         for (int b = 0; b < kBatch && rest; ++b) rest &= rest - 1;  // the super-clusters this pass took
       }
     }
-    if (!WRITE && lane == 0) d.tile_cnt[I] = count;
+    if (!WRITE && lane == 0) {
+      d.tile_cnt[I] = count;
+      d.row_alive[I] = 0;
+    }
   }
 }
 
@@ -469,6 +478,121 @@ __device__ void phase_tiles_scan(const Dev& d) {
     if (threadIdx.x == 0) {
       if (total > S.tile_cap) atomicOr(&d.err[s], kErrTileCapacity);
       d.tile_count[s] = total < S.tile_cap ? total : S.tile_cap;
+    }
+  }
+}
+
+// Drop the tiles whose atoms are all farther apart than cutoff + skin (the
+// box test is conservative: about a fifth of 8x8 tiles have no pair inside).
+// Tiles are spread over every warp, 32/C at a time, one group of C lanes per
+// tile running the pair kernel's rotation on distances only; the verdict goes
+// to tile_alive and the row's survivor count.
+template <int C>
+__device__ void phase_tiles_prune(const Dev& d) {
+  constexpr int G = 32 / C;
+  const int lane = threadIdx.x & 31, g = lane / C, l = lane & (C - 1);
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int src = (l + 1) & (C - 1);
+  constexpr unsigned kGroup = C == 32 ? 0xffffffffu : ((1u << C) - 1u);
+  for (int s = 0; s < d.S; ++s) {
+    if (!d.rebuild_now[s]) continue;
+    const SysDev& S = d.sys[s];
+    const int n = d.tile_count[s];
+    const float inv = S.pc_inv, list2 = S.list2 * (1.0f + 1e-5f);
+    for (int b = warp * G; b < n; b += warps * G) {
+      const int t = b + g;
+      const bool active = t < n;
+      const long long ti = S.tile_off + (active ? t : 0);
+      const int2 tile = d.raw_tiles[ti];
+      const int4 sh = d.raw_shift[ti];
+      unsigned int mask = active ? row_bits<C>(d.raw_masks, ti, l) : 0u;
+      mask = (mask >> l) | (mask << ((C - l) & (C - 1)));  // bit k <-> j = l + k (mod C)
+      const int4 pi = d.pc[tile.x * C + l];
+      int4 pj = d.pc[tile.y * C + l];
+      if (!sh.w) {
+        pj.x = int(unsigned(pj.x) + unsigned(sh.x));
+        pj.y = int(unsigned(pj.y) + unsigned(sh.y));
+        pj.z = int(unsigned(pj.z) + unsigned(sh.z));
+      }
+      bool hit = false;
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        int dx = int(unsigned(pj.x) - unsigned(pi.x)), dy = int(unsigned(pj.y) - unsigned(pi.y)),
+            dz = int(unsigned(pj.z) - unsigned(pi.z));
+        if (sh.w) {
+          if (S.triclinic) min_image<true>(S, dx, dy, dz);
+          else min_image<false>(S, dx, dy, dz);
+        }
+        const float rx = dx * inv, ry = dy * inv, rz = dz * inv;
+        hit |= ((mask >> k) & 1u) && rx * rx + ry * ry + rz * rz < list2;
+        pj.x = __shfl_sync(0xffffffffu, pj.x, src, C);
+        pj.y = __shfl_sync(0xffffffffu, pj.y, src, C);
+        pj.z = __shfl_sync(0xffffffffu, pj.z, src, C);
+      }
+      const unsigned int hits = __ballot_sync(0xffffffffu, hit);
+      const bool alive = ((hits >> (g * C)) & kGroup) != 0u;
+      if (active && l == 0) {
+        d.tile_alive[ti] = alive ? 1 : 0;
+        if (alive) atomicAdd(&d.row_alive[tile.x], 1);
+      }
+    }
+  }
+}
+
+__device__ void phase_tiles_rescan(const Dev& d) {
+  for (int s = blockIdx.x; s < d.S; s += gridDim.x) {
+    if (!d.rebuild_now[s]) continue;
+    const SysDev& S = d.sys[s];
+    const int total = block_exclusive_scan(d.row_alive + S.block_off, d.alive_start + S.block_off, S.n_blocks);
+    if (threadIdx.x == 0) d.tile_count[s] = total;
+  }
+}
+
+// Warp per row: the row's surviving tiles, in order, into the list the pair
+// kernel reads; the row's start and count follow them.
+template <int C>
+__device__ void phase_tiles_compact(const Dev& d) {
+  constexpr int kWords = C * C / 32;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < d.n_blocks; I += warps) {
+    const int s = d.block_sys[I];
+    if (!d.rebuild_now[s]) continue;
+    const SysDev& S = d.sys[s];
+    const int old_start = d.tile_start[I], old_n = min(d.tile_cnt[I], S.tile_cap - old_start);
+    const int new_start = d.alive_start[I];
+    int written = 0;
+    for (int k0 = 0; k0 < old_n; k0 += 32) {
+      const int k = k0 + lane;
+      const long long src = static_cast<long long>(S.tile_off) + old_start + k;
+      const bool keep = k < old_n && d.tile_alive[src];
+      const unsigned int keepers = __ballot_sync(0xffffffffu, keep);
+      const long long dst = static_cast<long long>(S.tile_off) + new_start + written +
+                            __popc(keepers & ((1u << lane) - 1u));
+      if (keep) {
+        d.tiles[dst] = d.raw_tiles[src];
+        d.tile_shift[dst] = d.raw_shift[src];
+        if (C < 32)
+          for (int w = 0; w < kWords; ++w) d.masks[dst * kWords + w] = d.raw_masks[src * kWords + w];
+      }
+      if (C == 32) {
+        // a 32x32 tile's mask is 32 words: the warp copies each kept tile's
+        unsigned int f = keepers;
+        while (f) {
+          const int from = __ffs(f) - 1;
+          f &= f - 1;
+          const long long sidx = static_cast<long long>(S.tile_off) + old_start + k0 + from;
+          const long long didx = static_cast<long long>(S.tile_off) + new_start + written +
+                                 __popc(keepers & ((1u << from) - 1u));
+          d.masks[didx * kWords + lane] = d.raw_masks[sidx * kWords + lane];
+        }
+      }
+      written += __popc(keepers);
+    }
+    if (lane == 0) {
+      d.tile_start[I] = new_start;
+      d.tile_cnt[I] = written;
     }
   }
 }
@@ -581,6 +705,14 @@ __global__ void __launch_bounds__(kThreads) k_list(Dev d) {
   if (!grid_barrier(d.list_barrier, err)) return;
   phase_tiles_find<C, true>(d);
   if (!grid_barrier(d.list_barrier, err)) return;
+  if (d.prune) {
+    phase_tiles_prune<C>(d);
+    if (!grid_barrier(d.list_barrier, err)) return;
+    phase_tiles_rescan(d);
+    if (!grid_barrier(d.list_barrier, err)) return;
+    phase_tiles_compact<C>(d);
+    if (!grid_barrier(d.list_barrier, err)) return;
+  }
   phase_tiles_exclusions<C>(d);
   if (!grid_barrier(d.list_barrier, err)) return;
   phase_tiles_finish(d);
@@ -600,6 +732,7 @@ MDB_PHASE_KERNEL(cells_scatter, true)
 MDB_PHASE_KERNEL(cells_order, true)
 MDB_PHASE_KERNEL(wrap, false)
 MDB_PHASE_KERNEL(tiles_scan, true)
+MDB_PHASE_KERNEL(tiles_rescan, true)
 MDB_PHASE_KERNEL(tiles_finish, true)
 #undef MDB_PHASE_KERNEL
 #define MDB_PHASE_KERNEL_C(name)                                   \
@@ -609,6 +742,8 @@ MDB_PHASE_KERNEL(tiles_finish, true)
     phase_##name<C>(d);                                            \
   }
 MDB_PHASE_KERNEL_C(tiles_blocks)
+MDB_PHASE_KERNEL_C(tiles_prune)
+MDB_PHASE_KERNEL_C(tiles_compact)
 template <int C>
 __global__ void __launch_bounds__(kThreads) k_tiles_count(Dev d) {
   if (!*d.any_rebuild) return;
@@ -680,6 +815,11 @@ void rebuild_tiles(const Dev& d, cudaStream_t st) {
   k_tiles_count<C><<<warp_blocks, kThreads, 0, st>>>(d);
   k_tiles_scan<<<d.S < 148 ? d.S : 148, kThreads, 0, st>>>(d);
   k_tiles_fill<C><<<warp_blocks, kThreads, 0, st>>>(d);
+  if (d.prune) {
+    k_tiles_prune<C><<<148 * 4, kThreads, 0, st>>>(d);
+    k_tiles_rescan<<<d.S < 148 ? d.S : 148, kThreads, 0, st>>>(d);
+    k_tiles_compact<C><<<warp_blocks, kThreads, 0, st>>>(d);
+  }
   k_tiles_exclusions<C><<<blocks_for(d.n_excl, kThreads), kThreads, 0, st>>>(d);
   k_tiles_finish<<<1, 32, 0, st>>>(d);
 }

@@ -59,13 +59,6 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
   return v;
 }
 
-// The mask bits of row l (one bit per j of the tile).
-template <int C>
-__device__ __forceinline__ unsigned int row_bits(const unsigned int* masks, long long ti, int l) {
-  if (C == 32) return masks[ti * 32 + l];
-  return (masks[ti * (C * C / 32) + (l >> 2)] >> ((l & 3) * 8)) & 0xFFu;
-}
-
 // `per_pair`: take the minimum image of every pair; otherwise pj already
 // carries the tile's lattice shift and the plain difference is the separation.
 template <int C, bool ENERGY, bool TRICLINIC>

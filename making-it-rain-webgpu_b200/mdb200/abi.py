@@ -114,7 +114,8 @@ class StateDesc(C.Structure):
 class Tuning(C.Structure):
     """`mdb_tuning` (no reference counterpart)."""
 
-    _fields_ = [("verlet_skin", C.c_double), ("sort_cell", C.c_double), ("tile_atoms", C.c_int32)]
+    _fields_ = [("verlet_skin", C.c_double), ("sort_cell", C.c_double), ("tile_atoms", C.c_int32),
+                ("prune_tiles", C.c_int32)]
 
 
 class RunOptions(C.Structure):

@@ -76,7 +76,7 @@ class RunOptions:
     graphs: bool = True
     always_rebuild: bool = False
     phase_launches: bool = False  # list build as separate launches (profiling)
-    # per-system (verlet_skin, sort_cell[, tile_atoms]) from `autotune`; None = defaults
+    # per-system (verlet_skin, sort_cell[, tile_atoms[, prune_tiles]]) from `autotune`; None = defaults
     tuning: Optional[Sequence[tuple]] = None
     # > 0: each barostat learns a screening network from that many exact
     # attempts, then screens proposals by delayed acceptance
@@ -98,7 +98,9 @@ class RunOptions:
                    | (abi.FLAG_PHASE_LAUNCHES if self.phase_launches else 0))
         o.surrogate_attempts = int(self.surrogate_attempts)
         if self.tuning is not None:
-            arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(t[0]), float(t[1]), int(t[2]) if len(t) > 2 else 0)
+            arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(t[0]), float(t[1]),
+                                                               int(t[2]) if len(t) > 2 else 0,
+                                                               int(t[3]) if len(t) > 3 else 0)
                                                     for t in self.tuning])
             o.tuning = C.cast(arr, C.POINTER(abi.Tuning))
             o._keep = arr  # the array must outlive the create call
@@ -329,7 +331,7 @@ def autotune(system: System, state: State, options: RunOptions | None = None, st
     if status != abi.OK:
         raise _ERRORS.get(status, EngineError)(status, lib.mdb_status_string(status).decode())
     return {"verlet_skin": best.verlet_skin, "sort_cell": best.sort_cell, "tile_atoms": best.tile_atoms,
-            "ms_per_step": ms.value, "candidates": tried.value}
+            "prune_tiles": best.prune_tiles, "ms_per_step": ms.value, "candidates": tried.value}
 
 
 def size_bucket(atoms: int) -> int:
@@ -353,7 +355,8 @@ def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: 
         members = sorted(members, key=lambda k: systems[k].particle_count)
         rep = members[len(members) // 2]
         cache[b] = autotune(systems[rep], states[rep], options, steps)
-    tuning = [tuple(cache[size_bucket(s.particle_count)][k] for k in ("verlet_skin", "sort_cell", "tile_atoms"))
+    tuning = [tuple(cache[size_bucket(s.particle_count)][k]
+                    for k in ("verlet_skin", "sort_cell", "tile_atoms", "prune_tiles"))
               for s in systems]
     return tuning, cache
 

@@ -266,13 +266,13 @@ def test_autotune_picks_a_candidate_and_tuned_batch_equals_tuned_single(mdb):
     b = synth.water_box(n_waters=900, width=3.1, seed=4, grid=(32, 32, 32))
     best = mdb.autotune(*a, steps=50)
     print("autotune", best)
-    assert best["candidates"] == 18
-    assert best["verlet_skin"] in (0.10, 0.15, 0.20) and best["sort_cell"] in (0.20, 0.25, 0.35)
-    assert best["tile_atoms"] in (8, 32)
-    tuning = [(best["verlet_skin"], best["sort_cell"], best["tile_atoms"]), (0.20, 0.35, 0)]
+    assert best["candidates"] == 24
+    assert best["verlet_skin"] in (0.15, 0.20) and best["sort_cell"] in (0.20, 0.25, 0.35)
+    assert best["tile_atoms"] in (8, 32) and best["prune_tiles"] in (1, 2)
+    tuning = [(best["verlet_skin"], best["sort_cell"], best["tile_atoms"], best["prune_tiles"]), (0.20, 0.35, 0, 0)]
     single = []
     for (s, st), t in zip((a, b), tuning):
-        t = (t[0], t[1], tuning[0][2])
+        t = (t[0], t[1], tuning[0][2], tuning[0][3])
         loop = mdb.StepLoop.from_parsed(s, st, mdb.RunOptions(seed=5, tuning=[t]))
         loop.run(30)
         single.append(loop.positions())
@@ -283,3 +283,22 @@ def test_autotune_picks_a_candidate_and_tuned_batch_equals_tuned_single(mdb):
     assert np.array_equal(batch.positions(0), single[0])
     assert np.array_equal(batch.positions(1), single[1])
     batch.destroy()
+
+
+@pytest.mark.parametrize("shape,prune", [(8, 1), (8, 2), (32, 1), (32, 2)])
+def test_every_tile_shape_and_pruning_matches_oracle(mdb, oracle, peptide, shape, prune):
+    """The tuning options change the list, never the forces: each tile shape,
+    with and without pruning, against the oracle on the peptide workload."""
+    system, state = peptide
+    loop = make_loop(mdb, system, state, tuning=[(0.2, 0.25, shape, prune)])
+    e, f = loop.evaluate()
+    loop.run(30)  # a few rebuilds' worth of dynamics on the same list settings
+    e2, f2 = loop.evaluate()
+    want2, wf2 = oracle.potential(system, loop.positions(), grid=(50, 50, 50), threads=8)
+    loop.destroy()
+    want, wf = oracle.potential(system, state.positions, grid=(50, 50, 50), threads=8)
+    for got, ref, gf, rf in ((e, want, f, wf), (e2, want2, f2, wf2)):
+        err = rel_rms(gf, rf)
+        print(f"tiles {shape} prune {prune}: force rel RMS {err:.2e}, pairs {got['pairs_within_cutoff']}")
+        assert err <= FORCE_REL_RMS, err
+        assert got["pairs_within_cutoff"] == ref["pairs_within_cutoff"]
