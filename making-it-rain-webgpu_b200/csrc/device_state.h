@@ -73,6 +73,7 @@ struct Dev {
   unsigned int* masks;
   int* tile_count;   // per system
   int* tile_prefix;  // S+1
+  int tile_cap_total; // sum of the systems' tile capacities
 
   // flags and status
   int* rebuild_flag;  // set by the integrator: some atom moved skin/2

@@ -281,7 +281,8 @@ int run_steps(mdb_engine* e, int64_t steps) {
       for (int64_t k = 0; k < steps; ++k) launch_step(e);
       CUDA_TRY(e, cudaStreamEndCapture(e->s0, &g));
       cudaGraphExec_t exec = nullptr;
-      CUDA_TRY(e, cudaGraphInstantiate(&exec, g, 0));
+      // keep the captured streams' priorities (PME and listed above the pair kernel)
+      CUDA_TRY(e, cudaGraphInstantiate(&exec, g, cudaGraphInstantiateFlagUseNodePriority));
       cudaGraphDestroy(g);
       it = e->graphs.emplace(steps, exec).first;
     }
@@ -585,6 +586,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.n_atoms = atoms;
   d.n_slots = slots;
   d.n_blocks = blocks;
+  d.tile_cap_total = tiles;
   d.cluster = e->cluster;
   d.prune = e->prune ? 1 : 0;
   d.any_triclinic = 0;
@@ -760,9 +762,13 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   e->step = states[0].step;
   set_pme_smem(smem_z, smem_y, smem_x);
 
+  // PME and the listed terms run beside the pair kernel at the highest
+  // priority: their small, latency-bound grids take SMs as pair blocks retire
+  int least = 0, greatest = 0;
+  CUDA_TRY(e, cudaDeviceGetStreamPriorityRange(&least, &greatest));
   CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking));
-  CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s1, cudaStreamNonBlocking));
-  CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s2, cudaStreamNonBlocking));
+  CUDA_TRY(e, cudaStreamCreateWithPriority(&e->s1, cudaStreamNonBlocking, greatest));
+  CUDA_TRY(e, cudaStreamCreateWithPriority(&e->s2, cudaStreamNonBlocking, greatest));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->join1, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->join2, cudaEventDisableTiming));

@@ -27,6 +27,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
+// Tiles per warp: blocks take fixed chunks of the list and retire as they
+// finish, so the PME stream's kernels can take SMs while the pair kernel runs.
+constexpr int kTilesPerWarp = 32;
 
 // erfc(x) = exp(-x^2) P(u): P fits erfcx on x in [0, 3.6] as a degree-7
 // polynomial in u = 3.111 t - 2.111, t = 1/(1 + x/2) (fit_erfcx.py in this
@@ -124,9 +127,11 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
   }
 }
 
-// A warp takes a contiguous run of the list and walks it 32/C tiles at a
-// time; group g of the warp runs tile t + g.  Every lane keeps its own row
-// and system, because the groups of one warp may be at different ones.
+// A warp takes chunks of kTilesPerWarp consecutive tiles of the list (chunk
+// w, then w + warps, ...) and walks each 32/C tiles at a time; group g of the
+// warp runs tile t + g.  Every lane keeps its own row and system, because the
+// groups of one warp may be at different ones.  The grid is sized for a
+// typical list, so most warps take one chunk and then retire.
 template <int C, bool ENERGY, bool TRICLINIC>
 __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   constexpr int G = 32 / C;
@@ -136,123 +141,127 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int total = d.tile_prefix[d.S];
-  const int per = ((total + nwarps - 1) / nwarps + G - 1) / G * G;
-  const int t0 = warp * per;
-  const int tend = min(total, t0 + per);
-  if (t0 >= tend) return;
-  int s = find_system(d.tile_prefix, d.S, min(t0 + g, tend - 1));
+  for (int t0 = warp * kTilesPerWarp; t0 < total; t0 += nwarps * kTilesPerWarp) {
+    const int tend = min(total, t0 + kTilesPerWarp);
+    int s = find_system(d.tile_prefix, d.S, min(t0 + g, tend - 1));
 
-  long long aix = 0, aiy = 0, aiz = 0;
-  int cur_row = -1;
-  long long ecoul64 = 0, elj64 = 0, pairs64 = 0;
-  long long vir64[6] = {0, 0, 0, 0, 0, 0};
+    long long aix = 0, aiy = 0, aiz = 0;
+    int cur_row = -1;
+    long long ecoul64 = 0, elj64 = 0, pairs64 = 0;
+    long long vir64[6] = {0, 0, 0, 0, 0, 0};
 
-  auto flush_row = [&]() {
-    if (cur_row >= 0) {
-      const int gi = cur_row * C + l;
-      if (aix | aiy | aiz) {
-        add_fixed64(&d.fx[gi], aix);
-        add_fixed64(&d.fy[gi], aiy);
-        add_fixed64(&d.fz[gi], aiz);
-      }
-    }
-    aix = aiy = aiz = 0;
-  };
-  // energies of the group's tiles so far, into system `sys` (every lane of the
-  // group calls it together)
-  auto flush_energy = [&](int sys) {
-    if (ENERGY) {
-      const long long c = group_sum64<C>(ecoul64, gmask), lj = group_sum64<C>(elj64, gmask),
-                      p = group_sum64<C>(pairs64, gmask);
-      long long v[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) v[k] = group_sum64<C>(vir64[k], gmask);
-      if (l == 0) {
-        unsigned long long* e = &d.energy[d.sys[sys].energy_base];
-        if (c) add_fixed64(&e[kECoulomb], c);
-        if (lj) add_fixed64(&e[kELj], lj);
-        if (p) add_fixed64(&e[kEPairs], p);
-        // slots: row-major 3x3, the symmetric pair tensor written to both halves
-        const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          if (!v[k]) continue;
-          add_fixed64(&e[kEVirial0 + slot[k]], v[k]);
-          if (mirror[k] >= 0) add_fixed64(&e[kEVirial0 + mirror[k]], v[k]);
+    auto flush_row = [&]() {
+      if (cur_row >= 0) {
+        const int gi = cur_row * C + l;
+        if (aix | aiy | aiz) {
+          add_fixed64(&d.fx[gi], aix);
+          add_fixed64(&d.fy[gi], aiy);
+          add_fixed64(&d.fz[gi], aiz);
         }
       }
-      ecoul64 = elj64 = pairs64 = 0;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) vir64[k] = 0;
-    }
-  };
+      aix = aiy = aiz = 0;
+    };
+    // energies of the group's tiles so far, into system `sys` (every lane of the
+    // group calls it together)
+    auto flush_energy = [&](int sys) {
+      if (ENERGY) {
+        const long long c = group_sum64<C>(ecoul64, gmask), lj = group_sum64<C>(elj64, gmask),
+                        p = group_sum64<C>(pairs64, gmask);
+        long long v[6];
+  #pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = group_sum64<C>(vir64[k], gmask);
+        if (l == 0) {
+          unsigned long long* e = &d.energy[d.sys[sys].energy_base];
+          if (c) add_fixed64(&e[kECoulomb], c);
+          if (lj) add_fixed64(&e[kELj], lj);
+          if (p) add_fixed64(&e[kEPairs], p);
+          // slots: row-major 3x3, the symmetric pair tensor written to both halves
+          const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
+  #pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            if (!v[k]) continue;
+            add_fixed64(&e[kEVirial0 + slot[k]], v[k]);
+            if (mirror[k] >= 0) add_fixed64(&e[kEVirial0 + mirror[k]], v[k]);
+          }
+        }
+        ecoul64 = elj64 = pairs64 = 0;
+  #pragma unroll
+        for (int k = 0; k < 6; ++k) vir64[k] = 0;
+      }
+    };
 
-  for (int base = t0; base < tend; base += G) {
-    const int t = base + g;
-    const bool active = t < tend;  // the same for every lane of a group
-    unsigned int mask = 0u;
-    int4 pi = make_int4(0, 0, 0, 0), pj = pi;
-    float4 qi = make_float4(0.f, 0.f, 0.f, 0.f), qj = qi;
-    int gj = -1;
-    bool per_pair = false;
-    if (active) {
-      while (t >= d.tile_prefix[s + 1]) {
-        flush_energy(s);
-        ++s;
+    for (int base = t0; base < tend; base += G) {
+      const int t = base + g;
+      const bool active = t < tend;  // the same for every lane of a group
+      unsigned int mask = 0u;
+      int4 pi = make_int4(0, 0, 0, 0), pj = pi;
+      float4 qi = make_float4(0.f, 0.f, 0.f, 0.f), qj = qi;
+      int gj = -1;
+      bool per_pair = false;
+      if (active) {
+        while (t >= d.tile_prefix[s + 1]) {
+          flush_energy(s);
+          ++s;
+        }
+        const SysDev& S = d.sys[s];
+        const long long ti = S.tile_off + (t - d.tile_prefix[s]);
+        mask = row_bits<C>(d.masks, ti, l);
+        const int2 tile = d.tiles[ti];
+        if (tile.x != cur_row) {
+          flush_row();
+          cur_row = tile.x;
+        }
+        const int gi = tile.x * C + l;
+        gj = tile.y * C + l;
+        pi = d.pc[gi];
+        qi = d.prm[gi];
+        pj = d.pc[gj];
+        qj = d.prm[gj];
+        const int4 sh = d.tile_shift[ti];
+        per_pair = sh.w != 0;
+        if (!per_pair) {
+          pj.x = int(unsigned(pj.x) + unsigned(sh.x));
+          pj.y = int(unsigned(pj.y) + unsigned(sh.y));
+          pj.z = int(unsigned(pj.z) + unsigned(sh.z));
+        }
       }
-      const SysDev& S = d.sys[s];
-      const long long ti = S.tile_off + (t - d.tile_prefix[s]);
-      mask = row_bits<C>(d.masks, ti, l);
-      const int2 tile = d.tiles[ti];
-      if (tile.x != cur_row) {
-        flush_row();
-        cur_row = tile.x;
+      float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
+      float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      int np = 0;
+      tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy, fjz, ec,
+                                       el, np, vir);
+      if (!active) continue;
+      aix += to_fixed(fix);
+      aiy += to_fixed(fiy);
+      aiz += to_fixed(fiz);
+      if (fjx != 0.f || fjy != 0.f || fjz != 0.f) {
+        add_fixed(&d.fx[gj], fjx);
+        add_fixed(&d.fy[gj], fjy);
+        add_fixed(&d.fz[gj], fjz);
       }
-      const int gi = tile.x * C + l;
-      gj = tile.y * C + l;
-      pi = d.pc[gi];
-      qi = d.prm[gi];
-      pj = d.pc[gj];
-      qj = d.prm[gj];
-      const int4 sh = d.tile_shift[ti];
-      per_pair = sh.w != 0;
-      if (!per_pair) {
-        pj.x = int(unsigned(pj.x) + unsigned(sh.x));
-        pj.y = int(unsigned(pj.y) + unsigned(sh.y));
-        pj.z = int(unsigned(pj.z) + unsigned(sh.z));
+      if (ENERGY) {
+        ecoul64 += to_fixed(ec);
+        elj64 += to_fixed(el);
+        pairs64 += np;
+  #pragma unroll
+        for (int k = 0; k < 6; ++k) vir64[k] += to_fixed(vir[k]);
       }
     }
-    float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
-    float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int np = 0;
-    tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy, fjz, ec,
-                                     el, np, vir);
-    if (!active) continue;
-    aix += to_fixed(fix);
-    aiy += to_fixed(fiy);
-    aiz += to_fixed(fiz);
-    if (fjx != 0.f || fjy != 0.f || fjz != 0.f) {
-      add_fixed(&d.fx[gj], fjx);
-      add_fixed(&d.fy[gj], fjy);
-      add_fixed(&d.fz[gj], fjz);
-    }
-    if (ENERGY) {
-      ecoul64 += to_fixed(ec);
-      elj64 += to_fixed(el);
-      pairs64 += np;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) vir64[k] += to_fixed(vir[k]);
-    }
+    flush_row();
+    flush_energy(s);
   }
-  flush_row();
-  flush_energy(s);
 }
 
 template <int C>
 void launch_shape(const Dev& d, bool energy, bool triclinic, cudaStream_t st) {
-  // Persistent-style: a fixed grid of 148 SMs x 8 blocks of 8 warps, each warp
-  // taking a contiguous run of tiles so consecutive tiles of a row share i.
-  const int blocks = 148 * 8;
+  // one chunk per warp for a list of ~160 tiles per cluster (8x8 tiles in
+  // water run 90-150); a longer list makes warps take further chunks
+  const int warps_per_block = kThreads / 32;
+  const long long typical = static_cast<long long>(d.n_blocks) * (C == 8 ? 160 : 100);
+  const int blocks = static_cast<int>(std::max<long long>(
+      1, std::min<long long>((typical + kTilesPerWarp * warps_per_block - 1) / (kTilesPerWarp * warps_per_block),
+                             (d.tile_cap_total + kTilesPerWarp * warps_per_block - 1) /
+                                 (kTilesPerWarp * warps_per_block))));
   if (energy) {
     if (triclinic) k_nonbonded<C, true, true><<<blocks, kThreads, 0, st>>>(d);
     else k_nonbonded<C, true, false><<<blocks, kThreads, 0, st>>>(d);
