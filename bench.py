@@ -251,8 +251,9 @@ def main() -> None:
     stride = min(args.stride, args.steps)
     strides = [stride] * (args.steps // stride) + ([args.steps % stride] if args.steps % stride else [])
 
-    def timed(loop) -> tuple[float, dict]:
-        """Warm-up, then exactly args.steps steps as timed strides; device seconds."""
+    def timed(loop, on_stride=None) -> tuple[float, dict]:
+        """Warm-up, then exactly args.steps steps as timed strides; device seconds.
+        `on_stride(loop)` runs after each stride, outside its timed interval."""
         # clocks are sampled from before the warm-up, so nvidia-smi is running when
         # the timed region starts; only samples inside that region are reported
         clocks = ClockSampler(local).__enter__()
@@ -266,6 +267,8 @@ def main() -> None:
             flush_l2(flush)
             torch.cuda.synchronize()
             device_ms += loop.run_timed(s)
+            if on_stride is not None:
+                on_stride(loop)
         barrier()
         t1 = time.perf_counter()
         time.sleep(0.3)  # let the sampler flush the last line of the region
@@ -378,7 +381,9 @@ def main() -> None:
         # the plain Monte Carlo barostat on the same box, timed the same way
         plain = steploop.StepLoop.from_parsed(system, state, steploop.RunOptions(seed=7 + rank, device=local,
                                                                                 max_batch=args.stride))
-        plain_s, _ = timed(plain)
+        plain_volumes = []
+        plain_before = plain.barostat_statistics()
+        plain_s, _ = timed(plain, lambda lp: plain_volumes.append(abs(np.linalg.det(lp.box_vectors()))))
         plain_stats = plain.barostat_statistics()
         plain.destroy()
         # the screened barostat: learn from the first attempts (untimed), then time
@@ -389,12 +394,15 @@ def main() -> None:
         loop.run(args.surrogate_attempts * frequency)
         t_train = time.perf_counter() - t_train
         before = loop.barostat_statistics()
-        total_s, clock_summary = timed(loop)
+        volumes = []
+        total_s, clock_summary = timed(loop, lambda lp: volumes.append(abs(np.linalg.det(lp.box_vectors()))))
         after = loop.barostat_statistics()
         steps_per_s = args.steps / total_s
         value = steps_per_s * NS_PER_DAY_PER_STEP_PER_S * world
         plain_value = args.steps / plain_s * NS_PER_DAY_PER_STEP_PER_S * world
         attempts = after["attempts"] - before["attempts"]
+        exact_proposals = after["exactEvaluations"] - before["exactEvaluations"] - attempts
+        plain_attempts = plain_stats["attempts"] - plain_before["attempts"]
         cfg = {"workload": "NPT TIP3P cube 10 nm, 1 bar, 300 K, Monte Carlo volume move every "
                            f"{frequency} steps, screened by the device-trained network",
                "atoms": system.particle_count,
@@ -406,7 +414,14 @@ def main() -> None:
                                                   / max(1, attempts),
                              "screened_timed": after["screened"] - before["screened"],
                              "plain_exact_per_attempt": plain_stats["exactEvaluations"]
-                                                        / max(1, plain_stats["attempts"])}}
+                                                        / max(1, plain_stats["attempts"]),
+                             "attempts_per_ps": attempts / (args.steps * TIME_STEP_PS),
+                             "stage1_acceptance": exact_proposals / max(1, attempts),
+                             "stage2_acceptance": (after["accepted"] - before["accepted"]) / max(1, exact_proposals),
+                             "plain_acceptance": (plain_stats["accepted"] - plain_before["accepted"])
+                                                 / max(1, plain_attempts),
+                             "mean_volume_nm3": float(np.mean(volumes)) if volumes else None,
+                             "plain_mean_volume_nm3": float(np.mean(plain_volumes)) if plain_volumes else None}}
         e2e_s, h2d, d2h = end_to_end(loop, [state])
         e2e_value = args.steps / e2e_s * NS_PER_DAY_PER_STEP_PER_S * world
         result_loop, n_atoms = loop, system.particle_count
@@ -445,9 +460,12 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cpu_value, _, _, sample = cpu_rate(config, 1000, args.cpu_budget, threads)
+        one_value, _, _, one_sample = cpu_rate(config, 1000, args.cpu_budget / 2, 1)
         result["cpu_baseline"] = {
             "value": cpu_value, "unit": "ns/day", "cores": threads, "kind": "port",
-            "sample": sample + " (f64 C++ restatement of src/reference, OpenMP over all host threads)"}
+            "sample": sample + " (f64 C++ restatement of src/reference, OpenMP over all host threads)",
+            "single_thread": {"value": one_value, "cores": 1,
+                              "sample": one_sample + " (one thread, like the reference's single JS thread)"}}
     loop.destroy()
     if rank == 0:
         print(json.dumps(result))

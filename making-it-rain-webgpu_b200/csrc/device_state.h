@@ -7,7 +7,8 @@
 
 namespace mdb {
 
-struct BondDev { int a, b, sys; float r0, k; };
+// r0sq_hi + r0sq_lo is r0^2 to about 48 bits (an unevaluated f32 pair).
+struct BondDev { int a, b, sys; float r0, k, r0sq_hi, r0sq_lo; };
 struct AngleDev { int a, b, c, sys; float theta0, k; };
 struct TorsionDev { int a, b, c, d, sys, periodicity; float phase, k; };
 // qq values already carry ONE_4PI_EPS0 (kJ/mol nm).

@@ -66,12 +66,49 @@ __device__ __forceinline__ void add_virial(const Dev& d, const SysDev& S, float3
     for (int b = 0; b < 3; ++b) add_fixed(&w[3 * a + b], rr[a] * ff[b]);
 }
 
+// Error-free transformations on f32 (Knuth's TwoSum; the fma product error).
+// The _rn intrinsics keep the compiler from contracting them into fma.
+__device__ __forceinline__ float two_sum(float a, float b, float& err) {
+  const float s = __fadd_rn(a, b), bb = __fsub_rn(s, a);
+  err = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return s;
+}
+
+// The stretch r - r0 of one bond, to about 1e-12 nm where plain f32 gives
+// r0 * 2^-24 (~7e-9 nm, or ~3e-3 kJ/mol/nm of force at k = 4.8e5 on a C=O
+// bond).  The exact integer separation is split into f32 hi + lo parts,
+// r^2 - r0^2 is accumulated with TwoSum and fma product errors, and divided by
+// r + r0.  Still f32 arithmetic throughout.
+__device__ __forceinline__ float bond_stretch(const Dev& d, const BondDev& t, float3& v, float& r) {
+  const long long D[3] = {d.px[t.b] - d.px[t.a], d.py[t.b] - d.py[t.a], d.pz[t.b] - d.pz[t.a]};
+  float hi[3], lo[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float h = __ll2float_rn(D[k]);
+    hi[k] = h * 2.3283064365386963e-10f;
+    lo[k] = __ll2float_rn(D[k] - __float2ll_rn(h)) * 2.3283064365386963e-10f;
+  }
+  float p[3], tail = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    p[k] = __fmul_rn(hi[k], hi[k]);
+    tail += fmaf(hi[k], hi[k], -p[k]) + (2.f * hi[k] + lo[k]) * lo[k];
+  }
+  float e1, e2;
+  const float s1 = two_sum(p[0], p[1], e1);
+  const float s2 = two_sum(s1, p[2], e2);
+  const float delta = __fsub_rn(s2, t.r0sq_hi) + (e1 + e2 + tail - t.r0sq_lo);
+  v = make_float3(hi[0] + lo[0], hi[1] + lo[1], hi[2] + lo[2]);
+  r = sqrtf(s2);
+  return delta / (r + t.r0);
+}
+
 template <bool ENERGY>
 __device__ void bond(const Dev& d, const BondDev& t) {
   const SysDev& S = d.sys[t.sys];
-  const float3 v = diff(d, t.a, t.b);
-  const float r = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-  const float dr = r - t.r0;
+  float3 v;
+  float r;
+  const float dr = bond_stretch(d, t, v, r);
   add_energy<ENERGY>(d, S, kEBond, 0.5f * t.k * dr * dr);
   const float sc = t.k * dr / r;
   add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);

@@ -259,8 +259,12 @@ int prepare_system(const mdb_system_desc& in, const mdb_state_desc& state, const
     error = "bonded-term indices out of range";
     return MDB_ERR_INVALID_ARGUMENT;
   }
-  for (int t = 0; t < in.n_bonds; ++t)
-    h.bonds.push_back({in.bond_p1[t], in.bond_p2[t], 0, float(in.bond_length[t]), float(in.bond_k[t])});
+  for (int t = 0; t < in.n_bonds; ++t) {
+    const double r0sq = in.bond_length[t] * in.bond_length[t];
+    const float r0sq_hi = float(r0sq);
+    h.bonds.push_back({in.bond_p1[t], in.bond_p2[t], 0, float(in.bond_length[t]), float(in.bond_k[t]), r0sq_hi,
+                       float(r0sq - double(r0sq_hi))});
+  }
   for (int t = 0; t < in.n_angles; ++t)
     h.angles.push_back({in.angle_p1[t], in.angle_p2[t], in.angle_p3[t], 0, float(in.angle_theta[t]),
                         float(in.angle_k[t])});

@@ -368,6 +368,28 @@ inline void add_virial(double* w, double rx, double ry, double rz, double fx, do
 
 struct PairAcc { double coulomb = 0, lj = 0; int64_t pairs = 0; double vir[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}; };
 
+// erfc-Coulomb plus Lorentz-Berthelot LJ of one pair at squared distance r2
+// (nonbonded.ts:330): the energies, and dE/dr as the return value.
+inline double pair_terms(const mdb_system_desc* s, double alpha, int i, int j, double r2, double& coulomb,
+                         double& lj) {
+  const double r = std::sqrt(r2);
+  const double qq = kOne4PiEps0 * s->charge[i] * s->charge[j];
+  const double ar = alpha * r;
+  const double ec = erfc_ref(ar);
+  coulomb = qq * ec / r;
+  double dEdR = qq * (-ec / r2 - alpha * erf_derivative(ar) / r);
+  lj = 0;
+  const double eps = std::sqrt(s->epsilon[i] * s->epsilon[j]);
+  if (eps != 0) {
+    const double sig = 0.5 * (s->sigma[i] + s->sigma[j]);
+    const double s6 = std::pow(sig * sig / r2, 3);
+    const double s12 = s6 * s6;
+    lj = 4 * eps * (s12 - s6);
+    dEdR += (4 * eps / r) * (6 * s6 - 12 * s12);
+  }
+  return dEdR;
+}
+
 inline void pair_interaction(const mdb_system_desc* s, const double* pos, const double* box,
                              double alpha, double cut2, int i, int j, double* forces,
                              PairAcc& acc) {
@@ -377,20 +399,8 @@ inline void pair_interaction(const mdb_system_desc* s, const double* pos, const 
   const double r2 = dx * dx + dy * dy + dz * dz;
   if (r2 >= cut2) return;
   const double r = std::sqrt(r2);
-  const double qq = kOne4PiEps0 * s->charge[i] * s->charge[j];
-  const double ar = alpha * r;
-  const double ec = erfc_ref(ar);
-  const double coulomb = qq * ec / r;
-  double dEdR = qq * (-ec / r2 - alpha * erf_derivative(ar) / r);
-  double lj = 0;
-  const double eps = std::sqrt(s->epsilon[i] * s->epsilon[j]);
-  if (eps != 0) {
-    const double sig = 0.5 * (s->sigma[i] + s->sigma[j]);
-    const double s6 = std::pow(sig * sig / r2, 3);
-    const double s12 = s6 * s6;
-    lj = 4 * eps * (s12 - s6);
-    dEdR += (4 * eps / r) * (6 * s6 - 12 * s12);
-  }
+  double coulomb, lj;
+  const double dEdR = pair_terms(s, alpha, i, j, r2, coulomb, lj);
   if (forces) {
     const double sc = dEdR / r;
     forces[3 * i] += sc * dx;
@@ -1379,6 +1389,81 @@ int32_t orc_potential(const mdb_system_desc* sys, const double* positions, const
   Potential p = evaluate(sys, positions, box, grid, threads, naive_direct != 0, forces);
   if (out) *out = p.e;
   return p.status;
+}
+
+// The non-excluded pairs whose minimum-image distance lies within `eps` of
+// the cutoff, with the force each would put on its first atom if it were
+// inside.  The direct-space potential is discontinuous there (nonbonded.ts:330
+// truncates erfc-Coulomb and LJ without a shift), so a pair this close to the
+// cutoff may be counted by one precision and not by another; the parity tests
+// use this list to allow either.  Single-threaded; writes at most `max_pairs`
+// and returns how many there are.  No reference counterpart.
+int32_t orc_cutoff_shell(const mdb_system_desc* sys, const double* positions, const double box[9],
+                         double eps, int32_t max_pairs, int32_t* first, int32_t* second,
+                         double* force_on_first, int32_t* inside) {
+  const int n = sys->n_particles;
+  const double cut = sys->cutoff, lo2 = (cut - eps) * (cut - eps), hi2 = (cut + eps) * (cut + eps);
+  const double alpha = splitting_parameter(sys);
+  const auto excluded = exclusion_set(sys);
+  const Vec3 widths = perpendicular_widths(box);
+  int counts[3];
+  for (int a = 0; a < 3; ++a) counts[a] = std::max(1, int(std::floor(widths[a] / (cut + eps))));
+  const bool naive = counts[0] < 3 || counts[1] < 3 || counts[2] < 3;
+  int32_t found = 0;
+  auto visit = [&](int i, int j) {
+    const int lo = std::min(i, j), hi = std::max(i, j);
+    if (excluded.count(uint64_t(lo) * 2097152ull + hi)) return;
+    double dx = positions[3 * hi] - positions[3 * lo], dy = positions[3 * hi + 1] - positions[3 * lo + 1],
+           dz = positions[3 * hi + 2] - positions[3 * lo + 2];
+    nearest_image(box, dx, dy, dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 < lo2 || r2 >= hi2) return;
+    if (found < max_pairs) {
+      double coulomb, lj;
+      const double sc = pair_terms(sys, alpha, lo, hi, r2, coulomb, lj) / std::sqrt(r2);
+      first[found] = lo;
+      second[found] = hi;
+      force_on_first[3 * found] = sc * dx;
+      force_on_first[3 * found + 1] = sc * dy;
+      force_on_first[3 * found + 2] = sc * dz;
+      inside[found] = r2 < cut * cut ? 1 : 0;
+    }
+    ++found;
+  };
+  if (naive) {
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) visit(i, j);
+    return found;
+  }
+  const int ncell = counts[0] * counts[1] * counts[2];
+  const auto inv = inverse_box(box);
+  std::vector<int> cell_of(n), start(ncell + 1, 0), order(n);
+  auto bucket = [](double f, int div) {
+    const double w = f - std::floor(f);
+    const int idx = int(std::floor(w * div));
+    return idx == div ? div - 1 : idx;
+  };
+  for (int i = 0; i < n; ++i) {
+    const Vec3 f = fractional_of(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], inv);
+    cell_of[i] = (bucket(f[0], counts[0]) * counts[1] + bucket(f[1], counts[1])) * counts[2] + bucket(f[2], counts[2]);
+    start[cell_of[i] + 1]++;
+  }
+  for (int c = 0; c < ncell; ++c) start[c + 1] += start[c];
+  std::vector<int> cur(start.begin(), start.end() - 1);
+  for (int i = 0; i < n; ++i) order[cur[cell_of[i]]++] = i;
+  for (int cell = 0; cell < ncell; ++cell) {
+    const int cz = cell % counts[2], cy = (cell / counts[2]) % counts[1], cx = cell / (counts[1] * counts[2]);
+    for (int ddx = -1; ddx <= 1; ++ddx)
+      for (int ddy = -1; ddy <= 1; ++ddy)
+        for (int ddz = -1; ddz <= 1; ++ddz) {
+          const int nb = (((cx + ddx + counts[0]) % counts[0]) * counts[1] + (cy + ddy + counts[1]) % counts[1]) *
+                             counts[2] + (cz + ddz + counts[2]) % counts[2];
+          if (nb < cell) continue;
+          for (int a = start[cell]; a < start[cell + 1]; ++a)
+            for (int b = nb == cell ? a + 1 : start[nb]; b < start[nb + 1]; ++b) visit(order[a], order[b]);
+        }
+  }
+  return found;
 }
 
 int32_t orc_potential_virial(const mdb_system_desc* sys, const double* positions, const double box[9],

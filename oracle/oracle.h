@@ -94,6 +94,14 @@ int32_t orc_potential(const mdb_system_desc* sys, const double* positions,
 int32_t orc_mlp_gradient(const float* params, const float* x, const float* t, int32_t n, double* grad,
                          double* loss);
 
+/* The non-excluded pairs within `eps` of the cutoff (minimum image), the
+ * force each would put on `first` if inside, and whether it is inside in f64.
+ * Writes at most `max_pairs`; returns the total.  No reference counterpart:
+ * the parity tests allow such pairs either way. */
+int32_t orc_cutoff_shell(const mdb_system_desc* sys, const double* positions, const double box[9],
+                         double eps, int32_t max_pairs, int32_t* first, int32_t* second,
+                         double* force_on_first, int32_t* inside);
+
 int32_t orc_potential_virial(const mdb_system_desc* sys, const double* positions, const double box[9],
                              const int32_t* grid, int32_t threads, double* forces, orc_energies* out,
                              double virial[9]);

@@ -86,6 +86,8 @@ def lib() -> C.CDLL:
                                          C.c_int32, _dp, _dp]),
         "orc_potential_virial": (C.c_int32, [_SD, _dp, _dp, C.POINTER(C.c_int32), C.c_int32, _dp,
                                              C.POINTER(Energies), _dp]),
+        "orc_cutoff_shell": (C.c_int32, [_SD, _dp, _dp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32), _dp, C.POINTER(C.c_int32)]),
         "orc_ewald_reciprocal": (C.c_int32, [_SD, _dp, _dp, C.c_double, C.c_int32, _dp, _dp]),
         "orc_split_counts": (C.c_int32, [_SD] + [C.POINTER(C.c_int32)] * 4),
         "orc_degrees_of_freedom": (C.c_double, [_SD]),
@@ -143,6 +145,25 @@ def potential_virial(system: System, positions, box=None, grid=None, threads: in
     if status != 0:
         raise RuntimeError(f"oracle potential failed with status {status}")
     return e.as_dict(), f.reshape(-1, 3), w.reshape(3, 3)
+
+
+def cutoff_shell(system: System, positions, box=None, eps: float = 2e-7):
+    """Pairs within `eps` nm of the cutoff: (first, second, force on first if
+    inside (k, 3), inside in f64 (k,) bool)."""
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1))
+    b = _box(system.box if box is None else box)
+    cap = 64
+    while True:
+        i = np.zeros(cap, np.int32)
+        j = np.zeros(cap, np.int32)
+        f = np.zeros(3 * cap)
+        inside = np.zeros(cap, np.int32)
+        ip = C.POINTER(C.c_int32)
+        k = lib().orc_cutoff_shell(system.desc().pointer(), _p(pos), _p(b), eps, cap, i.ctypes.data_as(ip),
+                                   j.ctypes.data_as(ip), _p(f), inside.ctypes.data_as(ip))
+        if k <= cap:
+            return i[:k], j[:k], f.reshape(-1, 3)[:k], inside[:k].astype(bool)
+        cap = k
 
 
 def mlp_gradient(params, x, t):

@@ -197,3 +197,32 @@ def test_bspline_partition_of_unity_and_moduli(oracle):
     mod = np.zeros(30)
     oracle.lib().orc_bspline_moduli(30, mod.ctypes.data_as(dp))
     assert np.all(mod > 0) and abs(mod[0] - 1) < 1e-12
+
+
+def test_cutoff_shell_lists_pairs_at_the_cutoff(oracle):
+    """Pairs within eps of the cutoff, with the force each would add if inside
+    (erfc-Coulomb plus LJ at the pair's own distance); pairs farther away and
+    excluded pairs are not listed."""
+    from mdb200.system import Nonbonded, System
+
+    cut, alpha = 1.0, oracle.lib().orc_ewald_alpha(1.0, 5e-4)
+    d = [cut - 5e-8, cut + 5e-8, cut - 1e-3]
+    pos = np.array([[1, 1, 1], [1 + d[0], 1, 1], [1, 3.5, 1], [1, 3.5 + d[1], 1], [3, 5, 5], [3 + d[2], 5, 5],
+                    [6, 1, 1], [6, 1 + cut - 1e-8, 1]], dtype=np.float64)
+    q = np.array([0.5, -0.7, 0.4, 0.4, 1.0, -1.0, 0.3, 0.3])
+    system = System(masses=np.ones(8), box=np.eye(3) * 9.0,
+                    nonbonded=Nonbonded(cutoff=cut, ewald_tolerance=5e-4, charge=q, sigma=np.full(8, 0.3),
+                                        epsilon=np.full(8, 0.5),
+                                        exception_p1=np.array([6], np.int32), exception_p2=np.array([7], np.int32),
+                                        exception_charge_prod=np.zeros(1), exception_sigma=np.full(1, 0.3),
+                                        exception_epsilon=np.zeros(1)))
+    first, second, force, inside = oracle.cutoff_shell(system, pos, eps=2e-7)
+    assert sorted(zip(first.tolist(), second.tolist())) == [(0, 1), (2, 3)]
+    for a, b, f, ins in zip(first, second, force, inside):
+        r = float(np.linalg.norm(pos[b] - pos[a]))
+        assert ins == (r < cut)
+        qq = 138.935458 * q[a] * q[b]
+        s6 = (0.3 / r) ** 6
+        dedr = qq * (-math.erfc(alpha * r) / r**2 - alpha * 2 / math.sqrt(math.pi) * math.exp(-(alpha * r) ** 2) / r)
+        dedr += 4 * 0.5 / r * (6 * s6 - 12 * s6 * s6)
+        np.testing.assert_allclose(f, dedr / r * (pos[b] - pos[a]), rtol=1e-6)
