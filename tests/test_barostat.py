@@ -140,3 +140,42 @@ def test_delayed_acceptance_saves_exact_evaluations():
     assert s["exact_per_attempt"] < 0.9 * p["exact_per_attempt"]
     assert s["surrogateRms"] < 3 * KB * 300.0
     assert abs(s["volume"] - p["volume"]) < 0.03 * p["volume"]
+
+
+def test_screened_and_plain_barostat_sample_the_same_volume_distribution():
+    """Detailed balance is unchanged by the screening stage: from the same
+    equilibrated state, the plain and the screened barostat give the same
+    mean volume within four combined standard errors (block averages of 20
+    blocks over 20,000 attempts each), and volume fluctuations within 25%."""
+    from mdb200 import steploop, synth
+    from mdb200.system import State
+
+    system, state = synth.water_box(n_waters=884, width=3.0, seed=1, grid=(30, 30, 30), barostat=(1.0, 300.0, 4))
+    warm = steploop.StepLoop.from_parsed(system, state, steploop.RunOptions(seed=5))
+    warm.run(20000)
+    start = State(positions=warm.positions(), box=warm.box_vectors(), velocities=warm.velocities(), step=warm.steps)
+    warm.destroy()
+    samples = {}
+    for name, attempts, seed in (("plain", 0, 11), ("screened", 300, 12)):
+        loop = steploop.StepLoop.from_parsed(system, start,
+                                             steploop.RunOptions(seed=seed, surrogate_attempts=attempts))
+        loop.run(1200)  # the screened arm's 300 training attempts; the same steps for the plain one
+        v = []
+        for _ in range(2000):
+            loop.run(40)
+            v.append(abs(np.linalg.det(loop.box_vectors())))
+        stats = loop.barostat_statistics()
+        loop.destroy()
+        samples[name] = np.array(v)
+        print(name, float(np.mean(v)), float(np.std(v)), stats)
+    means, errors = {}, {}
+    for name, v in samples.items():
+        blocks = v.reshape(20, -1).mean(axis=1)
+        means[name] = float(v.mean())
+        errors[name] = float(blocks.std(ddof=1) / math.sqrt(len(blocks)))
+    gap = abs(means["screened"] - means["plain"])
+    bound = 4.0 * math.hypot(errors["screened"], errors["plain"])
+    print("mean volumes", means, "standard errors", errors, "gap", gap, "bound", bound)
+    assert gap < bound
+    ratio = samples["screened"].std() / samples["plain"].std()
+    assert 0.75 < ratio < 1.25, ratio
