@@ -3,9 +3,11 @@
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl mdb|reference]
 
 One "step" is one MD step (forces + LFMiddle + constraints) of the whole
-workload.  With N > 1 (torchrun, one process per GPU) every rank advances its
-own independent replica -- the step loop does not shard (replicas only) -- and
-`value` is the sum over ranks, timed as the max over ranks.
+workload.  With N > 1 (torchrun, one process per GPU) a single-system workload
+runs one independent replica per rank (one system does not shard: replicas
+only) and `value` is the sum over ranks; the 64-system ensemble is split
+between the ranks by longest processing time on atom count, and `value` is
+the whole ensemble's rate.  Both are timed as the max over ranks.
 
 Timing: W untimed warm-up steps, then exactly K steps replayed as CUDA-graph
 strides of `--stride` steps, each stride timed with CUDA events recorded on the
@@ -211,7 +213,8 @@ def main() -> None:
         print(json.dumps({
             "impl": "reference", "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": args.gpus,
             "steps": n, "warmup": 1, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "strong" if config == "ensemble-64" else "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
             "config": {**cfg, "parallelism": "host threads", "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port",
                              "sample": sample + " (f64 C++ restatement of src/reference; the TypeScript "
@@ -330,12 +333,18 @@ def main() -> None:
                     "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback", "stages": stages,
                 "launches_per_step": prof["launches_per_step"]}
 
+    scaling = "weak"  # single systems run as one replica per rank
     if config == "ensemble-64":
-        from mdb200 import synth
+        from mdb200 import shard, synth
 
-        members = synth.config_ensemble_64(seed=1 + rank)
-        systems = [m[0] for m in members]
-        states = [m[1] for m in members]
+        # one ensemble for the whole job; each rank advances its longest-
+        # processing-time share of the systems (no exchange during a stride)
+        members = synth.config_ensemble_64(seed=1)
+        share = shard.rank_share([m[0].particle_count for m in members], rank, world)
+        systems = [members[i][0] for i in share]
+        states = [members[i][1] for i in share]
+        n_total = len(members)
+        scaling = "strong"
         # plain engine: every system alone, default tuning, timed the same way
         plain_ms = 0.0
         plain_steps = max(100, min(args.steps, 500))
@@ -358,20 +367,22 @@ def main() -> None:
         loop = steploop.StepLoop.batch(systems, states, opts)
         total_s, clock_summary = timed(loop)
         steps_per_s = args.steps / total_s
-        n_sys = len(systems)
-        value = steps_per_s * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
-        plain_value = 1000.0 / plain_ms * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
+        value = steps_per_s * n_total * NS_PER_DAY_PER_STEP_PER_S
+        plain_value = 1000.0 / plain_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
         e2e_s, h2d, d2h = end_to_end(loop, states)
-        cfg = {"workload": f"{n_sys} independent systems, 2,000-30,000 atoms log-uniform, cubic or rhombic "
+        cfg = {"workload": f"{n_total} independent systems, 2,000-30,000 atoms log-uniform, cubic or rhombic "
                            "dodecahedral TIP3P, half with an Ala helix of 10-40 residues where it fits",
-               "systems": n_sys, "atoms": sum(s.particle_count for s in systems),
+               "systems": n_total, "atoms": sum(m[0].particle_count for m in members),
+               "systems_per_rank": len(systems), "atoms_per_rank": sum(s.particle_count for s in systems),
+               "sharding": "longest-processing-time on atom count, no collective during a stride"
+                           if world > 1 else "one GPU",
                "aggregate": "system-ns/day summed over the systems",
                "plain_engine_ns_per_day": plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
                "batched_over_plain": value / plain_value,
                "autotuner": {str(b): {k: round(v, 4) if isinstance(v, float) else v for k, v in r.items()}
                              for b, r in buckets.items()}}
         result_loop, n_atoms = loop, cfg["atoms"]
-        e2e_value = args.steps / e2e_s * n_sys * NS_PER_DAY_PER_STEP_PER_S * world
+        e2e_value = args.steps / e2e_s * n_total * NS_PER_DAY_PER_STEP_PER_S
         system, state = systems[0], states[0]
     elif config == "npt-100k":
         from mdb200 import synth
@@ -453,10 +464,12 @@ def main() -> None:
     result = {
         "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_s * 1000.0 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair math, int64 fixed-point accumulation",
+        "scaling": scaling, "vs_baseline": None, "dtype": "f32 pair math, int64 fixed-point accumulation",
         "data": "synthetic",
         "config": {**cfg, "time_step_ps": TIME_STEP_PS, "steps_per_s": steps_per_s * world,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "parallelism": ("single GPU" if world == 1 else
+                                   f"ensemble sharded over {world} GPUs" if scaling == "strong" else
+                                   f"replicas x{world}"),
                    "l2": f"flushed (256 MB write) between timed strides of {stride} steps"},
         "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps},
