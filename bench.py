@@ -192,6 +192,8 @@ def main() -> None:
     ap.add_argument("--impl", default="mdb", choices=("mdb", "reference"))
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default=None,
+                    help="skin,sort_cell,tile_atoms,prune_tiles[,inner_skin]: skip the autotuner (profiling runs)")
     ap.add_argument("--surrogate-attempts", type=int, default=2000,
                     help="npt-100k: exact attempts the screening network learns from (2,000 = 50,000 steps)")
     args = ap.parse_args()
@@ -320,7 +322,9 @@ def main() -> None:
             "pme_gather_ms": prof["ms_pme_gather"], "integrate_ms": prof["ms_integrate"],
             "list_check_ms": prof["ms_list_check"], "list_rebuild_ms": prof["ms_list_rebuild"],
             "step_ms": prof["ms_step"], "pairs_within_cutoff": pairs, "tiles": prof["tiles"],
-            "pair_fraction_in_tiles": pairs / max(1, prof["tiles"] * 1024),
+            "tiles_read": prof["inner_tiles"], "tile_atoms": prof["tile_atoms"],
+            "inner_prune_ms": prof["ms_inner_prune"],
+            "pair_fraction_in_tiles": pairs / max(1, prof["inner_tiles"] * prof["tile_atoms"] ** 2),
             "spread_GBs": spread_bytes / (prof["ms_pme_spread"] / 1000) / 1e9,
             "gather_GBs": gather_bytes / (prof["ms_pme_gather"] / 1000) / 1e9,
             "integrate_GBs": integ_bytes / (prof["ms_integrate"] / 1000) / 1e9,
@@ -447,11 +451,16 @@ def main() -> None:
         system, state, cfg = workload(config, seed=1 + rank)
         # the library's autotuner picks tile shape, skin and sort cell for this
         # system (untimed, like graph capture); the timed run uses its choice
-        best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=200)
+        if args.tuning:
+            v = [float(x) for x in args.tuning.split(",")]
+            best = {"verlet_skin": v[0], "sort_cell": v[1], "tile_atoms": int(v[2]), "prune_tiles": int(v[3]),
+                    "inner_skin": v[4] if len(v) > 4 else 0.0, "candidates": 0, "source": "--tuning"}
+        else:
+            best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=200)
         cfg["autotuner"] = {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
                                    tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"],
-                                            best["prune_tiles"])])
+                                            best["prune_tiles"], best["inner_skin"])])
         loop = steploop.StepLoop.from_parsed(system, state, opts)
         total_s, clock_summary = timed(loop)
         steps_per_s = args.steps / total_s

@@ -168,6 +168,10 @@ typedef struct mdb_tuning {
                           engine: a batch takes the first system's that sets one */
   int32_t prune_tiles; /* 1: each rebuild drops the tiles with no pair inside cutoff + skin;
                           2: keeps them; 0: default (1).  Per engine, like tile_atoms */
+  double inner_skin;   /* nm; > 0: the pair kernel reads an inner list of the tiles with a pair
+                          inside cutoff + inner_skin, pruned again from the outer list whenever an
+                          atom has moved inner_skin / 2 (results are bit-identical to the outer
+                          list's); negative: off; 0: the default */
 } mdb_tuning;
 
 typedef struct mdb_run_options {
@@ -261,6 +265,9 @@ typedef struct mdb_profile {
   int64_t tiles;
   int64_t atoms;
   int64_t mesh_points;
+  int64_t inner_tiles;         /* tiles the pair kernel reads (the inner list, or the whole list) */
+  double ms_inner_prune;       /* an inner-list prune with no rebuild (0 without an inner list) */
+  int64_t tile_atoms;          /* atoms per cluster: a tile holds tile_atoms^2 pair slots */
 } mdb_profile;
 
 /* Mirrors `StepLoop.verletFlags`, src/gpu/loop.ts:941. */
@@ -271,6 +278,9 @@ typedef struct mdb_neighbour_stats {
   int64_t blocks;         /* 32-atom clusters */
   int32_t overflowed;     /* a table ran out of room since creation */
   double skin;            /* nm */
+  int64_t inner_tiles;    /* tiles of the inner list the pair kernel reads (= tiles without one) */
+  int64_t prunes;         /* inner-list prunes between rebuilds since creation */
+  double inner_skin;      /* nm; 0 without an inner list */
 } mdb_neighbour_stats;
 
 typedef struct mdb_engine mdb_engine;
@@ -399,7 +409,7 @@ int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* cha
 
 /*
  * Autotuner (no reference counterpart).  Times every candidate of a fixed grid
- * of (tile_atoms, prune_tiles, verlet_skin, sort_cell) on the device -- a temporary engine per
+ * of (tile_atoms, prune_tiles, verlet_skin, sort_cell, inner_skin) on the device -- a temporary engine per
  * candidate, `steps` graph-replayed steps after a warm-up of the same length,
  * CUDA-event timed -- and returns the fastest in `best` and its ms per step.
  * `tried` (may be NULL) receives the number of candidates.  The state the

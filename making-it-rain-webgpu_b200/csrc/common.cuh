@@ -59,7 +59,10 @@ enum UnitKind : int { kUnitFree = 0, kUnitSettle = 1, kUnitShake = 2, kUnitStar 
 
 // Integrate blocks: kIntegrateUnits units per block, their atoms staged in a
 // shared-memory table of at most kIntegrateTable entries.
-constexpr int kIntegrateUnits = 32;
+#ifndef MDB_INTEGRATE_UNITS
+#define MDB_INTEGRATE_UNITS 32
+#endif
+constexpr int kIntegrateUnits = MDB_INTEGRATE_UNITS;
 constexpr int kIntegrateTable = kIntegrateUnits * kMaxClusterAtoms;
 
 // One integration unit: a free atom, a SETTLE water, or a SHAKE cluster.
@@ -98,6 +101,9 @@ struct SysDev {
   int pc_half[3];    // half of the diagonal in pair-coordinate units
   float pc_inv_diag[3];  // 1/diagonal in pair-coordinate units
   float cut2, list2, half_skin2, alpha, alpha_2_sqrtpi;
+  // the inner list: tiles with a pair inside (cutoff + inner skin)^2, re-pruned
+  // from the outer list once an atom has moved (inner skin / 2)^2 since the last prune
+  float inner2, half_inner2;
   // PME
   int grid[3];
   int kzh;            // Kz/2 + 1

@@ -25,6 +25,7 @@ struct Dev {
   int n_atoms, n_slots, n_blocks, n_cells, n_units, n_iblk;
   int cluster;        // atoms per cluster of the tile list: 8 or 32 (n_blocks counts clusters)
   int prune;          // rebuilds drop tiles with no pair inside cutoff + skin
+  int inner;          // the pair kernel reads the inner list (see in_tiles)
   int any_triclinic;  // some system's box is triclinic: the pair kernel takes the general minimum image
 
   // atoms, original order
@@ -53,13 +54,13 @@ struct Dev {
   float4 *bb_lo, *bb_hi;  // per cluster
   float4 *sb_lo, *sb_hi;  // per 32-slot super-cluster (the cluster boxes themselves when clusters are 32)
   int* fold;              // per slot: the lattice translation of the last rebuild's fold (3 x 10 bits)
-  int4* tile_shift;
   int2* raw_tiles;        // the fill pass's list, before pruning
   unsigned int* raw_masks;
   int4* raw_shift;
   unsigned char* tile_alive;  // per raw tile: some pair within cutoff + skin
   int* row_alive;         // per cluster: surviving tiles of its row
-  int* alive_start;       // per cluster: their start after pruning       // per tile: lattice shift of J in pair-coordinate units; w = 1: per-pair minimum image
+  int* alive_start;       // per cluster: their start after pruning
+  int4* tile_shift;       // per tile: lattice shift of J in pair-coordinate units; w = 1: per-pair minimum image
   int* tile_cnt;
   int* tile_start;
   const int* block_sys;
@@ -75,6 +76,24 @@ struct Dev {
   int* tile_count;   // per system
   int* tile_prefix;  // S+1
   int tile_cap_total; // sum of the systems' tile capacities
+
+  // inner list: the outer list's tiles that have a pair inside cutoff + inner
+  // skin, in each system's region of the same capacity; the pair kernel's list
+  // when `inner` is set.  Rebuilt from the outer list (copies of the tile, its
+  // mask words and its shift) at every rebuild and whenever an atom has moved
+  // half the inner skin since the last prune.
+  int2* in_tiles;
+  unsigned int* in_masks;
+  int4* in_shift;
+  int* in_count;      // per system
+  int* in_prefix;     // S+1
+  long long *prx, *pry, *prz;  // positions at the last prune, by atom
+  float4 *cb_lo, *cb_hi;       // per cluster: bounding box at the last prune (pair coordinates, nm)
+  int* prune_flag;    // set by the integrator: some atom moved inner skin/2
+  int* prune_now;     // snapshot the list kernel acts on
+  int* any_prune;
+  long long* prune_count;  // per system: prunes between rebuilds
+  int* inner_ticket;       // blocks of the inner-list kernel that have finished
 
   // flags and status
   int* rebuild_flag;  // set by the integrator: some atom moved skin/2
@@ -133,6 +152,7 @@ bool launch_list(const Dev& d, cudaStream_t s);            // sort + wrap + tile
 void launch_rebuild_sort(const Dev& d, cudaStream_t s);     // phases 0-4
 void launch_wrap(const Dev& d, cudaStream_t s);
 void launch_rebuild_tiles(const Dev& d, cudaStream_t s);    // phases 5-9
+void launch_inner_prune(const Dev& d, cudaStream_t s);      // the inner list, when one is due
 void launch_nonbonded(const Dev& d, bool energy, cudaStream_t s);
 void launch_listed(const Dev& d, bool energy, cudaStream_t s);
 void launch_pme(const Dev& d, bool energy, cudaStream_t s);

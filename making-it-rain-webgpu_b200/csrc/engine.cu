@@ -43,6 +43,7 @@ namespace {
 
 constexpr double kCellWidth = 0.25;  // nm, fractional cells of the spatial sort
 constexpr int kDefaultCluster = 8;   // atoms per cluster of the tile list
+constexpr double kDefaultInnerSkin = -1.0;  // nm; <= 0: no inner list unless a tuning asks for one
 // Capacity of the dense tile list, per cluster: about three times the mean
 // row at a 0.2 nm skin in water (~120 tiles for 8-atom clusters, ~90 for 32).
 int row_cap_for(int cluster) { return cluster == 8 ? 384 : 192; }
@@ -92,7 +93,7 @@ struct mdb_engine {
   Dev d{};
   std::vector<Allocation> allocs;
   cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
-  cudaEvent_t fork = nullptr, join1 = nullptr, join2 = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t fork = nullptr, listed = nullptr, join1 = nullptr, join2 = nullptr, t0 = nullptr, t1 = nullptr;
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t step = 0;
   std::string error;
@@ -105,6 +106,7 @@ struct mdb_engine {
   std::vector<int> mol_first, mol_count;  // per system: its molecules in d.mol_off
   double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel
   std::vector<double> sort_cell;   // per system, nm
+  std::vector<double> inner_skin;  // per system, nm; <= 0: that system's inner list is its outer list
 };
 
 namespace {
@@ -246,19 +248,28 @@ int check_device_status(mdb_engine* e) {
 // Sort, wrap and tile list: one cooperative launch when the device can, else
 // the phase kernels one by one.
 void list_kernels(mdb_engine* e, cudaStream_t st) {
-  if (e->coop_list && launch_list(e->d, st)) return;
-  launch_rebuild_sort(e->d, st);
-  launch_wrap(e->d, st);
-  launch_rebuild_tiles(e->d, st);
+  if (!(e->coop_list && launch_list(e->d, st))) {
+    launch_rebuild_sort(e->d, st);
+    launch_wrap(e->d, st);
+    launch_rebuild_tiles(e->d, st);
+  }
+  launch_inner_prune(e->d, st);
 }
 
+// One step on three streams: the PME spread and transforms depend only on the
+// positions, so they start at once and overlap the list kernels; the gather
+// and the listed terms write forces by slot and wait for the list.
 void launch_step(mdb_engine* e) {
   const Dev& d = e->d;
-  list_kernels(e, e->s0);
   cudaEventRecord(e->fork, e->s0);
   cudaStreamWaitEvent(e->s1, e->fork, 0);
-  cudaStreamWaitEvent(e->s2, e->fork, 0);
-  launch_pme(d, false, e->s1);
+  launch_pme_spread(d, e->s1);
+  launch_pme_fft(d, false, e->s1);
+  list_kernels(e, e->s0);
+  cudaEventRecord(e->listed, e->s0);
+  cudaStreamWaitEvent(e->s1, e->listed, 0);
+  cudaStreamWaitEvent(e->s2, e->listed, 0);
+  launch_pme_gather(d, e->s1);
   launch_listed(d, false, e->s2);
   launch_nonbonded(d, false, e->s0);
   cudaEventRecord(e->join1, e->s1);
@@ -310,12 +321,14 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   const double default_skin = e->opt.verlet_skin < 0 ? 0.15 : e->opt.verlet_skin;
   e->skin.assign(n, default_skin);
   e->sort_cell.assign(n, kCellWidth);
+  e->inner_skin.assign(n, kDefaultInnerSkin);
   e->cluster = kDefaultCluster;
   if (e->opt.tuning) {
     bool shape_set = false, prune_set = false;
     for (int s = 0; s < n; ++s) {
       if (e->opt.tuning[s].verlet_skin > 0) e->skin[s] = e->opt.tuning[s].verlet_skin;
       if (e->opt.tuning[s].sort_cell > 0) e->sort_cell[s] = e->opt.tuning[s].sort_cell;
+      if (e->opt.tuning[s].inner_skin != 0) e->inner_skin[s] = e->opt.tuning[s].inner_skin;
       const int shape = e->opt.tuning[s].tile_atoms;
       if (shape != 0 && shape != 8 && shape != 32)
         return fail(e, MDB_ERR_INVALID_ARGUMENT, "tile_atoms must be 8 or 32");
@@ -405,6 +418,10 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     const double skin = e->skin[s];
     S.list2 = float((h.cutoff + skin) * (h.cutoff + skin));
     S.half_skin2 = float(0.25 * skin * skin);
+    // a system without an inner skin keeps every outer tile and is never re-pruned
+    const double inner = e->inner_skin[s] > 0 ? std::min(e->inner_skin[s], skin) : skin;
+    S.inner2 = float((h.cutoff + inner) * (h.cutoff + inner));
+    S.half_inner2 = e->inner_skin[s] > 0 ? float(0.25 * inner * inner) : 3.0e38f;
     S.alpha = float(h.alpha);
     S.alpha_2_sqrtpi = float(h.alpha * 2.0 / std::sqrt(3.14159265358979323846));
     S.exp_scale = float(-1.0 / (4 * h.alpha * h.alpha));
@@ -589,6 +606,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.tile_cap_total = tiles;
   d.cluster = e->cluster;
   d.prune = e->prune ? 1 : 0;
+  d.inner = 0;
+  for (int s = 0; s < n; ++s) d.inner |= e->inner_skin[s] > 0 ? 1 : 0;
   d.any_triclinic = 0;
   for (int s = 0; s < n; ++s) d.any_triclinic |= e->sd[s].triclinic ? 1 : 0;
   d.n_cells = cells;
@@ -662,6 +681,23 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "surviving tiles per row", d.row_alive, blocks));
   TRY(alloc(e, "surviving tiles start", d.alive_start, blocks));
   TRY(alloc(e, "fold translations", d.fold, slots));
+  TRY(alloc(e, "inner prune flag", d.prune_flag, n));
+  TRY(alloc(e, "inner prune now", d.prune_now, n));
+  TRY(alloc(e, "any inner prune", d.any_prune, 1));
+  TRY(alloc(e, "inner prune count", d.prune_count, n));
+  TRY(alloc(e, "inner prune ticket", d.inner_ticket, 1));
+  if (d.inner) {
+    TRY(alloc(e, "inner tiles", d.in_tiles, tiles));
+    TRY(alloc(e, "inner tile masks", d.in_masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
+    TRY(alloc(e, "inner tile shifts", d.in_shift, tiles));
+    TRY(alloc(e, "inner tile count", d.in_count, n));
+    TRY(alloc(e, "inner tile prefix", d.in_prefix, n + 1));
+    TRY(alloc(e, "prune reference.x", d.prx, atoms));
+    TRY(alloc(e, "prune reference.y", d.pry, atoms));
+    TRY(alloc(e, "prune reference.z", d.prz, atoms));
+    TRY(alloc(e, "prune cluster bounds lo", d.cb_lo, blocks));
+    TRY(alloc(e, "prune cluster bounds hi", d.cb_hi, blocks));
+  }
   TRY(alloc(e, "tile count", d.tile_count, n));
   TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
   TRY(alloc(e, "rebuild flag", d.rebuild_flag, n));
@@ -772,6 +808,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->join1, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->join2, cudaEventDisableTiming));
+  CUDA_TRY(e, cudaEventCreateWithFlags(&e->listed, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreate(&e->t0));
   CUDA_TRY(e, cudaEventCreate(&e->t1));
   CUDA_TRY(e, cudaDeviceSynchronize());
@@ -781,6 +818,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   launch_rebuild_sort(d, e->s0);
   launch_wrap(d, e->s0);
   launch_rebuild_tiles(d, e->s0);
+  launch_inner_prune(d, e->s0);
   launch_momentum(d, e->s0);
   CUDA_TRY(e, cudaGetLastError());
   int status = check_device_status(e);
@@ -1285,7 +1323,7 @@ int mdb_destroy(mdb_engine* e, int64_t* leaked_bytes) {
   int64_t leaked = 0;
   for (auto& a : e->allocs)
     if (cudaFree(a.ptr) != cudaSuccess) leaked += int64_t(a.bytes);
-  for (cudaEvent_t ev : {e->fork, e->join1, e->join2, e->t0, e->t1})
+  for (cudaEvent_t ev : {e->fork, e->listed, e->join1, e->join2, e->t0, e->t1})
     if (ev) cudaEventDestroy(ev);
   for (cudaStream_t s : {e->s0, e->s1, e->s2})
     if (s) cudaStreamDestroy(s);
@@ -1302,41 +1340,48 @@ int mdb_system_count(const mdb_engine* e, int32_t* out) {
   return MDB_OK;
 }
 
-// The candidate grid: tile shape (8x8 or 32x32 clusters), tile pruning (a
-// cheaper pair kernel against a longer rebuild), list skin (rebuild frequency
-// against tile count) and spatial-sort cell width (how compact a cluster is).
+// The candidate grid: tile shape (8x8 or 32x32 clusters), tile pruning at
+// rebuilds (a cheaper pair kernel against a longer rebuild), list skin
+// (rebuild frequency against tile count), spatial-sort cell width (how compact
+// a cluster is) and, for 8x8 tiles, an inner list re-pruned between rebuilds
+// (which lets a long skin keep a short pair list).
 int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
                  int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried) {
   if (!system || !state || !options || !best || steps <= 0) return MDB_ERR_INVALID_ARGUMENT;
-  static const double kSkins[] = {0.15, 0.20};
-  static const double kCells[] = {0.20, 0.25, 0.35};
-  static const int kShapes[] = {8, 32};
+  struct Lists { double skin, inner; };
+  static const Lists kLists8[] = {{0.15, -1.0}, {0.20, -1.0}, {0.30, 0.08}, {0.40, 0.08}, {0.50, 0.10}};
+  static const Lists kLists32[] = {{0.15, -1.0}, {0.20, -1.0}};
+  static const double kCells8[] = {0.20, 0.25};
+  static const double kCells32[] = {0.20, 0.25, 0.35};
   static const int kPrune[] = {1, 2};
+  std::vector<mdb_tuning> grid;
+  for (int prune : kPrune) {
+    for (const Lists& l : kLists8)
+      for (double cell : kCells8) grid.push_back(mdb_tuning{l.skin, cell, 8, prune, l.inner});
+    for (const Lists& l : kLists32)
+      for (double cell : kCells32) grid.push_back(mdb_tuning{l.skin, cell, 32, prune, l.inner});
+  }
   double best_ms = std::numeric_limits<double>::infinity();
   int count = 0, last = MDB_OK;
-  for (int shape : kShapes)
-  for (int prune : kPrune)
-  for (double skin : kSkins)
-    for (double cell : kCells) {
-      mdb_tuning t{skin, cell, shape, prune};
-      mdb_run_options o = *options;
-      o.tuning = &t;
-      mdb_engine* e = nullptr;
-      int st = mdb_batch_create(1, system, state, &o, &e);
-      double ms = 0;
-      if (st == MDB_OK) st = mdb_run(e, steps);  // warm-up: lists, graph capture
-      if (st == MDB_OK) st = mdb_run_timed(e, steps, &ms);
-      if (e) mdb_destroy(e, nullptr);
-      ++count;
-      if (st != MDB_OK) {  // a candidate may overflow a table; the others still count
-        last = st;
-        continue;
-      }
-      if (ms / steps < best_ms) {
-        best_ms = ms / steps;
-        *best = t;
-      }
+  for (const mdb_tuning& t : grid) {
+    mdb_run_options o = *options;
+    o.tuning = &t;
+    mdb_engine* e = nullptr;
+    int st = mdb_batch_create(1, system, state, &o, &e);
+    double ms = 0;
+    if (st == MDB_OK) st = mdb_run(e, steps);  // warm-up: lists, graph capture
+    if (st == MDB_OK) st = mdb_run_timed(e, steps, &ms);
+    if (e) mdb_destroy(e, nullptr);
+    ++count;
+    if (st != MDB_OK) {  // a candidate may overflow a table; the others still count
+      last = st;
+      continue;
     }
+    if (ms / steps < best_ms) {
+      best_ms = ms / steps;
+      *best = t;
+    }
+  }
   if (tried) *tried = count;
   if (best_ms_per_step) *best_ms_per_step = best_ms;
   return std::isfinite(best_ms) ? MDB_OK : last;
@@ -1484,6 +1529,18 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   out->blocks = e->sd[s].n_blocks;
   out->overflowed = (err & kErrTileCapacity) ? 1 : 0;
   out->skin = e->skin[s];
+  out->inner_tiles = tiles;
+  out->prunes = 0;
+  out->inner_skin = 0;
+  if (e->d.inner) {
+    int inner = 0;
+    long long prunes = 0;
+    cudaMemcpy(&inner, e->d.in_count + s, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&prunes, e->d.prune_count + s, sizeof(long long), cudaMemcpyDeviceToHost);
+    out->inner_tiles = inner;
+    out->prunes = prunes;
+    out->inner_skin = e->inner_skin[s] > 0 ? std::min(e->inner_skin[s], e->skin[s]) : 0.0;
+  }
   return MDB_OK;
 }
 
@@ -1509,6 +1566,13 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
   int tiles = 0;
   cudaMemcpy(&tiles, d.tile_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost);
   out->tiles = tiles;
+  out->tile_atoms = d.cluster;
+  out->inner_tiles = tiles;
+  if (d.inner) {
+    int inner = 0;
+    cudaMemcpy(&inner, d.in_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost);
+    out->inner_tiles = inner;
+  }
   out->atoms = d.n_atoms;
   for (const auto& h : e->hs) out->mesh_points += int64_t(h.grid[0]) * h.grid[1] * h.grid[2];
   out->repeats = repeats;
@@ -1527,6 +1591,12 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
     cudaMemcpyAsync(d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, st);
     list_kernels(e, st);
   });
+  if (d.inner)
+    out->ms_inner_prune = time([&] {
+      cudaMemcpyAsync(d.prune_now, ones.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(d.any_prune, &one, sizeof(int), cudaMemcpyHostToDevice, st);
+      list_kernels(e, st);
+    });
   out->ms_nonbonded = time([&] { launch_nonbonded(d, false, st); });
   out->ms_listed = time([&] { launch_listed(d, false, st); });
   out->ms_pme_spread = time([&] { launch_pme_spread(d, st); });

@@ -176,33 +176,66 @@ __device__ void phase_cells_order(const Dev& d) {
 // 10-bit counts); between rebuilds the same translation is applied, so the
 // coordinates move continuously (an atom leaves the cell by at most half the
 // skin before the next rebuild) and the tiles' lattice shifts stay valid.
+//
+// With an inner list, a system about to be pruned (or rebuilt) also takes its
+// atoms' positions as the new prune reference and empties its inner list.
 __device__ void phase_wrap(const Dev& d) {
+  if (d.inner && blockIdx.x == 0)
+    for (int s = threadIdx.x; s < d.S; s += blockDim.x)
+      if (d.rebuild_now[s] || d.prune_now[s]) d.in_count[s] = 0;
+  // Lanes of a warp hold 32 consecutive slots (n_slots is a multiple of 32),
+  // one system's, so the inner-list branch below is warp-uniform.
   for (int gs = grid_stride_start(); gs < d.n_slots; gs += grid_stride()) {
     const int a = d.order[gs];
-    if (a < 0) {
-      d.pc[gs] = make_int4(0, 0, 0, 0);
-      continue;
-    }
     const int s = d.slot_sys[gs];
     const SysDev& S = d.sys[s];
-    long long na, nb, nc;
-    if (d.rebuild_now[s]) {
-      const Folded f = fold(S, d.px[a], d.py[a], d.pz[a]);
-      na = f.na;
-      nb = f.nb;
-      nc = f.nc;
-      d.fold[gs] = int((na & 1023) | ((nb & 1023) << 10) | ((nc & 1023) << 20));
-    } else {
-      const int w = d.fold[gs];
-      na = (w << 22) >> 22;
-      nb = (w << 12) >> 22;
-      nc = (w << 2) >> 22;
+    int4 p = make_int4(0, 0, 0, 0);
+    if (a >= 0) {
+      if (d.inner && (d.rebuild_now[s] || d.prune_now[s])) {
+        d.prx[a] = d.px[a];
+        d.pry[a] = d.py[a];
+        d.prz[a] = d.pz[a];
+      }
+      long long na, nb, nc;
+      if (d.rebuild_now[s]) {
+        const Folded f = fold(S, d.px[a], d.py[a], d.pz[a]);
+        na = f.na;
+        nb = f.nb;
+        nc = f.nc;
+        d.fold[gs] = int((na & 1023) | ((nb & 1023) << 10) | ((nc & 1023) << 20));
+      } else {
+        const int w = d.fold[gs];
+        na = (w << 22) >> 22;
+        nb = (w << 12) >> 22;
+        nc = (w << 2) >> 22;
+      }
+      const long long x = d.px[a] - na * S.box_fx[0] - nb * S.box_fx[3] - nc * S.box_fx[6];
+      const long long y = d.py[a] - nb * S.box_fx[4] - nc * S.box_fx[7];
+      const long long z = d.pz[a] - nc * S.box_fx[8];
+      p = make_int4(to_pair_coordinate(x, S.pc_shift), to_pair_coordinate(y, S.pc_shift),
+                    to_pair_coordinate(z, S.pc_shift), 0);
     }
-    const long long x = d.px[a] - na * S.box_fx[0] - nb * S.box_fx[3] - nc * S.box_fx[6];
-    const long long y = d.py[a] - nb * S.box_fx[4] - nc * S.box_fx[7];
-    const long long z = d.pz[a] - nc * S.box_fx[8];
-    d.pc[gs] = make_int4(to_pair_coordinate(x, S.pc_shift), to_pair_coordinate(y, S.pc_shift),
-                         to_pair_coordinate(z, S.pc_shift), 0);
+    d.pc[gs] = p;
+    if (d.inner && (d.rebuild_now[s] || d.prune_now[s])) {
+      // the cluster's bounding box at these coordinates, for the inner prune
+      const int C = d.cluster;
+      float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
+      if (a >= 0) {
+        lo[0] = hi[0] = p.x * S.pc_inv;
+        lo[1] = hi[1] = p.y * S.pc_inv;
+        lo[2] = hi[2] = p.z * S.pc_inv;
+      }
+      for (int o = C / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o, C));
+          hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o, C));
+        }
+      if ((gs & (C - 1)) == 0) {
+        d.cb_lo[gs / C] = make_float4(lo[0], lo[1], lo[2], 0.f);
+        d.cb_hi[gs / C] = make_float4(hi[0], hi[1], hi[2], 0.f);
+      }
+    }
   }
 }
 
@@ -360,10 +393,6 @@ __device__ __forceinline__ int4 tile_image(const SysDev& S, float4 li, float4 hi
                                 (hj.z - lj.z) * (hj.z - lj.z));
   const bool per_pair = 2.f * (ei + ej) + sqrtf(S.list2) + sqrtf(S.cut2) >= S.min_width;
   return make_int4(int(sx), int(sy), int(sz), per_pair ? 1 : 0);
-}
-
-__device__ __forceinline__ bool blocks_near(const SysDev& S, const Dev& d, int I, int J) {
-  return boxes_near(S, d.bb_lo[I], d.bb_hi[I], d.bb_lo[J], d.bb_hi[J]);
 }
 
 // Position of the k-th (from 0) set bit of m, or -1.
@@ -627,6 +656,138 @@ __device__ void phase_tiles_exclusions(const Dev& d) {
   }
 }
 
+// The inner list of every system that rebuilt or is due a prune: the outer
+// tiles with an unexcluded pair closer than cutoff + inner skin (GROMACS's
+// dynamic pruning, Pall et al., J. Chem. Phys. 153, 134110 (2020), made
+// exact: a prune is due as soon as any atom has moved half the inner skin, so
+// a dropped tile has no pair inside the cutoff until the next one and the
+// pair kernel's results are bit-identical to running the whole outer list).
+// A warp takes 32 consecutive outer tiles and one atomicAdd reserves room for
+// the survivors, which keep their order.  Chunks land in any order; the pair
+// kernel's sums do not depend on it (per-tile f32 partials become int64 fixed
+// point), and a chunk spans at most two rows.
+//
+// 8x8 tiles: one lane per tile tests its pairs until the first one within
+// reach, on f32 offsets from the tile's first atom (exact integer differences,
+// then one rounding), with the J cluster in registers -- independent loads and
+// no shuffles.  32x32 tiles (too many registers for that) keep a tile if some
+// atom of I is within reach of J's current bounding box and some atom of J of
+// I's, which any pair within reach implies: conservative, one lane per atom.
+template <int C>
+__device__ bool tile_within_reach(const Dev& d, const SysDev& S, long long ti, float reach2, int lane);
+
+template <>
+__device__ bool tile_within_reach<8>(const Dev& d, const SysDev& S, long long ti, float reach2, int) {
+  const int2 tile = __ldcg(&d.tiles[ti]);
+  const int4 sh = __ldcg(&d.tile_shift[ti]);
+  if (sh.w) return true;  // per-pair images: kept as they are
+  const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
+  const float inv = S.pc_inv;
+  const int4 r0 = d.pc[tile.x * 8];
+  const unsigned ox = unsigned(r0.x) - unsigned(sh.x), oy = unsigned(r0.y) - unsigned(sh.y),
+                 oz = unsigned(r0.z) - unsigned(sh.z);
+  float jx[8], jy[8], jz[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int4 q = d.pc[tile.y * 8 + j];
+    jx[j] = int(unsigned(q.x) - ox) * inv;
+    jy[j] = int(unsigned(q.y) - oy) * inv;
+    jz[j] = int(unsigned(q.z) - oz) * inv;
+  }
+  for (int i = 0; i < 8; ++i) {
+    const unsigned int row = ((i < 4 ? w0 : w1) >> ((i & 3) * 8)) & 0xFFu;
+    if (!row) continue;
+    const int4 q = d.pc[tile.x * 8 + i];
+    const float ix = int(unsigned(q.x) - unsigned(r0.x)) * inv, iy = int(unsigned(q.y) - unsigned(r0.y)) * inv,
+                iz = int(unsigned(q.z) - unsigned(r0.z)) * inv;
+    bool hit = false;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const float dx = jx[j] - ix, dy = jy[j] - iy, dz = jz[j] - iz;
+      hit |= ((row >> j) & 1u) && dx * dx + dy * dy + dz * dz < reach2;
+    }
+    if (hit) return true;
+  }
+  return false;
+}
+
+template <>
+__device__ bool tile_within_reach<32>(const Dev& d, const SysDev& S, long long ti, float reach2, int l) {
+  const int2 tile = __ldcg(&d.tiles[ti]);
+  const int4 sh = __ldcg(&d.tile_shift[ti]);
+  const unsigned int row = __ldcg(&d.masks[ti * 32 + l]);
+  const unsigned int cols = __reduce_or_sync(0xffffffffu, row);
+  if (sh.w) return true;  // warp-uniform: one tile per warp
+  const float inv = S.pc_inv;
+  const float4 ilo = d.cb_lo[tile.x], ihi = d.cb_hi[tile.x];
+  const float4 jlo = d.cb_lo[tile.y], jhi = d.cb_hi[tile.y];
+  const float sx = sh.x * inv, sy = sh.y * inv, sz = sh.z * inv;
+  const int4 qi = d.pc[tile.x * 32 + l], qj = d.pc[tile.y * 32 + l];
+  const float ix = qi.x * inv, iy = qi.y * inv, iz = qi.z * inv;
+  const float jx = qj.x * inv + sx, jy = qj.y * inv + sy, jz = qj.z * inv + sz;
+  const float ax = fmaxf(fmaxf(jlo.x + sx - ix, ix - (jhi.x + sx)), 0.f);
+  const float ay = fmaxf(fmaxf(jlo.y + sy - iy, iy - (jhi.y + sy)), 0.f);
+  const float az = fmaxf(fmaxf(jlo.z + sz - iz, iz - (jhi.z + sz)), 0.f);
+  const float bx = fmaxf(fmaxf(ilo.x - jx, jx - ihi.x), 0.f);
+  const float by = fmaxf(fmaxf(ilo.y - jy, jy - ihi.y), 0.f);
+  const float bz = fmaxf(fmaxf(ilo.z - jz, jz - ihi.z), 0.f);
+  const bool hit_i = row != 0u && ax * ax + ay * ay + az * az < reach2;
+  const bool hit_j = ((cols >> l) & 1u) && bx * bx + by * by + bz * bz < reach2;
+  return __any_sync(0xffffffffu, hit_i) && __any_sync(0xffffffffu, hit_j);
+}
+
+template <int C>
+__device__ void phase_inner(const Dev& d) {
+  constexpr int kWords = C * C / 32;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (int s = 0; s < d.S; ++s) {
+    if (!d.rebuild_now[s] && !d.prune_now[s]) continue;
+    const SysDev& S = d.sys[s];
+    const int n = min(d.tile_count[s], S.tile_cap);
+    const float reach2 = S.inner2 * (1.0f + 1e-5f);
+    for (int c0 = warp * 32; c0 < n; c0 += warps * 32) {
+      unsigned int keep = 0u;  // bit k: outer tile c0 + k survives (the same in every lane)
+      if (C == 8) {
+        const bool alive = c0 + lane < n && tile_within_reach<C>(d, S, S.tile_off + c0 + lane, reach2, lane);
+        keep = __ballot_sync(0xffffffffu, alive);
+      } else {
+        for (int k = 0; k < 32 && c0 + k < n; ++k)
+          if (tile_within_reach<C>(d, S, S.tile_off + c0 + k, reach2, lane)) keep |= 1u << k;
+      }
+      const int count = __popc(keep);
+      int base = 0;
+      if (lane == 0 && count) base = atomicAdd(&d.in_count[s], count);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if ((keep >> lane) & 1u) {
+        const long long from = static_cast<long long>(S.tile_off) + c0 + lane;
+        const long long to = static_cast<long long>(S.tile_off) + base + __popc(keep & ((1u << lane) - 1u));
+        d.in_tiles[to] = __ldcg(&d.tiles[from]);
+        d.in_shift[to] = __ldcg(&d.tile_shift[from]);
+        if (C < 32) {
+#pragma unroll
+          for (int w = 0; w < kWords; ++w) d.in_masks[to * kWords + w] = __ldcg(&d.masks[from * kWords + w]);
+        }
+      }
+      if (C == 32) {
+        // a 32x32 tile's mask is 32 words: the warp copies each kept tile's
+        unsigned int f = keep;
+        while (f) {
+          const int k = __ffs(f) - 1;
+          f &= f - 1;
+          const long long from = static_cast<long long>(S.tile_off) + c0 + k;
+          const long long to = static_cast<long long>(S.tile_off) + base + __popc(keep & ((1u << k) - 1u));
+          d.in_masks[to * kWords + lane] = __ldcg(&d.masks[from * kWords + lane]);
+        }
+      }
+    }
+  }
+}
+
+// After the outer list: per-system offsets and rebuild counts.  Without an
+// inner list the rebuild requests are cleared here; with one, the inner-list
+// kernel that follows still needs them and clears them itself.
 __device__ void phase_tiles_finish(const Dev& d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     int total = 0;
@@ -634,11 +795,27 @@ __device__ void phase_tiles_finish(const Dev& d) {
       d.tile_prefix[s] = total;
       total += d.tile_count[s];
       if (d.rebuild_now[s]) d.rebuild_count[s] += 1;
-      d.rebuild_now[s] = 0;
+      if (!d.inner) d.rebuild_now[s] = 0;
     }
     d.tile_prefix[d.S] = total;
-    *d.any_rebuild = 0;
+    if (!d.inner) *d.any_rebuild = 0;
   }
+}
+
+// After the inner list (one thread): its offsets, the prune count, and every
+// list request cleared for the next step.
+__device__ void inner_finish(const Dev& d) {
+  int total = 0;
+  for (int s = 0; s < d.S; ++s) {
+    d.in_prefix[s] = total;
+    total += d.in_count[s];
+    if (d.prune_now[s] && !d.rebuild_now[s]) d.prune_count[s] += 1;
+    d.prune_now[s] = 0;
+    d.rebuild_now[s] = 0;
+  }
+  d.in_prefix[d.S] = total;
+  *d.any_rebuild = 0;
+  *d.any_prune = 0;
 }
 
 // Grid-wide barrier for the cooperative list kernel: arrive on a counter,
@@ -680,11 +857,11 @@ __device__ bool grid_barrier(unsigned int* bar, int* err) {
 template <int C>
 __global__ void __launch_bounds__(kThreads) k_list(Dev d) {
   const bool rebuild = *d.any_rebuild != 0;
+  int* err = d.err;  // system 0's word carries a barrier timeout
   if (!rebuild) {
     phase_wrap(d);
     return;
   }
-  int* err = d.err;  // system 0's word carries a barrier timeout
   phase_cells_clear(d);
   if (!grid_barrier(d.list_barrier, err)) return;
   phase_cells_assign(d);
@@ -735,6 +912,26 @@ MDB_PHASE_KERNEL(tiles_scan, true)
 MDB_PHASE_KERNEL(tiles_rescan, true)
 MDB_PHASE_KERNEL(tiles_finish, true)
 #undef MDB_PHASE_KERNEL
+// The inner list, its own launch after the list kernels (a full grid, where
+// the cooperative list kernel has two blocks per SM): nothing to do unless a
+// system rebuilt or is due a prune.  The last block to finish writes the
+// offsets and clears the requests; every block has read them by then, since
+// each reads them before taking its ticket.
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_inner_prune(Dev d) {
+  if (!*d.any_rebuild && !*d.any_prune) return;
+  phase_inner<C>(d);
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(d.inner_ticket, 1) == int(gridDim.x) - 1;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    inner_finish(d);
+    *d.inner_ticket = 0;
+  }
+}
 #define MDB_PHASE_KERNEL_C(name)                                   \
   template <int C>                                                 \
   __global__ void __launch_bounds__(kThreads) k_##name(Dev d) {   \
@@ -822,6 +1019,12 @@ void rebuild_tiles(const Dev& d, cudaStream_t st) {
   }
   k_tiles_exclusions<C><<<blocks_for(d.n_excl, kThreads), kThreads, 0, st>>>(d);
   k_tiles_finish<<<1, 32, 0, st>>>(d);
+}
+
+void launch_inner_prune(const Dev& d, cudaStream_t st) {
+  if (!d.inner) return;
+  if (d.cluster == 8) k_inner_prune<8><<<148 * 4, kThreads, 0, st>>>(d);
+  else k_inner_prune<32><<<148 * 4, kThreads, 0, st>>>(d);
 }
 
 void launch_rebuild_tiles(const Dev& d, cudaStream_t st) {

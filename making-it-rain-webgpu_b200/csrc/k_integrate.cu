@@ -26,7 +26,10 @@
 namespace mdb {
 namespace {
 
-constexpr int kThreads = 128;
+#ifndef MDB_INTEGRATE_THREADS
+#define MDB_INTEGRATE_THREADS 128
+#endif
+constexpr int kThreads = MDB_INTEGRATE_THREADS;
 
 struct Atom {
   long long x, y, z;  // start-of-step position (reference for the constraints)
@@ -380,14 +383,21 @@ __device__ void finish_block(const Dev& d, int s, const SysDev& S, bool advance,
   __syncthreads();
   if (last_of_launch && threadIdx.x == 0) {
     __threadfence();
-    int any = 0;
+    int any = 0, any_prune = 0;
     for (int k = 0; k < d.S; ++k) {
       const int f = __ldcg(&d.rebuild_flag[k]) | d.run.always_rebuild;
       d.rebuild_now[k] = f;
       d.rebuild_flag[k] = 0;
       any |= f;
+      if (d.inner) {
+        const int p = __ldcg(&d.prune_flag[k]);
+        d.prune_now[k] = p;
+        d.prune_flag[k] = 0;
+        any_prune |= p;
+      }
     }
     *d.any_rebuild = any;
+    if (d.inner) *d.any_prune = any_prune;
     *d.global_ticket = 0;
   }
 }
@@ -607,7 +617,7 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   // ---- atoms: velocity correction, store, rebuild test, momentum
   const float idt = 1.f / dt;
   double mom[3] = {0, 0, 0};
-  bool moved = false;
+  bool moved = false, strayed = false;
 #pragma unroll
   for (int j = 0; j < kPerThread; ++j) {
     const int e = threadIdx.x + j * kThreads;
@@ -637,8 +647,14 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
     const float ex = from_fixed(px[j] - d.refx[a]), ey = from_fixed(py[j] - d.refy[a]),
                 ez = from_fixed(pz[j] - d.refz[a]);
     moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
+    if (d.inner) {
+      const float qx = from_fixed(px[j] - d.prx[a]), qy = from_fixed(py[j] - d.pry[a]),
+                  qz = from_fixed(pz[j] - d.prz[a]);
+      strayed |= qx * qx + qy * qy + qz * qz > S.half_inner2;
+    }
   }
   if (moved) atomicOr(&d.rebuild_flag[s], 1);
+  if (strayed) atomicOr(&d.prune_flag[s], 1);
   if (bad) atomicAdd(&d.shake_failures[s], 1);
   block_sum3(mom, red);
   if (threadIdx.x == 0)

@@ -28,8 +28,12 @@ namespace {
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
 // Tiles per warp: blocks take fixed chunks of the list and retire as they
-// finish, so the PME stream's kernels can take SMs while the pair kernel runs.
-constexpr int kTilesPerWarp = 32;
+// finish, so the PME stream's kernels can take SMs while the pair kernel runs;
+// short chunks (two passes of four 8x8 tiles) balance best.
+#ifndef MDB_NB_TILES_PER_WARP
+#define MDB_NB_TILES_PER_WARP 8
+#endif
+constexpr int kTilesPerWarp = MDB_NB_TILES_PER_WARP;
 
 // erfc(x) = exp(-x^2) P(u): P fits erfcx on x in [0, 3.6] as a degree-7
 // polynomial in u = 3.111 t - 2.111, t = 1/(1 + x/2) (fit_erfcx.py in this
@@ -274,8 +278,15 @@ void launch_shape(const Dev& d, bool energy, bool triclinic, cudaStream_t st) {
 }  // namespace
 
 void launch_nonbonded(const Dev& d, bool energy, cudaStream_t st) {
-  if (d.cluster == 8) launch_shape<8>(d, energy, d.any_triclinic != 0, st);
-  else launch_shape<32>(d, energy, d.any_triclinic != 0, st);
+  Dev list = d;
+  if (d.inner) {  // the inner list has the outer list's layout: per-system regions, offsets by prefix
+    list.tiles = d.in_tiles;
+    list.masks = d.in_masks;
+    list.tile_shift = d.in_shift;
+    list.tile_prefix = d.in_prefix;
+  }
+  if (d.cluster == 8) launch_shape<8>(list, energy, d.any_triclinic != 0, st);
+  else launch_shape<32>(list, energy, d.any_triclinic != 0, st);
 }
 
 }  // namespace mdb

@@ -204,19 +204,21 @@ __device__ __forceinline__ void spline_for(const SysDev& S, long long x, long lo
 }
 
 // ---------------------------------------------------------------- spread --
-// Slots are spatially sorted, so 32 consecutive slots would send 32 atoms'
-// 125 atomics to largely the same grid points at once and serialise in L2.
-// Lane l of warp w takes slot l * W + w instead (W = slots / 32): the 32 atoms
-// of one warp instruction sit far apart on the mesh.
+// By atom, not by slot: the spread reads nothing the list kernels write, so it
+// runs on its own stream while they sort and rebuild.  Consecutive atoms are
+// neighbours in space (molecules, and solvent laid down in order), so 32 of
+// them would send their 125 atomics to largely the same grid points at once
+// and serialise in L2; lane l of warp w takes atom l * W + w instead
+// (W = ceil(atoms / 32)), and the 32 atoms of one warp instruction sit far
+// apart on the mesh.
 __global__ void __launch_bounds__(kThreads) k_spread(Dev d) {
-  const int W = d.n_slots >> 5;
-  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < d.n_slots; it += gridDim.x * blockDim.x) {
-    const int gs = (it & 31) * W + (it >> 5);
-    const int a = d.order[gs];
-    if (a < 0) continue;
-    const float q = d.prm[gs].w;
+  const int W = (d.n_atoms + 31) >> 5;
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < W * 32; it += gridDim.x * blockDim.x) {
+    const int a = (it & 31) * W + (it >> 5);
+    if (a >= d.n_atoms) continue;
+    const float q = d.prm_atom[a].w;
     if (q == 0.f) continue;
-    const SysDev& S = d.sys[d.slot_sys[gs]];
+    const SysDev& S = d.sys[d.atom_sys[a]];
     Spline sp;
     spline_for(S, d.px[a], d.py[a], d.pz[a], sp, false);
     const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
@@ -466,7 +468,7 @@ void set_pme_smem(int z, int y, int x) {
 
 void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
-  k_spread<<<grid_blocks(d.n_slots), kThreads, 0, st>>>(d);
+  k_spread<<<grid_blocks(d.n_atoms), kThreads, 0, st>>>(d);
 }
 
 void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {

@@ -115,7 +115,7 @@ class Tuning(C.Structure):
     """`mdb_tuning` (no reference counterpart)."""
 
     _fields_ = [("verlet_skin", C.c_double), ("sort_cell", C.c_double), ("tile_atoms", C.c_int32),
-                ("prune_tiles", C.c_int32)]
+                ("prune_tiles", C.c_int32), ("inner_skin", C.c_double)]
 
 
 class RunOptions(C.Structure):
@@ -207,6 +207,9 @@ class Profile(C.Structure):
         ("tiles", C.c_int64),
         ("atoms", C.c_int64),
         ("mesh_points", C.c_int64),
+        ("inner_tiles", C.c_int64),
+        ("ms_inner_prune", C.c_double),
+        ("tile_atoms", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -221,6 +224,9 @@ class NeighbourStats(C.Structure):
         ("blocks", C.c_int64),
         ("overflowed", C.c_int32),
         ("skin", C.c_double),
+        ("inner_tiles", C.c_int64),
+        ("prunes", C.c_int64),
+        ("inner_skin", C.c_double),
     ]
 
 

@@ -100,7 +100,8 @@ class RunOptions:
         if self.tuning is not None:
             arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(t[0]), float(t[1]),
                                                                int(t[2]) if len(t) > 2 else 0,
-                                                               int(t[3]) if len(t) > 3 else 0)
+                                                               int(t[3]) if len(t) > 3 else 0,
+                                                               float(t[4]) if len(t) > 4 else 0.0)
                                                     for t in self.tuning])
             o.tuning = C.cast(arr, C.POINTER(abi.Tuning))
             o._keep = arr  # the array must outlive the create call
@@ -275,7 +276,8 @@ class StepLoop:
         s = abi.NeighbourStats()
         self._check(self._lib.mdb_get_neighbour_stats(self._handle, system, C.byref(s)))
         return {"rebuilds": s.rebuilds, "tiles": s.tiles, "tileCapacity": s.tile_capacity,
-                "blocks": s.blocks, "overflowed": bool(s.overflowed), "skin": s.skin}
+                "blocks": s.blocks, "overflowed": bool(s.overflowed), "skin": s.skin,
+                "innerTiles": s.inner_tiles, "prunes": s.prunes, "innerSkin": s.inner_skin}
 
     def profile_step(self, repeats: int = 20) -> dict:
         """`StepLoop.profileStep`, loop.ts:705: device ms per stage.  Advances the system."""
@@ -331,7 +333,8 @@ def autotune(system: System, state: State, options: RunOptions | None = None, st
     if status != abi.OK:
         raise _ERRORS.get(status, EngineError)(status, lib.mdb_status_string(status).decode())
     return {"verlet_skin": best.verlet_skin, "sort_cell": best.sort_cell, "tile_atoms": best.tile_atoms,
-            "prune_tiles": best.prune_tiles, "ms_per_step": ms.value, "candidates": tried.value}
+            "prune_tiles": best.prune_tiles, "inner_skin": best.inner_skin, "ms_per_step": ms.value,
+            "candidates": tried.value}
 
 
 def size_bucket(atoms: int) -> int:
@@ -356,7 +359,7 @@ def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: 
         rep = members[len(members) // 2]
         cache[b] = autotune(systems[rep], states[rep], options, steps)
     tuning = [tuple(cache[size_bucket(s.particle_count)][k]
-                    for k in ("verlet_skin", "sort_cell", "tile_atoms", "prune_tiles"))
+                    for k in ("verlet_skin", "sort_cell", "tile_atoms", "prune_tiles", "inner_skin"))
               for s in systems]
     return tuning, cache
 

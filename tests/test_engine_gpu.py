@@ -266,13 +266,15 @@ def test_autotune_picks_a_candidate_and_tuned_batch_equals_tuned_single(mdb):
     b = synth.water_box(n_waters=900, width=3.1, seed=4, grid=(32, 32, 32))
     best = mdb.autotune(*a, steps=50)
     print("autotune", best)
-    assert best["candidates"] == 24
-    assert best["verlet_skin"] in (0.15, 0.20) and best["sort_cell"] in (0.20, 0.25, 0.35)
+    assert best["candidates"] == 32
+    assert best["verlet_skin"] in (0.15, 0.20, 0.30, 0.40, 0.50) and best["sort_cell"] in (0.20, 0.25, 0.35)
     assert best["tile_atoms"] in (8, 32) and best["prune_tiles"] in (1, 2)
-    tuning = [(best["verlet_skin"], best["sort_cell"], best["tile_atoms"], best["prune_tiles"]), (0.20, 0.35, 0, 0)]
+    assert best["inner_skin"] in (-1.0, 0.08, 0.10)
+    tuning = [(best["verlet_skin"], best["sort_cell"], best["tile_atoms"], best["prune_tiles"], best["inner_skin"]),
+              (0.20, 0.35, 0, 0)]
     single = []
     for (s, st), t in zip((a, b), tuning):
-        t = (t[0], t[1], tuning[0][2], tuning[0][3])
+        t = (t[0], t[1], tuning[0][2], tuning[0][3], t[4] if len(t) > 4 else 0.0)
         loop = mdb.StepLoop.from_parsed(s, st, mdb.RunOptions(seed=5, tuning=[t]))
         loop.run(30)
         single.append(loop.positions())
@@ -303,3 +305,22 @@ def test_every_tile_shape_and_pruning_matches_oracle(mdb, oracle, peptide, shape
         print(f"tiles {shape} prune {prune}: force rel RMS {err:.2e}, pairs {got['pairs_within_cutoff']}")
         assert err <= FORCE_REL_RMS, err
         assert got["pairs_within_cutoff"] == ref["pairs_within_cutoff"] + change
+
+
+@pytest.mark.parametrize("shape", [8, 32])
+def test_inner_list_changes_nothing(mdb, peptide, shape):
+    """An inner list re-pruned between rebuilds drops only tiles that cannot
+    reach inside the cutoff before the next prune, so the trajectory is
+    bit-identical to the one on the whole list -- with fewer tiles read."""
+    system, state = peptide
+    runs = {}
+    for inner in (-1.0, 0.06):
+        loop = make_loop(mdb, system, state, seed=9, tuning=[(0.4, 0.2, shape, 2, inner)])
+        loop.run(300)
+        runs[inner] = (loop.positions(), loop.velocities(), loop.verlet_flags())
+        loop.destroy()
+    (p0, v0, f0), (p1, v1, f1) = runs[-1.0], runs[0.06]
+    print("whole list", f0, "inner list", f1)
+    assert f1["prunes"] > 10 and f1["rebuilds"] == f0["rebuilds"]
+    assert f1["innerTiles"] < (0.8 if shape == 8 else 1.0) * f1["tiles"]
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
