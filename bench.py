@@ -46,8 +46,9 @@ NS_PER_DAY_PER_STEP_PER_S = TIME_STEP_PS * 86400 / 1000.0
 FLOP_PER_PAIR = 74.0
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate at max SM clock
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_nonbonded launch, from
-# the ncu capture summarised in profiles/nonbonded_peptide12k.md
-NB_TRAFFIC = {"peptide-12k": 4344832}
+# the ncu capture summarised in profiles/nonbonded_octahedron27k.md (captured
+# with the autotuned configuration; other workloads report null)
+NB_TRAFFIC = {"octa-27k": 11175936}
 
 
 def workload(name: str, seed: int):

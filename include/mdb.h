@@ -261,7 +261,7 @@ typedef struct mdb_profile {
   double ms_pme_fft;
   double ms_pme_gather;
   double ms_integrate;
-  int64_t pairs_within_cutoff; /* at the configuration profiled */
+  int64_t pairs_within_cutoff; /* at the configuration profiled, summed over the engine's systems */
   int64_t tiles;
   int64_t atoms;
   int64_t mesh_points;

@@ -1562,7 +1562,14 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
   mdb_energies en{};
   int status = evaluate(e, 0, nullptr, &en);
   if (status) return status;
-  out->pairs_within_cutoff = int64_t(en.pairs_within_cutoff);
+  // pairs of every system of the engine: the pair kernel's launch covers them all
+  {
+    std::vector<unsigned long long> all(size_t(d.S) * kECount);
+    cudaMemcpy(all.data(), d.energy, sizeof(unsigned long long) * all.size(), cudaMemcpyDeviceToHost);
+    int64_t pairs = 0;
+    for (int s = 0; s < d.S; ++s) pairs += static_cast<long long>(all[size_t(s) * kECount + kEPairs]);
+    out->pairs_within_cutoff = pairs;
+  }
   int tiles = 0;
   cudaMemcpy(&tiles, d.tile_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost);
   out->tiles = tiles;
