@@ -667,10 +667,11 @@ __device__ void phase_tiles_exclusions(const Dev& d) {
 // kernel's sums do not depend on it (per-tile f32 partials become int64 fixed
 // point), and a chunk spans at most two rows.
 //
-// 8x8 tiles: one lane per tile tests its pairs until the first one within
-// reach, on f32 offsets from the tile's first atom (exact integer differences,
-// then one rounding), with the J cluster in registers -- independent loads and
-// no shuffles.  32x32 tiles (too many registers for that) keep a tile if some
+// 8x8 tiles: one lane per tile; a tile whose clusters' current boxes are out
+// of reach is dropped at once, the others test their pairs until the first one
+// within reach, on f32 offsets from the tile's first atom (exact integer
+// differences, then one rounding), with the J cluster in registers --
+// independent loads and no shuffles.  32x32 tiles (too many registers for that) keep a tile if some
 // atom of I is within reach of J's current bounding box and some atom of J of
 // I's, which any pair within reach implies: conservative, one lane per atom.
 template <int C>
@@ -681,8 +682,19 @@ __device__ bool tile_within_reach<8>(const Dev& d, const SysDev& S, long long ti
   const int2 tile = __ldcg(&d.tiles[ti]);
   const int4 sh = __ldcg(&d.tile_shift[ti]);
   if (sh.w) return true;  // per-pair images: kept as they are
-  const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
   const float inv = S.pc_inv;
+  {
+    // the clusters' current boxes first: most outer tiles of a long skin are
+    // out of reach box to box and need no pair loop (the margin covers the
+    // boxes' f32 rounding)
+    const float4 ilo = d.cb_lo[tile.x], ihi = d.cb_hi[tile.x], jlo = d.cb_lo[tile.y], jhi = d.cb_hi[tile.y];
+    const float sx = sh.x * inv, sy = sh.y * inv, sz = sh.z * inv;
+    const float gx = fmaxf(fmaxf(jlo.x + sx - ihi.x, ilo.x - (jhi.x + sx)), 0.f);
+    const float gy = fmaxf(fmaxf(jlo.y + sy - ihi.y, ilo.y - (jhi.y + sy)), 0.f);
+    const float gz = fmaxf(fmaxf(jlo.z + sz - ihi.z, ilo.z - (jhi.z + sz)), 0.f);
+    if (gx * gx + gy * gy + gz * gz >= reach2 * (1.0f + 4e-5f)) return false;
+  }
+  const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
   const int4 r0 = d.pc[tile.x * 8];
   const unsigned ox = unsigned(r0.x) - unsigned(sh.x), oy = unsigned(r0.y) - unsigned(sh.y),
                  oz = unsigned(r0.z) - unsigned(sh.z);

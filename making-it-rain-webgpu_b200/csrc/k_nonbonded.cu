@@ -68,6 +68,9 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
 
 // `per_pair`: take the minimum image of every pair; otherwise pj already
 // carries the tile's lattice shift and the plain difference is the separation.
+// `mask` arrives rotated: bit k is the pair of step k (j = l + k mod C).  Every
+// tile runs this same code whatever its neighbours in the warp, so a tile's
+// result does not depend on where in the list it sits.
 template <int C, bool ENERGY, bool TRICLINIC>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
                                            unsigned int mask, bool per_pair, int l, float& fix, float& fiy,
@@ -76,15 +79,15 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
                                            int& pairs, float* vir) {
   const float alpha = S.alpha, a2sp = S.alpha_2_sqrtpi, cut2 = S.cut2, inv = S.pc_inv;
   const int src = (l + 1) & (C - 1);
-#pragma unroll 4
+  constexpr int kUnroll = C == 8 ? 8 : 4;
+#pragma unroll kUnroll
   for (int k = 0; k < C; ++k) {
-    const int jl = (l + k) & (C - 1);
     int dx = int(unsigned(pj.x) - unsigned(pi.x)), dy = int(unsigned(pj.y) - unsigned(pi.y)),
         dz = int(unsigned(pj.z) - unsigned(pi.z));
     if (per_pair) min_image<TRICLINIC>(S, dx, dy, dz);
     const float rx = dx * inv, ry = dy * inv, rz = dz * inv;
     const float r2 = rx * rx + ry * ry + rz * rz;
-    if (((mask >> jl) & 1u) && r2 < cut2) {
+    if (((mask >> k) & 1u) && r2 < cut2) {
       const float rinv = rsqrtf(r2);
       const float rinv2 = rinv * rinv;
       const float r = r2 * rinv;
@@ -232,6 +235,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
       float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, ec = 0.f, el = 0.f;
       float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       int np = 0;
+      mask = C == 32 ? __funnelshift_r(mask, mask, l) : ((mask >> l) | (mask << ((C - l) & (C - 1)))) & 0xFFu;
       tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy, fjz, ec,
                                        el, np, vir);
       if (!active) continue;
