@@ -1610,10 +1610,19 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
   out->ms_pme_fft = time([&] { launch_pme_fft(d, false, st); });
   out->ms_pme_gather = time([&] { launch_pme_gather(d, st); });
   out->ms_pme = time([&] { launch_pme(d, false, st); });
+  // the timings above piled up forces; the integrator is timed on cleared ones,
+  // so its constraint solves see an ordinary step
+  CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, st));
+  CUDA_TRY(e, cudaMemsetAsync(d.fy, 0, sizeof(long long) * d.n_slots, st));
+  CUDA_TRY(e, cudaMemsetAsync(d.fz, 0, sizeof(long long) * d.n_slots, st));
   out->ms_integrate = time([&] { launch_integrate(d, st); });
-  // 5 sort + 1 wrap + 6 tile-list kernels, 7 PME, listed, nonbonded, integrator
-  out->launches_per_step = 5 + 1 + 6 + (d.n_fft_z ? 7 : 0) + (d.n_bonds + d.n_angles + d.n_torsions +
-                                                              d.n_exceptions + d.n_restraints > 0 ? 1 : 0) + 1 + 1;
+  // per step: the list kernels (one cooperative launch, or 5 sort + 1 wrap +
+  // 6 tile-list kernels, 3 more when rebuilds prune), the inner-list kernel,
+  // 7 PME, listed, nonbonded, integrator
+  out->launches_per_step = (e->coop_list ? 1 : 5 + 1 + 6 + (d.prune ? 3 : 0)) + (d.inner ? 1 : 0) +
+                           (d.n_fft_z ? 7 : 0) +
+                           (d.n_bonds + d.n_angles + d.n_torsions + d.n_exceptions + d.n_restraints > 0 ? 1 : 0) +
+                           1 + 1;
   CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, st));
   CUDA_TRY(e, cudaMemsetAsync(d.fy, 0, sizeof(long long) * d.n_slots, st));
   CUDA_TRY(e, cudaMemsetAsync(d.fz, 0, sizeof(long long) * d.n_slots, st));

@@ -253,6 +253,38 @@ class StepLoop:
         self._check(self._lib.mdb_potential(self._handle, system, self._dp(p), self._dp(f), C.byref(e)))
         return e.potential, f.reshape(-1, 3)
 
+    @property
+    def options(self) -> RunOptions:
+        return self._options
+
+    def set_velocities_to_temperature(self, temperature: float, seed: int, system: int = 0) -> np.ndarray:
+        """`Context.setVelocitiesToTemperature` as src/reference/velocities.ts:78
+        restates it: a Maxwell-Boltzmann draw from the velocity domain of the
+        counter-based generator, shifted by -(dt/2) F/m (the velocity time
+        offset of both integrators) with the forces from the device, projected
+        onto the constraints at 1e-5.  Sets and returns the velocities."""
+        from .velocities import velocities_at_temperature
+
+        _, forces = self.evaluate(system)
+        v = velocities_at_temperature(self._systems[system], self.positions(system), temperature, seed,
+                                      0.5 * self._options.time_step, forces)
+        self.set_velocities(v, system)
+        return v
+
+    def minimise(self, tolerance: float = 10.0, max_iterations: int = 0, system: int = 0):
+        """`minimiseOnDevice`, src/gpu/minimise.ts:33: OpenMM's minimisation of
+        this system's current configuration with the device's forces (one
+        `potential` call per evaluation); the result is left in place and the
+        `MinimiseResult` returned."""
+        from .minimise import minimise
+
+        result = minimise(self._systems[system], self.positions(system), lambda p: self.potential(p, system),
+                          tolerance=tolerance, max_iterations=max_iterations,
+                          constraint_tolerance=self._options.constraint_tolerance)
+        # the last evaluation was the line search's last trial, not necessarily the result
+        self.set_positions(result.positions, system)
+        return result
+
     def report(self, system: int = 0) -> Report:
         """`StepLoop.report()`, loop.ts:761."""
         energies, _ = self.evaluate(system)
