@@ -127,6 +127,8 @@ struct Dev {
   const FftWork* fft_z; int n_fft_z;
   const FftWork* fft_y; int n_fft_y;
   const FftWork* fft_x; int n_fft_x;
+  const FftWork* fft_p; int n_fft_p;  // whole x-planes (sys, x): the fused z+y passes, when they fit
+  int fft_planes;                     // 1: the plane kernels replace the separate z and y passes
 
   // energies, int64 2^32 fixed, [S][kECount]
   unsigned long long* energy;

@@ -34,7 +34,7 @@
 #include "prep.h"
 
 namespace mdb {
-void set_pme_smem(int z, int y, int x);
+void set_pme_smem(int z, int y, int x, int plane);
 }
 
 using namespace mdb;
@@ -48,6 +48,7 @@ constexpr double kDefaultInnerSkin = -1.0;  // nm; <= 0: no inner list unless a 
 // row at a 0.2 nm skin in water (~120 tiles for 8-atom clusters, ~90 for 32).
 int row_cap_for(int cluster) { return cluster == 8 ? 384 : 192; }
 constexpr int kFftTile = 8;  // kz columns per y- and x-pass CTA
+constexpr int kPlaneSmemLimit = 200 * 1024;  // bytes: two complex Ky x Kz planes per CTA
 
 struct Allocation {
   std::string label;
@@ -390,7 +391,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   std::vector<int> iblk_sys, iblk_unit0, iblk_nunit, iblk_atom0, iblk_natom, iatom;
   int atoms = 0, slots = 0, blocks = 0, cells = 0, tiles = 0, units_n = 0, iblk = 0;
   long long grid_pts = 0, cgrid_pts = 0;
-  int smem_z = 0, smem_y = 0, smem_x = 0;
+  int smem_z = 0, smem_y = 0, smem_x = 0, smem_p = 0;
+  std::vector<FftWork> wp;
   const float sq = float(std::sqrt(kOne4PiEps0));
   for (int s = 0; s < n; ++s) {
     HostSystem& h = e->hs[s];
@@ -462,6 +464,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
         e->fft_x_sys.push_back(s);
       }
     smem_x = std::max(smem_x, 2 * kFftTile * Kx * int(sizeof(float2)));
+    for (int x = 0; x < Kx; ++x) wp.push_back({s, x, 0, 1});
+    smem_p = std::max(smem_p, 2 * Ky * Kz * int(sizeof(float2)));
 
     // atoms
     const double* pos = states[s].positions;
@@ -747,6 +751,10 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.fft_y = w_dev; d.n_fft_y = int(wy.size());
   TRY(upload(e, "fft x work", w_dev, wx));
   d.fft_x = w_dev; d.n_fft_x = int(wx.size());
+  TRY(upload(e, "fft plane work", w_dev, wp));
+  d.fft_p = w_dev; d.n_fft_p = int(wp.size());
+  // a whole x-plane in shared memory, twice, when every system's fits
+  d.fft_planes = smem_p <= kPlaneSmemLimit ? 1 : 0;
   e->n_mesh_items = int(wx.size());
   TRY(alloc(e, "energies", d.energy, size_t(n) * kECount));
   {
@@ -796,7 +804,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "constraint failures", d.shake_failures, n));
 #undef TRY
   e->step = states[0].step;
-  set_pme_smem(smem_z, smem_y, smem_x);
+  set_pme_smem(smem_z, smem_y, smem_x, d.fft_planes ? smem_p : 0);
 
   // PME and the listed terms run beside the pair kernel at the highest
   // priority: their small, latency-bound grids take SMs as pair blocks retire

@@ -375,6 +375,74 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   }
 }
 
+// ------------------------------------------------- whole x-plane passes ---
+// With the plane in shared memory one CTA does both the z and the y
+// transforms of an x-plane (Ky x Kz grid points; 2 x 16 Ky Kz bytes), so a
+// forward or inverse transform is three launches instead of five and the
+// launches that remain have a plane of work each.
+constexpr int kPlaneThreads = 512;
+
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
+  extern __shared__ float2 smem[];
+  const FftWork w = d.fft_p[blockIdx.x];
+  const SysDev& S = d.sys[w.sys];
+  const int Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  float2* A = smem;
+  float2* B = smem + Ky * Kz;
+  unsigned long long* grid = d.qgrid + S.grid_off + static_cast<long long>(w.a) * Ky * Kz;
+  for (int i = threadIdx.x; i < Ky * Kz; i += blockDim.x) {
+    A[i] = make_float2(from_fixed(static_cast<long long>(grid[i])), 0.f);
+    grid[i] = 0ull;  // consumer clears: the next spread starts from zero
+  }
+  __syncthreads();
+  float2* R = fft_lines(A, B, Kz, Ky, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], -1);
+  float2* T = R == A ? B : A;
+  // the half spectrum's kz columns become y-lines
+  for (int i = threadIdx.x; i < kzh * Ky; i += blockDim.x) {
+    const int k = i / Ky, y = i - k * Ky;
+    T[k * Ky + y] = R[y * Kz + k];
+  }
+  __syncthreads();
+  const float2* Y = fft_lines(T, R, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], -1);
+  float2* out = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
+  for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
+    const int y = i / kzh, k = i - y * kzh;
+    out[i] = Y[k * Ky + y];
+  }
+}
+
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
+  extern __shared__ float2 smem[];
+  const FftWork w = d.fft_p[blockIdx.x];
+  const SysDev& S = d.sys[w.sys];
+  const int Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  float2* A = smem;
+  float2* B = smem + Ky * Kz;
+  const float2* in = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
+  for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
+    const int y = i / kzh, k = i - y * kzh;
+    A[k * Ky + y] = in[i];
+  }
+  __syncthreads();
+  float2* Y = fft_lines(A, B, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], +1);
+  float2* Z = Y == A ? B : A;
+  for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
+    const int y = i / kzh, k = i - y * kzh;
+    Z[y * Kz + k] = Y[k * Ky + y];
+  }
+  __syncthreads();
+  // the rest of each z-line from Hermitian symmetry (the result is real)
+  for (int i = threadIdx.x; i < Ky * (Kz - kzh); i += blockDim.x) {
+    const int y = i / (Kz - kzh), k = kzh + (i - y * (Kz - kzh));
+    const float2 c = Z[y * Kz + (Kz - k)];
+    Z[y * Kz + k] = make_float2(c.x, -c.y);
+  }
+  __syncthreads();
+  const float2* R = fft_lines(Z, Y, Kz, Ky, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], +1);
+  float* out = d.phi + S.grid_off + static_cast<long long>(w.a) * Ky * Kz;
+  for (int i = threadIdx.x; i < Ky * Kz; i += blockDim.x) out[i] = R[i].x;
+}
+
 // ---------------------------------------------------------- z inverse ----
 // complex half spectrum -> real potential grid along z.
 __global__ void __launch_bounds__(kThreads) k_fft_z_inverse(Dev d) {
@@ -455,10 +523,14 @@ int grid_blocks(int n) {
 }  // namespace
 
 // Shared-memory bytes for the largest work item of each pass, set by the host.
-struct PmeSmem { int z, y, x; };
-static PmeSmem g_smem{0, 0, 0};
-void set_pme_smem(int z, int y, int x) {
-  g_smem = {z, y, x};
+struct PmeSmem { int z, y, x, p; };
+static PmeSmem g_smem{0, 0, 0, 0};
+void set_pme_smem(int z, int y, int x, int plane) {
+  g_smem = {z, y, x, plane};
+  if (plane > 0) {
+    cudaFuncSetAttribute(k_fft_zy_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, plane);
+    cudaFuncSetAttribute(k_fft_yz_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, plane);
+  }
   cudaFuncSetAttribute(k_fft_z_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, z);
   cudaFuncSetAttribute(k_fft_z_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, z);
   cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, y);
@@ -473,12 +545,18 @@ void launch_pme_spread(const Dev& d, cudaStream_t st) {
 
 void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
-  k_fft_z_forward<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
-  k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, -1);
+  if (d.fft_planes) k_fft_zy_forward<<<d.n_fft_p, kPlaneThreads, g_smem.p, st>>>(d);
+  else {
+    k_fft_z_forward<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+    k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, -1);
+  }
   if (energy) k_fft_x_convolve<true><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
   else k_fft_x_convolve<false><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
-  k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, +1);
-  k_fft_z_inverse<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+  if (d.fft_planes) k_fft_yz_inverse<<<d.n_fft_p, kPlaneThreads, g_smem.p, st>>>(d);
+  else {
+    k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, +1);
+    k_fft_z_inverse<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+  }
 }
 
 void launch_pme_gather(const Dev& d, cudaStream_t st) {
