@@ -48,6 +48,9 @@ constexpr double kDefaultInnerSkin = -1.0;  // nm; <= 0: no inner list unless a 
 // row at a 0.2 nm skin in water (~120 tiles for 8-atom clusters, ~90 for 32).
 int row_cap_for(int cluster) { return cluster == 8 ? 384 : 192; }
 constexpr int kFftTile = 8;  // kz columns per y- and x-pass CTA
+// the exact stage switches the screening network off once its running RMS
+// error exceeds this many kT (the plain barostat takes over)
+constexpr double kSurrogateMaxRmsKT = 1.5;
 constexpr int kPlaneSmemLimit = 200 * 1024;  // bytes: two complex Ky x Kz planes per CTA
 
 struct Allocation {
@@ -63,6 +66,7 @@ struct Surrogate {
   bool disabled = false;          // the exact stage judged it too inaccurate: plain barostat
   std::vector<float> feats;       // raw features of every exact attempt, kMlpIn each
   std::vector<double> delta_u;    // exact change minus its first-order term, per atom, kJ/mol
+  std::vector<double> dlnv;       // the move of each attempt
   double mu[kMlpIn] = {}, sd[kMlpIn] = {}, mu_t = 0, sd_t = 1;
   double err2 = 0;                // running mean square of (predicted - exact) change
   int64_t judged = 0;
@@ -1018,9 +1022,12 @@ int set_box(mdb_engine* e, int s, const double* box) {
 // ---- the barostat's screening network (no reference counterpart) ----------
 // Inputs: dlnV, the energy components and the molecular virial's diagonal per
 // atom, the box diagonal, and the first-order change -tr(W_mol) dlnV / 3 per
-// atom.  The network learns what the first-order term misses: its target is
-// (dU - first order) per atom, so its error stays on the kT scale however
-// large the system (the first-order term itself grows with it).
+// atom.  The network learns what the first-order term misses, which is second
+// order in the move: its target is (dU - first order) / (atoms x dlnV^2), a
+// smooth function of the state (the compressibility term) whose error stays on
+// the kT scale however large the system, and which carries over to moves of
+// another size -- the barostat rescales its moves as it runs, and a target
+// learnt in plain (dU - first order) would have to be extrapolated in dlnV.
 double first_order_change(const mdb_energies& en, double dlnv) {
   return -(en.molecular_virial[0] + en.molecular_virial[4] + en.molecular_virial[8]) * dlnv / 3.0;
 }
@@ -1069,23 +1076,35 @@ int surrogate_alloc(mdb_engine* e, Surrogate& net, int samples) {
 }
 
 // Standardise the collected attempts, then train on the device from a seeded
-// start (mlp_train).
+// start (mlp_train).  Attempts whose move is under a tenth of the largest are
+// left out: dividing by dlnV^2 would turn their energy noise into large targets.
 int surrogate_train(mdb_engine* e, Surrogate& net, uint32_t seed, int epochs) {
-  const int n = int(net.delta_u.size());
+  double largest = 0;
+  for (double v : net.dlnv) largest = std::max(largest, std::fabs(v));
+  std::vector<int> use;
+  for (int i = 0; i < int(net.dlnv.size()); ++i)
+    if (std::fabs(net.dlnv[i]) >= 0.1 * largest && net.dlnv[i] != 0) use.push_back(i);
+  const int n = int(use.size());
   if (n < kMlpBatch) return MDB_OK;
+  std::vector<double> feats(size_t(n) * kMlpIn), target(n);
+  for (int i = 0; i < n; ++i) {
+    const int j = use[i];
+    for (int k = 0; k < kMlpIn; ++k) feats[size_t(i) * kMlpIn + k] = net.feats[size_t(j) * kMlpIn + k];
+    target[i] = net.delta_u[j] / (net.dlnv[j] * net.dlnv[j]);
+  }
   for (int k = 0; k < kMlpIn; ++k) {
     double m = 0, v = 0;
-    for (int i = 0; i < n; ++i) m += net.feats[size_t(i) * kMlpIn + k];
+    for (int i = 0; i < n; ++i) m += feats[size_t(i) * kMlpIn + k];
     m /= n;
-    for (int i = 0; i < n; ++i) v += (net.feats[size_t(i) * kMlpIn + k] - m) * (net.feats[size_t(i) * kMlpIn + k] - m);
+    for (int i = 0; i < n; ++i) v += (feats[size_t(i) * kMlpIn + k] - m) * (feats[size_t(i) * kMlpIn + k] - m);
     net.mu[k] = m;
     net.sd[k] = std::sqrt(v / n) > 1e-12 ? std::sqrt(v / n) : 1.0;
   }
   {
     double m = 0, v = 0;
-    for (double t : net.delta_u) m += t;
+    for (double t : target) m += t;
     m /= n;
-    for (double t : net.delta_u) v += (t - m) * (t - m);
+    for (double t : target) v += (t - m) * (t - m);
     net.mu_t = m;
     net.sd_t = std::sqrt(v / n) > 1e-12 ? std::sqrt(v / n) : 1.0;
   }
@@ -1094,8 +1113,8 @@ int surrogate_train(mdb_engine* e, Surrogate& net, uint32_t seed, int epochs) {
   std::vector<float> x(size_t(n) * kMlpIn), t(n);
   for (int i = 0; i < n; ++i) {
     for (int k = 0; k < kMlpIn; ++k)
-      x[size_t(i) * kMlpIn + k] = float((net.feats[size_t(i) * kMlpIn + k] - net.mu[k]) / net.sd[k]);
-    t[i] = float((net.delta_u[i] - net.mu_t) / net.sd_t);
+      x[size_t(i) * kMlpIn + k] = float((feats[size_t(i) * kMlpIn + k] - net.mu[k]) / net.sd[k]);
+    t[i] = float((target[i] - net.mu_t) / net.sd_t);
   }
   CUDA_TRY(e, cudaMemcpy(net.x, x.data(), sizeof(float) * x.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(e, cudaMemcpy(net.t, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
@@ -1123,7 +1142,7 @@ int surrogate_predict(mdb_engine* e, Surrogate& net, const HostSystem& h, const 
   float y = 0;
   CUDA_TRY(e, cudaMemcpyAsync(&y, net.y, sizeof(float), cudaMemcpyDeviceToHost, e->s0));
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  *out = first_order_change(en, dlnv) + (double(y) * net.sd_t + net.mu_t) * std::max(1, h.n);
+  *out = first_order_change(en, dlnv) + (double(y) * net.sd_t + net.mu_t) * std::max(1, h.n) * dlnv * dlnv;
   return MDB_OK;
 }
 
@@ -1210,7 +1229,7 @@ int barostat_attempt(mdb_engine* e, int s) {
       // the exact stage judges the network
       const double err = du_pred - du;
       net.err2 = net.judged == 0 ? err * err : 0.98 * net.err2 + 0.02 * err * err;
-      if (++net.judged >= 50 && std::sqrt(net.err2) > 3.0 * kT) net.disabled = true;
+      if (++net.judged >= 50 && std::sqrt(net.err2) > kSurrogateMaxRmsKT * kT) net.disabled = true;
     } else {
       accepted = !(w > 0 && uniform() > std::exp(-w / kT));
       if (net.target > 0 && !net.active) {
@@ -1219,6 +1238,7 @@ int barostat_attempt(mdb_engine* e, int s) {
         for (double v : f) net.feats.push_back(float(v));
         // what the first-order term misses, per atom like the energy features
         net.delta_u.push_back((du - first_order_change(e0, dlnv)) / std::max(1, h.n));
+        net.dlnv.push_back(dlnv);
         if (int(net.delta_u.size()) >= net.target) {
           if ((st = surrogate_train(e, net, e->opt.seed, 300))) return st;
         }

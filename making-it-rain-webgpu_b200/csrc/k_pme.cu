@@ -205,41 +205,71 @@ __device__ __forceinline__ void spline_for(const SysDev& S, long long x, long lo
 
 // ---------------------------------------------------------------- spread --
 // By atom, not by slot: the spread reads nothing the list kernels write, so it
-// runs on its own stream while they sort and rebuild.  Consecutive atoms are
-// neighbours in space (molecules, and solvent laid down in order), so 32 of
-// them would send their 125 atomics to largely the same grid points at once
-// and serialise in L2; lane l of warp w takes atom l * W + w instead
-// (W = ceil(atoms / 32)), and the 32 atoms of one warp instruction sit far
-// apart on the mesh.
+// runs on its own stream while they sort and rebuild.  A block takes
+// kSplineAtoms atoms: their splines are computed once each into shared memory,
+// then all its threads share the 25 (ix, iy) rows of 5 z points per atom, so
+// no thread makes more than a few atomics in a row (one thread per atom making
+// all 125 left the kernel latency-bound at any size).  Consecutive atoms are
+// neighbours in space (molecules, solvent laid down in order), so block b
+// takes atoms b, b + B, b + 2B, ... (B blocks): atoms spread at once sit far
+// apart on the mesh.  The grid is int64 fixed point: the order of the atomics
+// does not change the sums.
+#ifndef MDB_SPREAD_ATOMS
+#define MDB_SPREAD_ATOMS 128
+#endif
+constexpr int kSplineAtoms = MDB_SPREAD_ATOMS;
+static_assert(kSplineAtoms <= kThreads, "one thread per atom computes the splines");
+
+struct SplineTable {
+  int base[kSplineAtoms][3];
+  float th[kSplineAtoms][3][5];
+  float q[kSplineAtoms];
+  int sys[kSplineAtoms];
+};
+
 __global__ void __launch_bounds__(kThreads) k_spread(Dev d) {
-  const int W = (d.n_atoms + 31) >> 5;
-  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < W * 32; it += gridDim.x * blockDim.x) {
-    const int a = (it & 31) * W + (it >> 5);
-    if (a >= d.n_atoms) continue;
-    const float q = d.prm_atom[a].w;
-    if (q == 0.f) continue;
-    const SysDev& S = d.sys[d.atom_sys[a]];
-    Spline sp;
-    spline_for(S, d.px[a], d.py[a], d.pz[a], sp, false);
-    const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
-    unsigned long long* grid = d.qgrid + S.grid_off;
-    for (int ix = 0; ix < kPmeOrder; ++ix) {
-      int gx = sp.base[0] + ix;
-      if (gx >= Kx) gx -= Kx;
-      const float wx = q * sp.th[0][ix];
-      for (int iy = 0; iy < kPmeOrder; ++iy) {
-        int gy = sp.base[1] + iy;
-        if (gy >= Ky) gy -= Ky;
-        const float wxy = wx * sp.th[1][iy];
-        unsigned long long* row = grid + (static_cast<long long>(gx) * Ky + gy) * Kz;
-#pragma unroll
-        for (int iz = 0; iz < kPmeOrder; ++iz) {
-          int gz = sp.base[2] + iz;
-          if (gz >= Kz) gz -= Kz;
-          add_fixed(&row[gz], wxy * sp.th[2][iz]);
+  __shared__ SplineTable t;
+  const int nblocks = gridDim.x;
+  for (int first = blockIdx.x; first < d.n_atoms; first += nblocks * kSplineAtoms) {
+    // atom k of this round is first + k * nblocks
+    if (threadIdx.x < kSplineAtoms) {
+      const int k = threadIdx.x, a = first + k * nblocks;
+      float q = 0.f;
+      if (a < d.n_atoms) q = d.prm_atom[a].w;
+      t.q[k] = q;
+      if (q != 0.f) {
+        const int s = d.atom_sys[a];
+        Spline sp;
+        spline_for(d.sys[s], d.px[a], d.py[a], d.pz[a], sp, false);
+        t.sys[k] = s;
+        for (int ax = 0; ax < 3; ++ax) {
+          t.base[k][ax] = sp.base[ax];
+          for (int i = 0; i < kPmeOrder; ++i) t.th[k][ax][i] = sp.th[ax][i];
         }
       }
     }
+    __syncthreads();
+    for (int w = threadIdx.x; w < kSplineAtoms * kPmeOrder * kPmeOrder; w += blockDim.x) {
+      const int k = w / (kPmeOrder * kPmeOrder), r = w - k * kPmeOrder * kPmeOrder;
+      const float q = t.q[k];
+      if (q == 0.f) continue;
+      const SysDev& S = d.sys[t.sys[k]];
+      const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2];
+      const int ix = r / kPmeOrder, iy = r - ix * kPmeOrder;
+      int gx = t.base[k][0] + ix;
+      if (gx >= Kx) gx -= Kx;
+      int gy = t.base[k][1] + iy;
+      if (gy >= Ky) gy -= Ky;
+      const float wxy = q * t.th[k][0][ix] * t.th[k][1][iy];
+      unsigned long long* row = d.qgrid + S.grid_off + (static_cast<long long>(gx) * Ky + gy) * Kz;
+#pragma unroll
+      for (int iz = 0; iz < kPmeOrder; ++iz) {
+        int gz = t.base[k][2] + iz;
+        if (gz >= Kz) gz -= Kz;
+        add_fixed(&row[gz], wxy * t.th[k][2][iz]);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -540,7 +570,7 @@ void set_pme_smem(int z, int y, int x, int plane) {
 
 void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
-  k_spread<<<grid_blocks(d.n_atoms), kThreads, 0, st>>>(d);
+  k_spread<<<std::max(1, std::min((d.n_atoms + kSplineAtoms - 1) / kSplineAtoms, 148 * 8)), kThreads, 0, st>>>(d);
 }
 
 void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {

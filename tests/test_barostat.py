@@ -110,7 +110,8 @@ def test_delayed_acceptance_saves_exact_evaluations():
     """The same NPT water box with the plain barostat and with the screening
     network trained on its first 300 exact attempts: the network must reject
     some proposals on its own (fewer exact evaluations per attempt), stay
-    within 3 kT RMS of the exact change, and sample the same volume."""
+    within 1.5 kT RMS of the exact change (the limit above which the exact
+    stage switches it off), and sample the same volume."""
     import time
 
     from mdb200 import steploop, synth
@@ -138,7 +139,7 @@ def test_delayed_acceptance_saves_exact_evaluations():
     assert s["surrogateActive"] and s["trainingSamples"] == 300
     assert s["screened"] > 0
     assert s["exact_per_attempt"] < 0.9 * p["exact_per_attempt"]
-    assert s["surrogateRms"] < 3 * KB * 300.0
+    assert s["surrogateRms"] < 1.5 * KB * 300.0
     assert abs(s["volume"] - p["volume"]) < 0.03 * p["volume"]
 
 
