@@ -98,25 +98,31 @@ __device__ __forceinline__ void small_dft(float2* v, int sign) {
   }
 }
 
+// Quotient by a per-stage divisor d > 1 without a division: magic = 2^32 / d
+// rounded up is exact for numerator x divisor < 2^32 (all FFT indices here
+// are below 2^16).  d = 1 (magic 0) means the numerator itself.
+__device__ __forceinline__ unsigned quotient(unsigned x, unsigned magic) { return magic ? __umulhi(x, magic) : x; }
+__host__ __device__ __forceinline__ unsigned magic_for(unsigned d) { return d > 1 ? 0xFFFFFFFFu / d + 1u : 0u; }
+
 template <int R>
 __device__ __forceinline__ void stage_butterfly(const float2* src, float2* dst, int n, int j, int ns,
-                                                const float2* tw, int sign) {
+                                                unsigned ns_magic, int step, const float2* tw, int sign) {
   const int bf = n / R;
-  const int k = j % ns;
-  const int step = n / (ns * R);
+  const int jq = int(quotient(unsigned(j), ns_magic));
+  const int k = j - jq * ns;
   float2 v[R];
 #pragma unroll
   for (int q = 0; q < R; ++q) {
     float2 x = src[j + q * bf];
     if (q > 0 && k > 0) {
-      float2 w = tw[(k * q * step) % n];
+      float2 w = tw[k * q * step];  // k q step < ns R step = n
       if (sign > 0) w.y = -w.y;
       x = cmul(x, w);
     }
     v[q] = x;
   }
   small_dft<R>(v, sign);
-  const int dest = (j / ns) * ns * R + k;
+  const int dest = jq * ns * R + k;
 #pragma unroll
   for (int q = 0; q < R; ++q) dst[dest + q * ns] = v[q];
 }
@@ -130,16 +136,18 @@ __device__ float2* fft_lines(float2* a, float2* b, int n, int nl, const int* rad
   for (int st = 0; st < nrad; ++st) {
     const int r = radices[st];
     const int bf = n / r;
+    const int step = n / (ns * r);
+    const unsigned bf_magic = magic_for(unsigned(bf)), ns_magic = magic_for(unsigned(ns));
     for (int idx = threadIdx.x; idx < nl * bf; idx += blockDim.x) {
-      const int line = idx / bf, j = idx - line * bf;
+      const int line = int(quotient(unsigned(idx), bf_magic)), j = idx - line * bf;
       const float2* src = a + line * n;
       float2* dst = b + line * n;
       switch (r) {
-        case 2: stage_butterfly<2>(src, dst, n, j, ns, tw, sign); break;
-        case 3: stage_butterfly<3>(src, dst, n, j, ns, tw, sign); break;
-        case 4: stage_butterfly<4>(src, dst, n, j, ns, tw, sign); break;
-        case 5: stage_butterfly<5>(src, dst, n, j, ns, tw, sign); break;
-        default: stage_butterfly<7>(src, dst, n, j, ns, tw, sign); break;
+        case 2: stage_butterfly<2>(src, dst, n, j, ns, ns_magic, step, tw, sign); break;
+        case 3: stage_butterfly<3>(src, dst, n, j, ns, ns_magic, step, tw, sign); break;
+        case 4: stage_butterfly<4>(src, dst, n, j, ns, ns_magic, step, tw, sign); break;
+        case 5: stage_butterfly<5>(src, dst, n, j, ns, ns_magic, step, tw, sign); break;
+        default: stage_butterfly<7>(src, dst, n, j, ns, ns_magic, step, tw, sign); break;
       }
     }
     __syncthreads();
@@ -205,7 +213,7 @@ __device__ __forceinline__ void spline_for(const SysDev& S, long long x, long lo
 
 // ---------------------------------------------------------------- spread --
 // By atom, not by slot: the spread reads nothing the list kernels write, so it
-// runs on its own stream while they sort and rebuild.  A block takes
+// runs on its own stream while they sort and rebuild.  A block takes up to
 // kSplineAtoms atoms: their splines are computed once each into shared memory,
 // then all its threads share the 25 (ix, iy) rows of 5 z points per atom, so
 // no thread makes more than a few atomics in a row (one thread per atom making
@@ -227,12 +235,12 @@ struct SplineTable {
   int sys[kSplineAtoms];
 };
 
-__global__ void __launch_bounds__(kThreads) k_spread(Dev d) {
+__global__ void __launch_bounds__(kThreads) k_spread(Dev d, int per) {
   __shared__ SplineTable t;
   const int nblocks = gridDim.x;
-  for (int first = blockIdx.x; first < d.n_atoms; first += nblocks * kSplineAtoms) {
-    // atom k of this round is first + k * nblocks
-    if (threadIdx.x < kSplineAtoms) {
+  for (int first = blockIdx.x; first < d.n_atoms; first += nblocks * per) {
+    // atom k (< per <= kSplineAtoms) of this round is first + k * nblocks
+    if (threadIdx.x < per) {
       const int k = threadIdx.x, a = first + k * nblocks;
       float q = 0.f;
       if (a < d.n_atoms) q = d.prm_atom[a].w;
@@ -249,7 +257,7 @@ __global__ void __launch_bounds__(kThreads) k_spread(Dev d) {
       }
     }
     __syncthreads();
-    for (int w = threadIdx.x; w < kSplineAtoms * kPmeOrder * kPmeOrder; w += blockDim.x) {
+    for (int w = threadIdx.x; w < per * kPmeOrder * kPmeOrder; w += blockDim.x) {
       const int k = w / (kPmeOrder * kPmeOrder), r = w - k * kPmeOrder * kPmeOrder;
       const float q = t.q[k];
       if (q == 0.f) continue;
@@ -570,7 +578,11 @@ void set_pme_smem(int z, int y, int x, int plane) {
 
 void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
-  k_spread<<<std::max(1, std::min((d.n_atoms + kSplineAtoms - 1) / kSplineAtoms, 148 * 8)), kThreads, 0, st>>>(d);
+  // about one block per two SMs, up to kSplineAtoms atoms each: small systems
+  // get short blocks (latency), large ones full ones (fewer SMs taken from the
+  // pair kernel running beside)
+  const int per = std::max(16, std::min(kSplineAtoms, (d.n_atoms + 73) / 74));
+  k_spread<<<std::max(1, std::min((d.n_atoms + per - 1) / per, 148 * 8)), kThreads, 0, st>>>(d, per);
 }
 
 void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {
