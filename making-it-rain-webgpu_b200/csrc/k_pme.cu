@@ -338,8 +338,9 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   float2* B = smem + w.n * Kx;
   const long long stride = static_cast<long long>(Ky) * kzh;
   float2* base = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * kzh + w.b;
+  const unsigned n_magic = magic_for(unsigned(w.n)), kx_magic = magic_for(unsigned(Kx));
   for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
-    const int x = i / w.n, l = i - x * w.n;
+    const int x = int(quotient(unsigned(i), n_magic)), l = i - x * w.n;
     A[l * Kx + x] = base[x * stride + l];
   }
   __syncthreads();
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   const float* modz = mody + Ky;
   const float two_pi = 6.283185307179586f;
   for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
-    const int l = i / Kx, mx = i - l * Kx;
+    const int l = int(quotient(unsigned(i), kx_magic)), mx = i - l * Kx;
     const int kz = w.b + l;
     const int ma = mx <= Kx / 2 ? mx : mx - Kx;
     const int mc = kz;  // kz <= Kz/2 on the half spectrum
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   __syncthreads();
   const float2* Q = fft_lines(R, other, Kx, w.n, S.radices[0], S.nradix[0], d.twiddles + S.tw_off[0], +1);
   for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
-    const int x = i / w.n, l = i - x * w.n;
+    const int x = int(quotient(unsigned(i), n_magic)), l = i - x * w.n;
     base[x * stride + l] = Q[l * Kx + x];
   }
   if (ENERGY) {
@@ -425,6 +426,8 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
   const FftWork w = d.fft_p[blockIdx.x];
   const SysDev& S = d.sys[w.sys];
   const int Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  const unsigned ky_magic = magic_for(unsigned(Ky)), kzh_magic = magic_for(unsigned(kzh)),
+                 rest_magic = magic_for(unsigned(Kz - kzh));
   float2* A = smem;
   float2* B = smem + Ky * Kz;
   unsigned long long* grid = d.qgrid + S.grid_off + static_cast<long long>(w.a) * Ky * Kz;
@@ -437,14 +440,14 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
   float2* T = R == A ? B : A;
   // the half spectrum's kz columns become y-lines
   for (int i = threadIdx.x; i < kzh * Ky; i += blockDim.x) {
-    const int k = i / Ky, y = i - k * Ky;
+    const int k = int(quotient(unsigned(i), ky_magic)), y = i - k * Ky;
     T[k * Ky + y] = R[y * Kz + k];
   }
   __syncthreads();
   const float2* Y = fft_lines(T, R, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], -1);
   float2* out = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
   for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
-    const int y = i / kzh, k = i - y * kzh;
+    const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
     out[i] = Y[k * Ky + y];
   }
 }
@@ -454,24 +457,26 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
   const FftWork w = d.fft_p[blockIdx.x];
   const SysDev& S = d.sys[w.sys];
   const int Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
+  const unsigned ky_magic = magic_for(unsigned(Ky)), kzh_magic = magic_for(unsigned(kzh)),
+                 rest_magic = magic_for(unsigned(Kz - kzh));
   float2* A = smem;
   float2* B = smem + Ky * Kz;
   const float2* in = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
   for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
-    const int y = i / kzh, k = i - y * kzh;
+    const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
     A[k * Ky + y] = in[i];
   }
   __syncthreads();
   float2* Y = fft_lines(A, B, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], +1);
   float2* Z = Y == A ? B : A;
   for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
-    const int y = i / kzh, k = i - y * kzh;
+    const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
     Z[y * Kz + k] = Y[k * Ky + y];
   }
   __syncthreads();
   // the rest of each z-line from Hermitian symmetry (the result is real)
   for (int i = threadIdx.x; i < Ky * (Kz - kzh); i += blockDim.x) {
-    const int y = i / (Kz - kzh), k = kzh + (i - y * (Kz - kzh));
+    const int y = int(quotient(unsigned(i), rest_magic)), k = kzh + (i - y * (Kz - kzh));
     const float2 c = Z[y * Kz + (Kz - k)];
     Z[y * Kz + k] = make_float2(c.x, -c.y);
   }
