@@ -339,9 +339,19 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   const long long stride = static_cast<long long>(Ky) * kzh;
   float2* base = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * kzh + w.b;
   const unsigned n_magic = magic_for(unsigned(w.n)), kx_magic = magic_for(unsigned(Kx));
-  for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
-    const int x = int(quotient(unsigned(i), n_magic)), l = i - x * w.n;
-    A[l * Kx + x] = base[x * stride + l];
+  for (int i0 = threadIdx.x; i0 < w.n * Kx; i0 += 2 * blockDim.x) {
+    float2 v[2];
+    int x[2], l[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int i = i0 + u * blockDim.x;
+      x[u] = int(quotient(unsigned(i), n_magic));
+      l[u] = i - x[u] * w.n;
+      v[u] = i < w.n * Kx ? __ldcg(&base[x[u] * stride + l[u]]) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      if (i0 + u * int(blockDim.x) < w.n * Kx) A[l[u] * Kx + x[u]] = v[u];
   }
   __syncthreads();
   float2* R = fft_lines(A, B, Kx, w.n, S.radices[0], S.nradix[0], d.twiddles + S.tw_off[0], -1);
@@ -431,9 +441,22 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
   float2* A = smem;
   float2* B = smem + Ky * Kz;
   unsigned long long* grid = d.qgrid + S.grid_off + static_cast<long long>(w.a) * Ky * Kz;
-  for (int i = threadIdx.x; i < Ky * Kz; i += blockDim.x) {
-    A[i] = make_float2(from_fixed(static_cast<long long>(grid[i])), 0.f);
-    grid[i] = 0ull;  // consumer clears: the next spread starts from zero
+  // four loads in flight per thread before any is used
+  for (int i0 = threadIdx.x; i0 < Ky * Kz; i0 += 4 * blockDim.x) {
+    long long v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * blockDim.x;
+      v[u] = i < Ky * Kz ? static_cast<long long>(__ldcg(&grid[i])) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < Ky * Kz) {
+        A[i] = make_float2(from_fixed(v[u]), 0.f);
+        grid[i] = 0ull;  // consumer clears: the next spread starts from zero
+      }
+    }
   }
   __syncthreads();
   float2* R = fft_lines(A, B, Kz, Ky, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], -1);
@@ -462,9 +485,21 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
   float2* A = smem;
   float2* B = smem + Ky * Kz;
   const float2* in = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
-  for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
-    const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
-    A[k * Ky + y] = in[i];
+  for (int i0 = threadIdx.x; i0 < Ky * kzh; i0 += 4 * blockDim.x) {
+    float2 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * blockDim.x;
+      v[u] = i < Ky * kzh ? __ldcg(&in[i]) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < Ky * kzh) {
+        const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
+        A[k * Ky + y] = v[u];
+      }
+    }
   }
   __syncthreads();
   float2* Y = fft_lines(A, B, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], +1);
