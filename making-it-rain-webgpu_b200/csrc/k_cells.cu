@@ -671,7 +671,9 @@ __device__ void phase_tiles_exclusions(const Dev& d) {
 // of reach is dropped at once, the others test their pairs until the first one
 // within reach, on f32 offsets from the tile's first atom (exact integer
 // differences, then one rounding), with the J cluster in registers --
-// independent loads and no shuffles.  32x32 tiles (too many registers for that) keep a tile if some
+// independent loads and no shuffles.  Tiles flagged for per-pair images (the
+// cell is too small for one shift per tile) take each pair's minimum image, as
+// the pair kernel does, so small systems get an inner list too.  32x32 tiles (too many registers for that) keep a tile if some
 // atom of I is within reach of J's current bounding box and some atom of J of
 // I's, which any pair within reach implies: conservative, one lane per atom.
 template <int C>
@@ -681,8 +683,27 @@ template <>
 __device__ bool tile_within_reach<8>(const Dev& d, const SysDev& S, long long ti, float reach2, int) {
   const int2 tile = __ldcg(&d.tiles[ti]);
   const int4 sh = __ldcg(&d.tile_shift[ti]);
-  if (sh.w) return true;  // per-pair images: kept as they are
   const float inv = S.pc_inv;
+  if (sh.w) {
+    // per-pair images (small cells): the pair kernel's own minimum image of each pair
+    const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
+    for (int i = 0; i < 8; ++i) {
+      const unsigned int row = ((i < 4 ? w0 : w1) >> ((i & 3) * 8)) & 0xFFu;
+      if (!row) continue;
+      const int4 qi = d.pc[tile.x * 8 + i];
+      for (int j = 0; j < 8; ++j) {
+        if (!((row >> j) & 1u)) continue;
+        const int4 qj = d.pc[tile.y * 8 + j];
+        int dx = int(unsigned(qj.x) - unsigned(qi.x)), dy = int(unsigned(qj.y) - unsigned(qi.y)),
+            dz = int(unsigned(qj.z) - unsigned(qi.z));
+        if (S.triclinic) min_image<true>(S, dx, dy, dz);
+        else min_image<false>(S, dx, dy, dz);
+        const float rx = dx * inv, ry = dy * inv, rz = dz * inv;
+        if (rx * rx + ry * ry + rz * rz < reach2) return true;
+      }
+    }
+    return false;
+  }
   {
     // the clusters' current boxes first: most outer tiles of a long skin are
     // out of reach box to box and need no pair loop (the margin covers the

@@ -324,3 +324,22 @@ def test_inner_list_changes_nothing(mdb, peptide, shape):
     assert f1["prunes"] > 10 and f1["rebuilds"] == f0["rebuilds"]
     assert f1["innerTiles"] < (0.8 if shape == 8 else 1.0) * f1["tiles"]
     assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+
+
+def test_inner_list_on_a_small_cell_changes_nothing(mdb):
+    """A 2.8 nm water box: every tile needs per-pair images (the cell is too
+    small for one shift per tile); the inner prune takes those images too, drops
+    tiles, and the trajectory stays bit-identical to the whole list's."""
+    from mdb200 import synth
+
+    system, state = synth.water_box(n_waters=700, width=2.8, seed=3, grid=(28, 28, 28))
+    runs = {}
+    for inner in (-1.0, 0.06):
+        loop = make_loop(mdb, system, state, seed=9, tuning=[(0.4, 0.2, 8, 2, inner)])
+        loop.run(300)
+        runs[inner] = (loop.positions(), loop.velocities(), loop.verlet_flags())
+        loop.destroy()
+    (p0, v0, f0), (p1, v1, f1) = runs[-1.0], runs[0.06]
+    print("small cell: whole list", f0, "inner list", f1)
+    assert f1["prunes"] > 10 and f1["innerTiles"] < 0.9 * f1["tiles"]
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
