@@ -104,6 +104,9 @@ struct SysDev {
   // the inner list: tiles with a pair inside (cutoff + inner skin)^2, re-pruned
   // from the outer list once an atom has moved (inner skin / 2)^2 since the last prune
   float inner2, half_inner2;
+  // the inner prune also tests tiles flagged for per-pair images: worth it in
+  // small cells, where nearly every tile is, and not where only a few are
+  int prune_per_pair;
   // PME
   int grid[3];
   int kzh;            // Kz/2 + 1

@@ -215,6 +215,8 @@ void fill_box(const HostSystem& h, SysDev& S, bool keep_shift) {
   double widths[3];
   perpendicular_widths(B, widths);
   S.min_width = float(std::min({widths[0], widths[1], widths[2]}));
+  // cells narrower than cutoff + list radius + 1 nm flag most tiles per-pair
+  S.prune_per_pair = S.min_width < std::sqrt(S.cut2) + std::sqrt(S.list2) + 1.0f ? 1 : 0;
   // Pair coordinates: the folded extent plus one box stays below 2^31.
   const double ext = std::max({B[0] + std::fabs(B[3]) + std::fabs(B[6]), B[4] + std::fabs(B[7]), B[8]});
   int shift = int(std::floor(std::log2(std::ldexp(1.0, 30) / ext)));

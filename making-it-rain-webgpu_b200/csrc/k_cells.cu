@@ -673,7 +673,9 @@ __device__ void phase_tiles_exclusions(const Dev& d) {
 // differences, then one rounding), with the J cluster in registers --
 // independent loads and no shuffles.  Tiles flagged for per-pair images (the
 // cell is too small for one shift per tile) take each pair's minimum image, as
-// the pair kernel does, so small systems get an inner list too.  32x32 tiles (too many registers for that) keep a tile if some
+// the pair kernel does, in cells narrower than cutoff + list radius + 1 nm,
+// where nearly every tile is flagged; in wider cells the few flagged tiles
+// are kept without a test.  32x32 tiles (too many registers for that) keep a tile if some
 // atom of I is within reach of J's current bounding box and some atom of J of
 // I's, which any pair within reach implies: conservative, one lane per atom.
 template <int C>
@@ -685,17 +687,21 @@ __device__ bool tile_within_reach<8>(const Dev& d, const SysDev& S, long long ti
   const int4 sh = __ldcg(&d.tile_shift[ti]);
   const float inv = S.pc_inv;
   if (sh.w) {
+    if (!S.prune_per_pair) return true;
     // per-pair images (small cells): the pair kernel's own minimum image of each pair
     const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
+    int4 qj[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) qj[j] = d.pc[tile.y * 8 + j];
     for (int i = 0; i < 8; ++i) {
       const unsigned int row = ((i < 4 ? w0 : w1) >> ((i & 3) * 8)) & 0xFFu;
       if (!row) continue;
       const int4 qi = d.pc[tile.x * 8 + i];
+#pragma unroll
       for (int j = 0; j < 8; ++j) {
         if (!((row >> j) & 1u)) continue;
-        const int4 qj = d.pc[tile.y * 8 + j];
-        int dx = int(unsigned(qj.x) - unsigned(qi.x)), dy = int(unsigned(qj.y) - unsigned(qi.y)),
-            dz = int(unsigned(qj.z) - unsigned(qi.z));
+        int dx = int(unsigned(qj[j].x) - unsigned(qi.x)), dy = int(unsigned(qj[j].y) - unsigned(qi.y)),
+            dz = int(unsigned(qj[j].z) - unsigned(qi.z));
         if (S.triclinic) min_image<true>(S, dx, dy, dz);
         else min_image<false>(S, dx, dy, dz);
         const float rx = dx * inv, ry = dy * inv, rz = dz * inv;

@@ -643,7 +643,8 @@ void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {
 
 void launch_pme_gather(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
-  k_gather<<<grid_blocks(d.n_slots), kThreads, 0, st>>>(d);
+  // a thread per slot; blocks of 64 so that even 10k atoms spread over every SM
+  k_gather<<<std::max(1, std::min((d.n_slots + 63) / 64, 148 * 16)), 64, 0, st>>>(d);
 }
 
 void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
