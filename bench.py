@@ -367,7 +367,7 @@ def main() -> None:
             one.destroy()
         plain_ms = max_over_ranks(plain_ms)
         # autotuner per size bucket (untimed), then one batched engine
-        tuning, buckets = steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local))
+        tuning, buckets = steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=400)
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride, tuning=tuning)
         loop = steploop.StepLoop.batch(systems, states, opts)
         total_s, clock_summary = timed(loop)
@@ -396,9 +396,12 @@ def main() -> None:
 
         system, state = synth.config_npt_100k(seed=1 + rank)
         frequency = system.barostat[2]
+        # one autotuned list configuration for both barostats (untimed)
+        best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=200)
+        tuned = [(best["verlet_skin"], best["sort_cell"], best["tile_atoms"], best["prune_tiles"], best["inner_skin"])]
         # the screened barostat learns from its first exact attempts (untimed)
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
-                                   surrogate_attempts=args.surrogate_attempts)
+                                   surrogate_attempts=args.surrogate_attempts, tuning=tuned)
         loop = steploop.StepLoop.from_parsed(system, state, opts)
         t_train = time.perf_counter()
         loop.run(args.surrogate_attempts * frequency)
@@ -407,7 +410,7 @@ def main() -> None:
         start = State(positions=loop.positions(), box=loop.box_vectors(), velocities=loop.velocities(),
                       step=loop.steps)
         plain = steploop.StepLoop.from_parsed(system, start, steploop.RunOptions(seed=7 + rank, device=local,
-                                                                                max_batch=args.stride))
+                                                                                max_batch=args.stride, tuning=tuned))
         plain_volumes = []
         plain_before = plain.barostat_statistics()
         plain_s, _ = timed(plain, lambda lp: plain_volumes.append(abs(np.linalg.det(lp.box_vectors()))))
@@ -428,6 +431,7 @@ def main() -> None:
                            f"screened barostat both timed from the state after the {args.surrogate_attempts * frequency}"
                            " training steps",
                "atoms": system.particle_count,
+               "autotuner": {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()},
                "plain_barostat_ns_per_day": plain_value, "screened_over_plain": value / plain_value,
                "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
                              "active": after["surrogateActive"], "rms_kj_mol": after["surrogateRms"],
@@ -457,7 +461,7 @@ def main() -> None:
             best = {"verlet_skin": v[0], "sort_cell": v[1], "tile_atoms": int(v[2]), "prune_tiles": int(v[3]),
                     "inner_skin": v[4] if len(v) > 4 else 0.0, "candidates": 0, "source": "--tuning"}
         else:
-            best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=200)
+            best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=600)
         cfg["autotuner"] = {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
                                    tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"],
