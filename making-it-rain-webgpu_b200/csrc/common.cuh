@@ -59,10 +59,7 @@ enum UnitKind : int { kUnitFree = 0, kUnitSettle = 1, kUnitShake = 2, kUnitStar 
 
 // Integrate blocks: kIntegrateUnits units per block, their atoms staged in a
 // shared-memory table of at most kIntegrateTable entries.
-#ifndef MDB_INTEGRATE_UNITS
-#define MDB_INTEGRATE_UNITS 32
-#endif
-constexpr int kIntegrateUnits = MDB_INTEGRATE_UNITS;
+constexpr int kIntegrateUnits = 32;
 constexpr int kIntegrateTable = kIntegrateUnits * kMaxClusterAtoms;
 
 // One integration unit: a free atom, a SETTLE water, or a SHAKE cluster.
