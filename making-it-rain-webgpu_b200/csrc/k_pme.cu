@@ -15,12 +15,14 @@
 //     index and the weight fraction carry no f32 coordinate rounding;
 //   * the charge grid is int64 fixed point filled with atomics, so the spread
 //     is order independent and runs are bit-identical;
-//   * the transform is five passes, each a CTA loading whole lines into shared
-//     memory and running a Stockham mixed-radix (2, 3, 4, 5, 7) FFT there: z
-//     (int64 -> complex, real-to-complex, clearing the grid it read), y, then
-//     x forward + convolution + x inverse in one pass, y inverse, z
-//     complex-to-real.  The reference's 7-13 global passes per direction and
-//     its separate load/convolve passes disappear.
+//   * the transform is three passes, each CTA running a Stockham mixed-radix
+//     (2, 3, 4, 5, 7) FFT over whole lines in shared memory: one CTA per
+//     x-plane does z (int64 -> complex, real-to-complex, clearing the grid it
+//     read) and y; the x pass does x forward + convolution + x inverse; one
+//     CTA per x-plane does y inverse and z complex-to-real.  Meshes whose
+//     planes do not fit shared memory take separate z and y passes (five in
+//     all).  The reference's 7-13 global passes per direction and its
+//     separate load/convolve passes disappear.
 #include <array>
 #include <cmath>
 #include <cstring>
