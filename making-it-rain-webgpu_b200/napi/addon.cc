@@ -202,6 +202,8 @@ napi_value Run(napi_env env, napi_callback_info info) {
   return nullptr;
 }
 
+napi_value energies_object(napi_env env, const mdb_energies& en);
+
 napi_value CopyOut(napi_env env, napi_callback_info info, int (*fn)(mdb_engine*, int32_t, double*)) {
   size_t argc = 2;
   napi_value argv[2];
@@ -229,6 +231,10 @@ napi_value Evaluate(napi_env env, napi_callback_info info) {
   mdb_energies en;
   const int status = mdb_evaluate(e, 0, forces, &en);
   if (status != MDB_OK) return throw_status(env, status, e);
+  return energies_object(env, en);
+}
+
+napi_value energies_object(napi_env env, const mdb_energies& en) {
   napi_value obj;
   napi_create_object(env, &obj);
   auto put = [&](const char* k, double v) {
@@ -244,6 +250,133 @@ napi_value Evaluate(napi_env env, napi_callback_info info) {
   put("HarmonicBondForce", en.bond);
   put("HarmonicAngleForce", en.angle);
   put("PeriodicTorsionForce", en.torsion);
+  return obj;
+}
+
+// potential(handle, positions, forces): the energies at `positions`, forces
+// written into `forces`; the engine's own state is left as it was.
+napi_value Potential(napi_env env, napi_callback_info info) {
+  size_t argc = 3;
+  napi_value argv[3];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  size_t n = 0, m = 0;
+  const double* positions = typed_array<double>(env, argv[1], &n);
+  double* forces = typed_array<double>(env, argv[2], &m);
+  mdb_energies en;
+  const int status = mdb_potential(e, 0, positions, forces, &en);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  return energies_object(env, en);
+}
+
+napi_value CopyIn(napi_env env, napi_callback_info info, int (*fn)(mdb_engine*, int32_t, const double*)) {
+  size_t argc = 2;
+  napi_value argv[2];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  size_t n = 0;
+  const double* in = typed_array<double>(env, argv[1], &n);
+  const int status = fn(e, 0, in);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  return nullptr;
+}
+
+napi_value SetPositions(napi_env env, napi_callback_info info) { return CopyIn(env, info, mdb_set_positions); }
+napi_value SetVelocities(napi_env env, napi_callback_info info) { return CopyIn(env, info, mdb_set_velocities); }
+napi_value SetBox(napi_env env, napi_callback_info info) { return CopyIn(env, info, mdb_set_box); }
+
+// box(handle): the nine box vector components, rows a, b, c.
+napi_value Box(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  void* data = nullptr;
+  napi_value buffer, array;
+  napi_create_arraybuffer(env, 9 * sizeof(double), &data, &buffer);
+  const int status = mdb_get_box(e, 0, static_cast<double*>(data));
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_create_typedarray(env, napi_float64_array, 9, buffer, 0, &array);
+  return array;
+}
+
+// mesh(handle): the PME mesh, three sizes.
+napi_value Mesh(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  void* data = nullptr;
+  napi_value buffer, array;
+  napi_create_arraybuffer(env, 3 * sizeof(int32_t), &data, &buffer);
+  const int status = mdb_get_mesh(e, 0, static_cast<int32_t*>(data));
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_create_typedarray(env, napi_int32_array, 3, buffer, 0, &array);
+  return array;
+}
+
+napi_value SetStep(napi_env env, napi_callback_info info) {
+  size_t argc = 2;
+  napi_value argv[2];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  int64_t step = 0;
+  napi_get_value_int64(env, argv[1], &step);
+  const int status = mdb_set_step(e, step);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  return nullptr;
+}
+
+napi_value Step(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  int64_t step = 0;
+  const int status = mdb_get_step(e, &step);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_value v;
+  napi_create_int64(env, step, &v);
+  return v;
+}
+
+// barostat(handle): {attempts, accepted, volumeScale}, barostatStatistics' fields.
+napi_value Barostat(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  mdb_barostat_stats b;
+  const int status = mdb_get_barostat_stats(e, 0, &b);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_value obj, v;
+  napi_create_object(env, &obj);
+  napi_create_int64(env, b.attempts, &v);
+  napi_set_named_property(env, obj, "attempts", v);
+  napi_create_int64(env, b.accepted, &v);
+  napi_set_named_property(env, obj, "accepted", v);
+  napi_create_double(env, b.volume_scale, &v);
+  napi_set_named_property(env, obj, "volumeScale", v);
+  return obj;
+}
+
+// neighbours(handle): {rebuilds, tiles, overflowed}, verletFlags' fields.
+napi_value Neighbours(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  mdb_neighbour_stats ns;
+  const int status = mdb_get_neighbour_stats(e, 0, &ns);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_value obj, v;
+  napi_create_object(env, &obj);
+  napi_create_int64(env, ns.rebuilds, &v);
+  napi_set_named_property(env, obj, "rebuilds", v);
+  napi_create_int64(env, ns.tiles, &v);
+  napi_set_named_property(env, obj, "tiles", v);
+  napi_get_boolean(env, ns.overflowed != 0, &v);
+  napi_set_named_property(env, obj, "overflowed", v);
   return obj;
 }
 
@@ -267,6 +400,16 @@ napi_value Init(napi_env env, napi_value exports) {
       {"positions", nullptr, Positions, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"velocities", nullptr, Velocities, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"evaluate", nullptr, Evaluate, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"potential", nullptr, Potential, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"setPositions", nullptr, SetPositions, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"setVelocities", nullptr, SetVelocities, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"setBox", nullptr, SetBox, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"box", nullptr, Box, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"mesh", nullptr, Mesh, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"setStep", nullptr, SetStep, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"step", nullptr, Step, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"barostat", nullptr, Barostat, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"neighbours", nullptr, Neighbours, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"destroy", nullptr, Destroy, nullptr, nullptr, nullptr, napi_default, nullptr},
   };
   napi_define_properties(env, exports, sizeof(props) / sizeof(props[0]), props);
