@@ -76,3 +76,57 @@ def test_null_arguments_are_refused_without_a_device(lib):
     assert lib.mdb_run(None, 1) == abi.ERR_INVALID_ARGUMENT
     assert lib.mdb_destroy(None, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.mdb_last_error(None) == b"no engine"
+
+
+def test_every_struct_mirror_matches_the_c_compiler(tmp_path):
+    """sizeof and every field offset of the header's structs, from gcc, against
+    the ctypes mirrors the Python host side passes to the library."""
+    import shutil
+    import subprocess
+
+    from mdb200 import abi
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    mirrors = {"mdb_tuning": abi.Tuning, "mdb_run_options": abi.RunOptions, "mdb_energies": abi.Energies,
+               "mdb_barostat_stats": abi.BarostatStats, "mdb_profile": abi.Profile,
+               "mdb_neighbour_stats": abi.NeighbourStats, "mdb_system_desc": abi.SystemDesc,
+               "mdb_state_desc": abi.StateDesc}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "mdb.h"', "int main(void) {"]
+    for cname, mirror in mirrors.items():
+        lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for field, _ in mirror._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines.append("  return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    include = ROOT / "include"
+    subprocess.run(["gcc", "-std=c11", "-I", str(include), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            cname, field, value = line.split()
+            got[(cname, field)] = int(value)
+    for cname, mirror in mirrors.items():
+        assert got[(cname, "sizeof")] == C.sizeof(mirror), cname
+        for field, _ in mirror._fields_:
+            assert got[(cname, field)] == getattr(mirror, field).offset, (cname, field)
+
+
+def test_node_addon_exports_what_the_typescript_shim_calls():
+    """The TypeScript StepLoop's addon interface and the Node-API addon's
+    export table name the same methods, and the addon calls only entry points
+    the header declares (neither can be built here: no Node)."""
+    ts = (ROOT / "making-it-rain-webgpu_b200" / "ts" / "step-loop.ts").read_text()
+    cc = (ROOT / "making-it-rain-webgpu_b200" / "napi" / "addon.cc").read_text()
+    header = (ROOT / "include" / "mdb.h").read_text()
+    block = ts[ts.index("interface MdbAddon {"):]
+    block = block[:block.index("\n}")]
+    wanted = set(re.findall(r"^\s+(\w+)\(", block, re.M))
+    exported = set(re.findall(r'\{"(\w+)", nullptr, \w+,', cc))
+    assert wanted == exported, (wanted ^ exported)
+    called = set(re.findall(r"\b(mdb_[a-z_]+)\(", cc))
+    declared = set(re.findall(r"\b(mdb_[a-z_]+)\(", header))
+    assert called <= declared, called - declared
