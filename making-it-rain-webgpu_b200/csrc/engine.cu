@@ -1648,9 +1648,10 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
   out->ms_integrate = time([&] { launch_integrate(d, st); });
   // per step: the list kernels (one cooperative launch, or 5 sort + 1 wrap +
   // 6 tile-list kernels, 3 more when rebuilds prune), the inner-list kernel,
-  // 7 PME, listed, nonbonded, integrator
+  // PME (spread, 3 transform passes or 5 without the plane kernels, gather),
+  // listed, nonbonded, integrator
   out->launches_per_step = (e->coop_list ? 1 : 5 + 1 + 6 + (d.prune ? 3 : 0)) + (d.inner ? 1 : 0) +
-                           (d.n_fft_z ? 7 : 0) +
+                           (d.n_fft_z ? (d.fft_planes ? 5 : 7) : 0) +
                            (d.n_bonds + d.n_angles + d.n_torsions + d.n_exceptions + d.n_restraints > 0 ? 1 : 0) +
                            1 + 1;
   CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, st));
