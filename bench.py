@@ -46,9 +46,10 @@ NS_PER_DAY_PER_STEP_PER_S = TIME_STEP_PS * 86400 / 1000.0
 FLOP_PER_PAIR = 74.0
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate at max SM clock
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_nonbonded launch, from
-# the ncu capture summarised in profiles/nonbonded_octahedron27k.md (captured
-# with the autotuned configuration; other workloads report null)
-NB_TRAFFIC = {"octa-27k": 11175936}
+# the ncu captures summarised in profiles/nonbonded_octahedron27k.md and
+# profiles/nonbonded_dram_peptide12k.md (each captured with the configuration
+# the autotuner picks; other workloads report null)
+NB_TRAFFIC = {"octa-27k": 11175936, "peptide-12k": 5061632}
 
 
 def workload(name: str, seed: int):
