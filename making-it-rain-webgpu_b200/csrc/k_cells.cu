@@ -786,7 +786,11 @@ __device__ void phase_inner(const Dev& d) {
     const SysDev& S = d.sys[s];
     const int n = min(d.tile_count[s], S.tile_cap);
     const float reach2 = S.inner2 * (1.0f + 1e-5f);
-    for (int c0 = warp * 32; c0 < n; c0 += warps * 32) {
+    // each system's first chunk goes to the warp after the previous system's
+    // last (the outer list's offsets, which this kernel only reads), so a
+    // batch of small systems spreads over every warp instead of the first few
+    const int first = (d.tile_prefix[s] >> 5) % warps;
+    for (int c0 = ((warp - first + warps) % warps) * 32; c0 < n; c0 += warps * 32) {
       unsigned int keep = 0u;  // bit k: outer tile c0 + k survives (the same in every lane)
       if (C == 8) {
         const bool alive = c0 + lane < n && tile_within_reach<C>(d, S, S.tile_off + c0 + lane, reach2, lane);
