@@ -41,8 +41,10 @@ sys.path.insert(0, str(ROOT))
 
 TIME_STEP_PS = 0.002
 NS_PER_DAY_PER_STEP_PER_S = TIME_STEP_PS * 86400 / 1000.0
-# Algorithmic FP32 work per unique in-cutoff pair: 74 flop (FMA = 2, special
-# functions = 1), the tally written down with the roofline in DESIGN.md.
+# Algorithmic FP32 work per unique in-cutoff pair: 74 flop, counting an FMA as 2
+# and a special function as 1: distance 8, rsqrt and r 2, alpha r 1, erfc by
+# exp and a rational 25, charge product 2, Coulomb energy 2 and derivative 6,
+# LJ 18, force scale and the two 3-vector updates 10.
 FLOP_PER_PAIR = 74.0
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate at max SM clock
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_nonbonded launch, from

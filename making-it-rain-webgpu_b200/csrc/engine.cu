@@ -63,13 +63,13 @@ struct Allocation {
 struct Surrogate {
   int target = 0;                 // exact attempts to learn from before screening; 0 = off
   bool active = false;            // trained: proposals go through the two-stage test
-  bool disabled = false;          // the exact stage judged it too inaccurate: plain barostat
+  bool disabled = false;          // the exact stage found it too inaccurate: plain barostat
   std::vector<float> feats;       // raw features of every exact attempt, kMlpIn each
   std::vector<double> delta_u;    // exact change minus its first-order term, per atom, kJ/mol
   std::vector<double> dlnv;       // the move of each attempt
   double mu[kMlpIn] = {}, sd[kMlpIn] = {}, mu_t = 0, sd_t = 1;
   double err2 = 0;                // running mean square of (predicted - exact) change
-  int64_t judged = 0;
+  int64_t checked = 0;
   MlpDev dev{};
   float* x = nullptr;             // device: normalised training inputs, then inference inputs
   float* t = nullptr;             // device: normalised targets
@@ -1228,10 +1228,10 @@ int barostat_attempt(mdb_engine* e, int s) {
       const double a1_rev = std::min(1.0, std::exp(-(du_rev - volume_term) / kT));
       const double a2 = std::min(1.0, std::exp(-w / kT) * a1_rev / a1);
       accepted = uniform() < a2;
-      // the exact stage judges the network
+      // the exact stage checks the network's prediction
       const double err = du_pred - du;
-      net.err2 = net.judged == 0 ? err * err : 0.98 * net.err2 + 0.02 * err * err;
-      if (++net.judged >= 50 && std::sqrt(net.err2) > kSurrogateMaxRmsKT * kT) net.disabled = true;
+      net.err2 = net.checked == 0 ? err * err : 0.98 * net.err2 + 0.02 * err * err;
+      if (++net.checked >= 50 && std::sqrt(net.err2) > kSurrogateMaxRmsKT * kT) net.disabled = true;
     } else {
       accepted = !(w > 0 && uniform() > std::exp(-w / kT));
       if (net.target > 0 && !net.active) {

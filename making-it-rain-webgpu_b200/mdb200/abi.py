@@ -292,8 +292,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
     target = Path(path) if path is not None else LIBRARY_PATH
     if not target.exists():
         raise EngineLibraryMissing(
-            f"{target} is not built. Run __graft_entry__.build() (or "
-            "`python making-it-rain-webgpu_b200/build.py`); this package has no "
+            f"{target} is not built. Run `python making-it-rain-webgpu_b200/build.py` "
+            "(nvcc for sm_100a); this package has no "
             "CPU fallback."
         )
     try:

@@ -1,7 +1,7 @@
 """Parity of the CUDA engine against the f64 oracle, through the C ABI.
 
 Tolerances are the reference's own (src/gpu/validate.ts:80-117,
-src/gpu/validate-loop.ts:90-100) and the north-star force bound:
+src/gpu/validate-loop.ts:90-100) and the engine's force bound:
   forces                     relative RMS <= 1.1e-6 against the f64 oracle
   direct-space group energy  1e-4 relative
   reciprocal group energy    1e-5 relative

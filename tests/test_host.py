@@ -78,7 +78,7 @@ def test_water_box_is_rigid_and_neutral():
 
 
 def test_peptide_workload_matches_the_configuration():
-    """Ala20 helix + caps, 5 nm TIP3P cube, 0.15 M NaCl, ~12,000 atoms."""
+    """The peptide workload: Ala20 helix + caps, 5 nm TIP3P cube, 0.15 M NaCl, ~12,000 atoms."""
     from mdb200 import synth
     from oracle import oracle
 

@@ -1,4 +1,4 @@
-"""Velocity initialisation and what a run writes (SURVEY f2): the
+"""Velocity initialisation and what a run writes: the
 counter-based draw against the Random123 known answers and the oracle, the
 constraint projection, the -(dt/2) F/m shift; DCD frames in OpenMM's layout
 (src/analysis/dcd.ts), the StateDataReporter log (src/analysis/log.ts) and
