@@ -142,31 +142,42 @@ def flush_l2(buffer) -> None:
     buffer.zero_()
 
 
-def cpu_time_oracle(system, state, steps_hint: int, budget_s: float, threads: int):
-    """Steps/s of the f64 CPU restatement (oracle/), a bounded sample."""
+def cpu_time_oracle(system, state, steps_hint: int, budget_s: float, threads: int, warmup: int = 1):
+    """Steps/s of the f64 CPU restatement (oracle/), a bounded sample after
+    untimed warm-up steps: `warmup` of them, but no more than fit in about ten
+    seconds (and never fewer than min(warmup, 3)).  Returns (steps/s, timed
+    steps, seconds, warm-up steps)."""
     from oracle import oracle as orc
+    from mdb200.system import State
 
     t = time.perf_counter()
     p, v, step = orc.run(system, state, 1, seed=1, threads=threads)
     one = time.perf_counter() - t
+    w = min(warmup, max(3, 1 + int(10.0 / max(one, 1e-6))))
+    if w > 1:
+        p, v, step = orc.run(system, State(positions=p, box=state.box, velocities=v, step=step), w - 1, seed=1,
+                             threads=threads)
     n = max(1, min(steps_hint, int(budget_s / max(one, 1e-6))))
-    from mdb200.system import State
-
     st = State(positions=p, box=state.box, velocities=v, step=step)
     t = time.perf_counter()
     orc.run(system, st, n, seed=1, threads=threads)
     elapsed = time.perf_counter() - t
-    return n / elapsed, n, elapsed
+    return n / elapsed, n, elapsed, max(1, w)
 
 
-def cpu_rate(config: str, steps_hint: int, budget_s: float, threads: int):
-    """ns/day of the oracle on the workload, and a description of the sample.
-    For the ensemble: one step of every system, summed into one ensemble step."""
+def cpu_rate(config: str, steps_hint: int, budget_s: float, threads: int, warmup: int = 1):
+    """ns/day of the oracle on the workload, a description of the sample, and
+    the warm-up steps taken.  For the ensemble: one step of every system,
+    summed into one ensemble step, after `warmup` (at most 3) steps of its
+    smallest system."""
     if config == "ensemble-64":
         from mdb200 import synth
         from oracle import oracle as orc
 
         members = synth.config_ensemble_64(seed=1)
+        w = max(1, min(warmup, 3))
+        small = min(members, key=lambda m: m[0].particle_count)
+        orc.run(small[0], small[1], w, seed=1, threads=threads)
         elapsed = 0.0
         for system, state, _ in members:
             t = time.perf_counter()
@@ -174,15 +185,16 @@ def cpu_rate(config: str, steps_hint: int, budget_s: float, threads: int):
             elapsed += time.perf_counter() - t
         value = len(members) / elapsed * NS_PER_DAY_PER_STEP_PER_S
         return value, 1, elapsed, (f"one MD step of each of the {len(members)} systems ({elapsed:.1f} s), "
-                                   "system-ns/day summed")
+                                   f"system-ns/day summed, after {w} warm-up steps of the smallest"), w
     if config == "npt-100k":
         from mdb200 import synth
 
         system, state = synth.config_npt_100k(seed=1)
     else:
         system, state, _ = workload(config, seed=1)
-    sps, n, elapsed = cpu_time_oracle(system, state, steps_hint, budget_s, threads)
-    return sps * NS_PER_DAY_PER_STEP_PER_S, n, elapsed, f"{n} MD steps of the same workload in {elapsed:.1f} s"
+    sps, n, elapsed, w = cpu_time_oracle(system, state, steps_hint, budget_s, threads, warmup)
+    return (sps * NS_PER_DAY_PER_STEP_PER_S, n, elapsed,
+            f"{n} MD steps of the same workload in {elapsed:.1f} s after {w} warm-up steps", w)
 
 
 def main() -> None:
@@ -214,11 +226,12 @@ def main() -> None:
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        value, n, elapsed, sample = cpu_rate(config, args.steps, min(args.cpu_budget * 6, 240.0), threads)
+        value, n, elapsed, sample, warm = cpu_rate(config, args.steps, min(args.cpu_budget * 6, 240.0), threads,
+                                                   args.warmup)
         cfg = {"workload": config} if config in ("ensemble-64", "npt-100k") else workload(config, seed=1)[2]
         print(json.dumps({
             "impl": "reference", "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": args.gpus,
-            "steps": n, "warmup": 1, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
+            "steps": n, "warmup": warm, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
             "scaling": "strong" if config == "ensemble-64" else "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {**cfg, "parallelism": "host threads", "l2": "n/a (CPU)"},
@@ -508,8 +521,8 @@ def main() -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cpu_value, _, _, sample = cpu_rate(config, 1000, args.cpu_budget, threads)
-        one_value, _, _, one_sample = cpu_rate(config, 1000, args.cpu_budget / 2, 1)
+        cpu_value, _, _, sample, _ = cpu_rate(config, 1000, args.cpu_budget, threads)
+        one_value, _, _, one_sample, _ = cpu_rate(config, 1000, args.cpu_budget / 2, 1)
         result["cpu_baseline"] = {
             "value": cpu_value, "unit": "ns/day", "cores": threads, "kind": "port",
             "sample": sample + " (f64 C++ restatement of src/reference, OpenMP over all host threads)",
