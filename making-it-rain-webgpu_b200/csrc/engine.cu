@@ -136,7 +136,11 @@ int alloc(mdb_engine* e, const char* label, T*& out, size_t count) {
   void* p = nullptr;
   cudaError_t err = cudaMalloc(&p, bytes);
   if (err != cudaSuccess) return fail(e, MDB_ERR_DEVICE, std::string("cudaMalloc ") + label + ": " + cudaGetErrorString(err));
-  cudaMemset(p, 0, bytes);
+  err = cudaMemset(p, 0, bytes);
+  if (err != cudaSuccess) {
+    cudaFree(p);
+    return fail(e, MDB_ERR_DEVICE, std::string("cudaMemset ") + label + ": " + cudaGetErrorString(err));
+  }
   e->allocs.push_back({label, p, bytes});
   out = static_cast<T*>(p);
   return MDB_OK;
@@ -243,7 +247,7 @@ int check_device_status(mdb_engine* e) {
   cudaError_t err = cudaStreamSynchronize(e->s0);
   if (err != cudaSuccess) return fail(e, MDB_ERR_DEVICE, std::string("device: ") + cudaGetErrorString(err));
   std::vector<int> flags(e->d.S), shake(e->d.S);
-  cudaMemcpy(flags.data(), e->d.err, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost);
+  CUDA_TRY(e, cudaMemcpy(flags.data(), e->d.err, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost));
   int any = 0;
   for (int f : flags) any |= f;
   if (any & kErrTileCapacity) return fail(e, MDB_ERR_CAPACITY, "the cluster-pair tile list ran out of room");
@@ -310,14 +314,15 @@ int run_steps(mdb_engine* e, int64_t steps) {
   return MDB_OK;
 }
 
-void request_rebuild(mdb_engine* e, int s) {
+int request_rebuild(mdb_engine* e, int s) {
   std::vector<int> now(e->d.S, 0);
-  cudaMemcpy(now.data(), e->d.rebuild_now, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost);
+  CUDA_TRY(e, cudaMemcpy(now.data(), e->d.rebuild_now, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost));
   if (s < 0) std::fill(now.begin(), now.end(), 1);
   else now[s] = 1;
   const int one = 1;
-  cudaMemcpy(e->d.rebuild_now, now.data(), sizeof(int) * e->d.S, cudaMemcpyHostToDevice);
-  cudaMemcpy(e->d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice);
+  CUDA_TRY(e, cudaMemcpy(e->d.rebuild_now, now.data(), sizeof(int) * e->d.S, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(e->d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+  return MDB_OK;
 }
 
 int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb_state_desc* states,
@@ -828,7 +833,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   CUDA_TRY(e, cudaDeviceSynchronize());
 
   // first list and the first COM velocity, by the phase kernels
-  request_rebuild(e, -1);
+  if (const int st = request_rebuild(e, -1)) return st;
   launch_rebuild_sort(d, e->s0);
   launch_wrap(d, e->s0);
   launch_rebuild_tiles(d, e->s0);
@@ -882,10 +887,10 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
     std::vector<unsigned long long> f[3];
     std::vector<int> order(S.n_slots);
     for (auto& v : f) v.resize(S.n_slots);
-    cudaMemcpy(f[0].data(), d.fx + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost);
-    cudaMemcpy(f[1].data(), d.fy + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost);
-    cudaMemcpy(f[2].data(), d.fz + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost);
-    cudaMemcpy(order.data(), d.order + S.slot_off, sizeof(int) * S.n_slots, cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(f[0].data(), d.fx + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost));
+    CUDA_TRY(e, cudaMemcpy(f[1].data(), d.fy + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost));
+    CUDA_TRY(e, cudaMemcpy(f[2].data(), d.fz + S.slot_off, sizeof(long long) * S.n_slots, cudaMemcpyDeviceToHost));
+    CUDA_TRY(e, cudaMemcpy(order.data(), d.order + S.slot_off, sizeof(int) * S.n_slots, cudaMemcpyDeviceToHost));
     for (int k = 0; k < S.n_slots; ++k) {
       const int a = order[k];
       if (a < 0) continue;
@@ -896,12 +901,12 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
   if (out) {
     std::memset(out, 0, sizeof(*out));
     std::vector<unsigned long long> en(kECount);
-    cudaMemcpy(en.data(), d.energy + S.energy_base, sizeof(long long) * kECount, cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(en.data(), d.energy + S.energy_base, sizeof(long long) * kECount, cudaMemcpyDeviceToHost));
     auto val = [&](int k) { return double((long long)en[k]) / 4294967296.0; };
     std::vector<double> mesh(e->n_mesh_items);
-    cudaMemcpy(mesh.data(), d.mesh_partial, sizeof(double) * e->n_mesh_items, cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(mesh.data(), d.mesh_partial, sizeof(double) * e->n_mesh_items, cudaMemcpyDeviceToHost));
     std::vector<double> mesh_vir(size_t(e->n_mesh_items) * 6);
-    cudaMemcpy(mesh_vir.data(), d.mesh_virial, sizeof(double) * mesh_vir.size(), cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(mesh_vir.data(), d.mesh_virial, sizeof(double) * mesh_vir.size(), cudaMemcpyDeviceToHost));
     double em = 0, wm[6] = {0, 0, 0, 0, 0, 0};
     for (int k = 0; k < e->n_mesh_items; ++k)
       if (e->fft_x_sys[k] == s) {
@@ -946,9 +951,9 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
     if (kinetic) {
       std::vector<float> v[3];
       for (auto& x : v) x.resize(h.n);
-      cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
-      cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
-      cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost);
+      CUDA_TRY(e, cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
+      CUDA_TRY(e, cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
+      CUDA_TRY(e, cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
       double ke = 0;
       for (int a = 0; a < h.n; ++a)
         if (h.mass[a] > 0)
@@ -972,9 +977,9 @@ int get_positions(mdb_engine* e, int s, double* out) {
   std::vector<long long> p[3];
   for (auto& v : p) v.resize(n);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  cudaMemcpy(p[0].data(), e->d.px + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost);
-  cudaMemcpy(p[1].data(), e->d.py + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost);
-  cudaMemcpy(p[2].data(), e->d.pz + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+  CUDA_TRY(e, cudaMemcpy(p[0].data(), e->d.px + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(p[1].data(), e->d.py + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(p[2].data(), e->d.pz + S.atom_off, sizeof(long long) * n, cudaMemcpyDeviceToHost));
   for (int a = 0; a < n; ++a)
     for (int k = 0; k < 3; ++k) out[3 * a + k] = double(p[k][a]) / 4294967296.0;
   return MDB_OK;
@@ -992,16 +997,15 @@ int set_positions(mdb_engine* e, int s, const double* in, bool clear_residual) {
       p[k][a] = to_fixed_host(in[3 * a + k]);
     }
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  cudaMemcpy(e->d.px + S.atom_off, p[0].data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(e->d.py + S.atom_off, p[1].data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(e->d.pz + S.atom_off, p[2].data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
+  CUDA_TRY(e, cudaMemcpy(e->d.px + S.atom_off, p[0].data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(e->d.py + S.atom_off, p[1].data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(e->d.pz + S.atom_off, p[2].data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
   if (clear_residual) {
-    cudaMemset(e->d.rx + S.atom_off, 0, sizeof(float) * n);
-    cudaMemset(e->d.ry + S.atom_off, 0, sizeof(float) * n);
-    cudaMemset(e->d.rz + S.atom_off, 0, sizeof(float) * n);
+    CUDA_TRY(e, cudaMemset(e->d.rx + S.atom_off, 0, sizeof(float) * n));
+    CUDA_TRY(e, cudaMemset(e->d.ry + S.atom_off, 0, sizeof(float) * n));
+    CUDA_TRY(e, cudaMemset(e->d.rz + S.atom_off, 0, sizeof(float) * n));
   }
-  request_rebuild(e, s);
-  return MDB_OK;
+  return request_rebuild(e, s);
 }
 
 int set_box(mdb_engine* e, int s, const double* box) {
@@ -1017,8 +1021,7 @@ int set_box(mdb_engine* e, int s, const double* box) {
   fill_box(h, e->sd[s], true);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys) + s, &e->sd[s], sizeof(SysDev), cudaMemcpyHostToDevice));
-  request_rebuild(e, s);
-  return MDB_OK;
+  return request_rebuild(e, s);
 }
 
 // ---- the barostat's screening network (no reference counterpart) ----------
@@ -1463,9 +1466,9 @@ int mdb_get_velocities(mdb_engine* e, int32_t s, double* out) {
   std::vector<float> v[3];
   for (auto& x : v) x.resize(n);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  cudaMemcpy(v[0].data(), e->d.vx + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost);
-  cudaMemcpy(v[1].data(), e->d.vy + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost);
-  cudaMemcpy(v[2].data(), e->d.vz + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  CUDA_TRY(e, cudaMemcpy(v[0].data(), e->d.vx + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(v[1].data(), e->d.vy + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(v[2].data(), e->d.vz + S.atom_off, sizeof(float) * n, cudaMemcpyDeviceToHost));
   for (int a = 0; a < n; ++a)
     for (int k = 0; k < 3; ++k) out[3 * a + k] = v[k][a];
   return MDB_OK;
@@ -1485,9 +1488,9 @@ int mdb_set_velocities(mdb_engine* e, int32_t s, const double* velocities) {
   for (int a = 0; a < n; ++a)
     for (int k = 0; k < 3; ++k) v[k][a] = float(velocities[3 * a + k]);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  cudaMemcpy(e->d.vx + S.atom_off, v[0].data(), sizeof(float) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(e->d.vy + S.atom_off, v[1].data(), sizeof(float) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(e->d.vz + S.atom_off, v[2].data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  CUDA_TRY(e, cudaMemcpy(e->d.vx + S.atom_off, v[0].data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(e->d.vy + S.atom_off, v[1].data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(e->d.vz + S.atom_off, v[2].data(), sizeof(float) * n, cudaMemcpyHostToDevice));
   launch_momentum(e->d, e->s0);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   return MDB_OK;
@@ -1550,9 +1553,9 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   long long rebuilds = 0;
   int tiles = 0, err = 0;
-  cudaMemcpy(&rebuilds, e->d.rebuild_count + s, sizeof(long long), cudaMemcpyDeviceToHost);
-  cudaMemcpy(&tiles, e->d.tile_count + s, sizeof(int), cudaMemcpyDeviceToHost);
-  cudaMemcpy(&err, e->d.err + s, sizeof(int), cudaMemcpyDeviceToHost);
+  CUDA_TRY(e, cudaMemcpy(&rebuilds, e->d.rebuild_count + s, sizeof(long long), cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(&tiles, e->d.tile_count + s, sizeof(int), cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(&err, e->d.err + s, sizeof(int), cudaMemcpyDeviceToHost));
   out->rebuilds = rebuilds;
   out->tiles = tiles;
   out->tile_capacity = e->sd[s].tile_cap;
@@ -1565,8 +1568,8 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   if (e->d.inner) {
     int inner = 0;
     long long prunes = 0;
-    cudaMemcpy(&inner, e->d.in_count + s, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&prunes, e->d.prune_count + s, sizeof(long long), cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(&inner, e->d.in_count + s, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(e, cudaMemcpy(&prunes, e->d.prune_count + s, sizeof(long long), cudaMemcpyDeviceToHost));
     out->inner_tiles = inner;
     out->prunes = prunes;
     out->inner_skin = e->inner_skin[s] > 0 ? std::min(e->inner_skin[s], e->skin[s]) : 0.0;
@@ -1595,19 +1598,19 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
   // pairs of every system of the engine: the pair kernel's launch covers them all
   {
     std::vector<unsigned long long> all(size_t(d.S) * kECount);
-    cudaMemcpy(all.data(), d.energy, sizeof(unsigned long long) * all.size(), cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(all.data(), d.energy, sizeof(unsigned long long) * all.size(), cudaMemcpyDeviceToHost));
     int64_t pairs = 0;
     for (int s = 0; s < d.S; ++s) pairs += static_cast<long long>(all[size_t(s) * kECount + kEPairs]);
     out->pairs_within_cutoff = pairs;
   }
   int tiles = 0;
-  cudaMemcpy(&tiles, d.tile_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost);
+  CUDA_TRY(e, cudaMemcpy(&tiles, d.tile_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost));
   out->tiles = tiles;
   out->tile_atoms = d.cluster;
   out->inner_tiles = tiles;
   if (d.inner) {
     int inner = 0;
-    cudaMemcpy(&inner, d.in_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost);
+    CUDA_TRY(e, cudaMemcpy(&inner, d.in_prefix + d.S, sizeof(int), cudaMemcpyDeviceToHost));
     out->inner_tiles = inner;
   }
   out->atoms = d.n_atoms;
@@ -1628,6 +1631,7 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
     cudaMemcpyAsync(d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, st);
     list_kernels(e, st);
   });
+  CUDA_TRY(e, cudaGetLastError());
   if (d.inner)
     out->ms_inner_prune = time([&] {
       cudaMemcpyAsync(d.prune_now, ones.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice, st);
