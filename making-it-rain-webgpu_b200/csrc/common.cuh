@@ -150,6 +150,33 @@ __device__ __forceinline__ void add_fixed64(unsigned long long* slot, long long 
   atomicAdd(slot, static_cast<unsigned long long>(v));
 }
 
+// ---------------------------------------------------- pair coordinates --
+// A 2^32 fixed-point coordinate as int32 at 2^shift per nm, rounded.
+__device__ __forceinline__ int to_pair_coordinate(long long v, int shift) {
+  const int down = 32 - shift;
+  return static_cast<int>((v + (1ll << (down - 1))) >> down);
+}
+
+// The lattice translation a rebuild stored for a slot: three signed 10-bit
+// counts in one word.
+__device__ __forceinline__ void unpack_fold(int w, long long& na, long long& nb, long long& nc) {
+  na = (w << 22) >> 22;
+  nb = (w << 12) >> 22;
+  nc = (w << 2) >> 22;
+}
+
+// The pair coordinates of a position folded by (na, nb, nc) lattice vectors.
+// The list kernel writes them at a rebuild or a prune and the integrator after
+// every step, through this one function, so both give the same bits.
+__device__ __forceinline__ int4 pair_coordinate(const SysDev& S, long long x, long long y, long long z, long long na,
+                                                long long nb, long long nc) {
+  x -= na * S.box_fx[0] + nb * S.box_fx[3] + nc * S.box_fx[6];
+  y -= nb * S.box_fx[4] + nc * S.box_fx[7];
+  z -= nc * S.box_fx[8];
+  return make_int4(to_pair_coordinate(x, S.pc_shift), to_pair_coordinate(y, S.pc_shift),
+                   to_pair_coordinate(z, S.pc_shift), 0);
+}
+
 // ------------------------------------------------------------------ RNG --
 // Threefry-2x32-20 and Box-Muller, the device twin of src/reference/random.ts
 // (random.wgsl:30-83).  The integer part is bit-exact with the oracle.

@@ -53,11 +53,6 @@ __device__ __forceinline__ Folded fold(const SysDev& S, long long x, long long y
   return f;
 }
 
-__device__ __forceinline__ int to_pair_coordinate(long long v, int shift) {
-  const int down = 32 - shift;
-  return static_cast<int>((v + (1ll << (down - 1))) >> down);
-}
-
 __device__ __forceinline__ int cell_index(unsigned int frac, int dim) {
   const int c = static_cast<int>((static_cast<unsigned long long>(frac) * static_cast<unsigned>(dim)) >> 32);
   return c < dim ? c : dim - 1;
@@ -204,16 +199,9 @@ __device__ void phase_wrap(const Dev& d) {
         nc = f.nc;
         d.fold[gs] = int((na & 1023) | ((nb & 1023) << 10) | ((nc & 1023) << 20));
       } else {
-        const int w = d.fold[gs];
-        na = (w << 22) >> 22;
-        nb = (w << 12) >> 22;
-        nc = (w << 2) >> 22;
+        unpack_fold(d.fold[gs], na, nb, nc);
       }
-      const long long x = d.px[a] - na * S.box_fx[0] - nb * S.box_fx[3] - nc * S.box_fx[6];
-      const long long y = d.py[a] - nb * S.box_fx[4] - nc * S.box_fx[7];
-      const long long z = d.pz[a] - nc * S.box_fx[8];
-      p = make_int4(to_pair_coordinate(x, S.pc_shift), to_pair_coordinate(y, S.pc_shift),
-                    to_pair_coordinate(z, S.pc_shift), 0);
+      p = pair_coordinate(S, d.px[a], d.py[a], d.pz[a], na, nb, nc);
     }
     d.pc[gs] = p;
     if (d.inner && (d.rebuild_now[s] || d.prune_now[s])) {
@@ -894,15 +882,17 @@ __device__ bool grid_barrier(unsigned int* bar, int* err) {
   return ok != 0;
 }
 
-// One launch per step.  With no rebuild requested it only folds the pair
-// coordinates; otherwise it runs the sort and tile-list phases with a grid
-// barrier between them.
+// One launch per step.  With no rebuild requested it returns at once, or folds
+// the pair coordinates when a prune is due; otherwise it runs the sort and
+// tile-list phases with a grid barrier between them.
 template <int C>
 __global__ void __launch_bounds__(kThreads) k_list(Dev d) {
   const bool rebuild = *d.any_rebuild != 0;
   int* err = d.err;  // system 0's word carries a barrier timeout
   if (!rebuild) {
-    phase_wrap(d);
+    // the integrator wrote this step's pair coordinates; the wrap runs again
+    // only for a prune, which needs reference positions and cluster boxes
+    if (*d.any_prune) phase_wrap(d);
     return;
   }
   phase_cells_clear(d);
@@ -950,11 +940,16 @@ MDB_PHASE_KERNEL(cells_assign, true)
 MDB_PHASE_KERNEL(cells_scan, true)
 MDB_PHASE_KERNEL(cells_scatter, true)
 MDB_PHASE_KERNEL(cells_order, true)
-MDB_PHASE_KERNEL(wrap, false)
 MDB_PHASE_KERNEL(tiles_scan, true)
 MDB_PHASE_KERNEL(tiles_rescan, true)
 MDB_PHASE_KERNEL(tiles_finish, true)
 #undef MDB_PHASE_KERNEL
+// the wrap, when a rebuild or a prune is due (otherwise the integrator wrote
+// the pair coordinates at the end of the previous step)
+__global__ void __launch_bounds__(kThreads) k_wrap(Dev d) {
+  if (!*d.any_rebuild && !*d.any_prune) return;
+  phase_wrap(d);
+}
 // The inner list, its own launch after the list kernels (a full grid, where
 // the cooperative list kernel has two blocks per SM): nothing to do unless a
 // system rebuilt or is due a prune.  The last block to finish writes the

@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   const float dt = R.dt;
   const bool lfm = R.integrator == 0;
 
-  int atom[kPerThread];
+  int atom[kPerThread], slot[kPerThread], fw[kPerThread];
   long long px[kPerThread], py[kPerThread], pz[kPerThread];
   float vx[kPerThread], vy[kPerThread], vz[kPerThread], rx[kPerThread], ry[kPerThread], rz[kPerThread];
   float im[kPerThread], n0[kPerThread], n1[kPerThread], n2[kPerThread];
@@ -546,6 +546,8 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
     rx[j] = d.rx[a]; ry[j] = d.ry[a]; rz[j] = d.rz[a];
     im[j] = d.invm[a];
     const int gs = S.slot_off + d.rank[a];
+    slot[j] = gs;
+    fw[j] = d.fold[gs];
     const float fx = from_fixed(static_cast<long long>(d.fx[gs]));
     const float fy = from_fixed(static_cast<long long>(d.fy[gs]));
     const float fz = from_fixed(static_cast<long long>(d.fz[gs]));
@@ -641,6 +643,13 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
       bad |= !isfinite(vx[j] + vy[j] + vz[j]);
     } else if (com) {
       d.vx[a] = vx[j]; d.vy[a] = vy[j]; d.vz[a] = vz[j];
+    }
+    {
+      // the next step's pair coordinates under this list's fold, so the list
+      // kernel need not wrap again unless a rebuild or a prune is due
+      long long na, nb, nc;
+      unpack_fold(fw[j], na, nb, nc);
+      d.pc[slot[j]] = pair_coordinate(S, px[j], py[j], pz[j], na, nb, nc);
     }
     const float ex = from_fixed(px[j] - d.refx[a]), ey = from_fixed(py[j] - d.refy[a]),
                 ez = from_fixed(pz[j] - d.refz[a]);
