@@ -130,3 +130,74 @@ def test_node_addon_exports_what_the_typescript_shim_calls():
     called = set(re.findall(r"\b(mdb_[a-z_]+)\(", cc))
     declared = set(re.findall(r"\b(mdb_[a-z_]+)\(", header))
     assert called <= declared, called - declared
+
+
+C_CLIENT = r"""
+#include <stdio.h>
+#include <string.h>
+#include "mdb.h"
+
+/* A C caller of the library: version, argument checks, and one engine whose
+   creation must stop at the device check on a machine without a GPU. */
+int main(void) {
+  if (mdb_abi_version() != MDB_ABI_VERSION) return 1;
+  mdb_engine* e = NULL;
+  if (mdb_create(NULL, NULL, NULL, &e) != MDB_ERR_INVALID_ARGUMENT) return 2;
+  static const double masses[3] = {15.99943, 1.007947, 1.007947};
+  static const double pos[9] = {1.0, 1.0, 1.0, 1.09572, 1.0, 1.0, 0.97600, 1.09267, 1.0};
+  mdb_system_desc sys;
+  memset(&sys, 0, sizeof sys);
+  sys.n_particles = 3;
+  sys.masses = masses;
+  sys.box[0] = sys.box[4] = sys.box[8] = 3.0;
+  mdb_state_desc st;
+  memset(&st, 0, sizeof st);
+  st.positions = pos;
+  st.box[0] = st.box[4] = st.box[8] = 3.0;
+  mdb_run_options opt;
+  memset(&opt, 0, sizeof opt);
+  int rc = mdb_create(&sys, &st, &opt, &e); /* time step 0 */
+  printf("%d %s\n", rc, mdb_last_error(e));
+  if (rc != MDB_ERR_INVALID_ARGUMENT) return 3;
+  mdb_destroy(e, NULL);
+  e = NULL;
+  opt.time_step = 0.002;
+  opt.temperature = 300.0;
+  opt.friction = 1.0;
+  rc = mdb_create(&sys, &st, &opt, &e);
+  printf("%d %s\n", rc, mdb_last_error(e));
+  int64_t leaked = -1;
+  if (e && mdb_destroy(e, &leaked) != MDB_OK) return 4;
+  if (leaked != 0) return 5;
+  return rc == MDB_ERR_NO_DEVICE ? 0 : rc == MDB_OK ? 7 : 6;
+}
+"""
+
+
+def test_a_c_program_links_the_library(tmp_path):
+    """The header is plain C11 (warnings are errors) and a C program links
+    libmdb200.so and gets the documented status codes.  Without a GPU the
+    engine stops at the device check; with one it is created and destroyed
+    (the GPU tests are the ones that run engines)."""
+    import shutil
+    import subprocess
+
+    from mdb200 import abi
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    lib_path = abi.LIBRARY_PATH
+    if not lib_path.exists():
+        pytest.skip("library not built")
+    src = tmp_path / "client.c"
+    src.write_text(C_CLIENT)
+    exe = tmp_path / "client"
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"), str(src),
+                    "-L", str(lib_path.parent), "-lmdb200", f"-Wl,-rpath,{lib_path.parent}", "-o", str(exe)],
+                   check=True)
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    if run.returncode == 7:
+        pytest.skip("a device is visible: the engine was created")
+    assert run.returncode == 0, (run.returncode, run.stdout)
+    assert "time_step must be positive" in run.stdout
+    assert "no CUDA device is visible" in run.stdout
