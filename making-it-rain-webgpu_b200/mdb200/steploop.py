@@ -293,6 +293,21 @@ class StepLoop:
                       potential_energy=energies["potential"], kinetic_energy=energies["kinetic"],
                       temperature=energies["temperature"], energies=energies)
 
+    def shifted_kinetic_energy(self, system: int = 0) -> float:
+        """The shifted kinetic energy `StepLoop.report()` carries (loop.ts:788-803):
+        the velocities advanced half a step with the forces at the current
+        coordinates and re-constrained, kJ/mol; potential plus this is the
+        total a leapfrog integrator conserves."""
+        from . import velocities as vel
+
+        _, forces = self.evaluate(system)
+        return vel.shifted_kinetic_energy(self._systems[system], self.positions(system), self.velocities(system),
+                                          forces, 0.5 * self._options.time_step)
+
+    def box_lengths(self, system: int = 0) -> np.ndarray:
+        """`StepLoop.boxLengths`, loop.ts:995: the box's diagonal, nm."""
+        return np.diag(self.box_vectors(system)).copy()
+
     # ---- statistics -----------------------------------------------------------
     def barostat_statistics(self, system: int = 0) -> dict:
         s = abi.BarostatStats()

@@ -113,3 +113,32 @@ def velocities_at_temperature(system: System, positions: np.ndarray, temperature
         f = np.asarray(forces, dtype=np.float64).reshape(-1, 3)
         v[moving] -= (time_offset / m[moving])[:, None] * f[moving]
     return constrain_velocities(system, positions, v, VELOCITY_CONSTRAINT_TOLERANCE)
+
+
+# the tolerance OpenMM re-constrains shifted velocities to (src/reference/kinetic.ts:28)
+SHIFTED_VELOCITY_TOLERANCE = 1e-4
+
+
+def kinetic_energy(system: System, velocities: np.ndarray) -> float:
+    """(1/2) sum m v^2 over the moving particles (kinetic.ts:31), kJ/mol."""
+    m = np.asarray(system.masses, dtype=np.float64)
+    v = np.asarray(velocities, dtype=np.float64).reshape(-1, 3)
+    moving = m > 0
+    return 0.5 * float(np.sum(m[moving, None] * v[moving] * v[moving]))
+
+
+def shifted_kinetic_energy(system: System, positions: np.ndarray, velocities: np.ndarray, forces: np.ndarray,
+                           time_shift: float, tolerance: float = SHIFTED_VELOCITY_TOLERANCE) -> float:
+    """`shiftedKineticEnergy` (kinetic.ts:87): the kinetic energy of the
+    velocities advanced by `time_shift` (v + time_shift F / m) and projected
+    back onto the constraints; a zero shift is the plain kinetic energy.  With
+    time_shift = dt / 2 this is the kinetic energy a leapfrog integrator's
+    conserved total needs, which `StepLoop.report` carries."""
+    if time_shift == 0:
+        return kinetic_energy(system, velocities)
+    m = np.asarray(system.masses, dtype=np.float64)
+    v = np.array(velocities, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(forces, dtype=np.float64).reshape(-1, 3)
+    moving = m > 0
+    v[moving] += f[moving] * (time_shift / m[moving])[:, None]
+    return kinetic_energy(system, constrain_velocities(system, positions, v, tolerance))

@@ -380,6 +380,29 @@ napi_value Neighbours(napi_env env, napi_callback_info info) {
   return obj;
 }
 
+// memory(handle): {count, totalBytes}, the engine's device allocations for
+// `report_pool()` (every allocation is a named one; there is no scratch pool).
+napi_value Memory(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  int64_t total = 0;
+  const int status = mdb_memory_report(e, nullptr, 0, &total);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  std::vector<char> text(1 << 16);
+  mdb_memory_report(e, text.data(), int64_t(text.size()), nullptr);
+  int64_t count = 0;
+  for (const char* c = text.data(); *c; ++c) count += *c == ';';
+  napi_value obj, v;
+  napi_create_object(env, &obj);
+  napi_create_int64(env, count, &v);
+  napi_set_named_property(env, obj, "count", v);
+  napi_create_int64(env, total, &v);
+  napi_set_named_property(env, obj, "totalBytes", v);
+  return obj;
+}
+
 napi_value Destroy(napi_env env, napi_callback_info info) {
   size_t argc = 1;
   napi_value argv[1];
@@ -410,6 +433,7 @@ napi_value Init(napi_env env, napi_value exports) {
       {"step", nullptr, Step, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"barostat", nullptr, Barostat, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"neighbours", nullptr, Neighbours, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"memory", nullptr, Memory, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"destroy", nullptr, Destroy, nullptr, nullptr, nullptr, napi_default, nullptr},
   };
   napi_define_properties(env, exports, sizeof(props) / sizeof(props[0]), props);

@@ -12,9 +12,13 @@
  * the same C ABI in the tests.
  */
 
+import { parseState } from "../../src/engine/state.js";
 import type { OpenMMState } from "../../src/engine/state.js";
+import { parseSystem } from "../../src/engine/system.js";
 import type { OpenMMSystem } from "../../src/engine/system.js";
+import type { PoolReport } from "../../src/gpu/allocator.js";
 import type { RunOptions, Report } from "../../src/gpu/loop.js";
+import { kineticEnergy, shiftedKineticEnergy } from "../../src/reference/kinetic.js";
 
 // eslint-disable-next-line @typescript-eslint/no-require-imports
 const addon = require("./build/Release/mdb200.node") as MdbAddon;
@@ -46,6 +50,7 @@ interface MdbAddon {
   step(handle: unknown): number;
   barostat(handle: unknown): { attempts: number; accepted: number; volumeScale: number };
   neighbours(handle: unknown): { rebuilds: number; tiles: number; overflowed: boolean };
+  memory(handle: unknown): { count: number; totalBytes: number };
   destroy(handle: unknown): { leaked: number };
 }
 
@@ -53,8 +58,17 @@ export class StepLoop {
   private constructor(
     private readonly handle: unknown,
     private readonly system: OpenMMSystem,
-    private readonly options: RunOptions,
+    readonly options: RunOptions,
   ) {}
+
+  /** `StepLoop.create`, loop.ts:268: parse the System and State XML, then `fromParsed`. */
+  static async create(
+    device: unknown,
+    texts: { readonly systemXml: string; readonly stateXml: string },
+    options: RunOptions,
+  ): Promise<StepLoop> {
+    return StepLoop.fromParsed(device, parseSystem(texts.systemXml), parseState(texts.stateXml), options);
+  }
 
   /** `StepLoop.fromParsed`, loop.ts:278.  The GPU device is chosen by `options`. */
   static async fromParsed(
@@ -82,16 +96,32 @@ export class StepLoop {
     if (steps > 0) addon.run(this.handle, steps);
   }
 
+  /** `StepLoop.evaluateForces`, loop.ts:924: one force evaluation at the current coordinates, no step. */
+  async evaluateForces(): Promise<void> {
+    addon.evaluate(this.handle, null);
+  }
+
+  /**
+   * `StepLoop.report`, loop.ts:761: the potential at the current coordinates,
+   * the kinetic energy as the velocities stand, and the shifted kinetic energy
+   * (velocities advanced half a step and re-constrained) through the
+   * reference's own host function, as its report computes it.
+   */
   async report(): Promise<Report> {
-    const e = addon.evaluate(this.handle, null);
+    const forces = new Float64Array(this.system.particleCount * 3);
+    const e = addon.evaluate(this.handle, forces);
+    const positions = await this.positions();
+    const velocities = await this.velocities();
+    const unshifted = kineticEnergy(this.system, velocities);
+    const shifted = shiftedKineticEnergy(this.system, positions, velocities, forces, 0.5 * this.options.timeStep);
     const step = this.steps;
     return {
       step,
       time: step * this.options.timeStep,
       potentialEnergy: e.potential,
-      kineticEnergy: e.kinetic,
-      shiftedKineticEnergy: e.kinetic,
-      totalEnergy: e.potential + e.kinetic,
+      kineticEnergy: unshifted,
+      shiftedKineticEnergy: shifted,
+      totalEnergy: e.potential + shifted,
       temperature: e.temperature,
     };
   }
@@ -137,6 +167,12 @@ export class StepLoop {
     return [m[0] as number, m[1] as number, m[2] as number];
   }
 
+  /** `StepLoop.boxLengths`, loop.ts:995: the box's diagonal (its product is the volume). */
+  get boxLengths(): Vec3 {
+    const b = this.boxVectorsNow;
+    return [b[0][0], b[1][1], b[2][2]];
+  }
+
   get boxVectorsNow(): [Vec3, Vec3, Vec3] {
     const b = addon.box(this.handle);
     return [
@@ -152,6 +188,24 @@ export class StepLoop {
 
   async verletFlags() {
     return addon.neighbours(this.handle);
+  }
+
+  /**
+   * `StepLoop.report_pool`, loop.ts:1109: the engine's device allocations.
+   * Every allocation is a named one made when the engine is built; there is
+   * no scratch pool and nothing is leased.
+   */
+  report_pool(): PoolReport {
+    const m = addon.memory(this.handle);
+    return {
+      namedCount: m.count,
+      namedBytes: m.totalBytes,
+      scratchCount: 0,
+      scratchBytes: 0,
+      totalBytes: m.totalBytes,
+      peakBytes: m.totalBytes,
+      outstandingLeases: 0,
+    };
   }
 
   destroy(): { leaked: number } {

@@ -62,6 +62,34 @@ def test_the_draw_is_maxwell_boltzmann_and_shifted_by_half_a_step():
         velocities.velocities_at_temperature(system, pos, 300.0, 3, time_offset=0.001)
 
 
+def test_shifted_kinetic_energy_matches_the_oracle_projection(oracle):
+    """The report's shifted kinetic energy (kinetic.ts:87): velocities
+    advanced by dt/2 with the forces, re-constrained, then (1/2) sum m v^2 --
+    against the same shift projected by the oracle's constraint solve."""
+    from mdb200 import synth
+
+    system, state = synth.water_box(n_waters=300, width=2.1, seed=5)
+    rng = np.random.default_rng(3)
+    v = velocities.velocities_at_temperature(system, state.positions, 300.0, 7, time_offset=0.0)
+    forces = rng.normal(0.0, 800.0, v.shape)
+    m = np.asarray(system.masses)
+    shifted = v + (0.001 / m)[:, None] * forces
+    flat = np.ascontiguousarray(shifted.reshape(-1))
+    pos = np.ascontiguousarray(np.asarray(state.positions, dtype=np.float64).reshape(-1))
+    assert oracle.lib().orc_constrain_velocities(system.desc().pointer(), oracle._p(pos), oracle._p(flat),
+                                                 1e-10) == 0
+    want = oracle.kinetic_energy(system, flat)
+    got = velocities.shifted_kinetic_energy(system, state.positions, v, forces, 0.001, tolerance=1e-10)
+    assert abs(got - want) <= 1e-8 * want, (got, want)
+    loose = velocities.shifted_kinetic_energy(system, state.positions, v, forces, 0.001)
+    assert abs(loose - want) <= 1e-4 * want, (loose, want)
+    # the shift moves energy: the unshifted and shifted values differ, and a zero shift is the plain sum
+    assert abs(velocities.kinetic_energy(system, v) - want) > 1e-3 * want
+    assert velocities.shifted_kinetic_energy(system, state.positions, v, forces, 0.0) == \
+        velocities.kinetic_energy(system, v)
+    assert abs(velocities.kinetic_energy(system, v) - oracle.kinetic_energy(system, v)) <= 1e-12 * want
+
+
 def test_dcd_layout_and_round_trip():
     buf = io.BytesIO()
     w = reporters.DcdWriter(buf, 37, time_step=0.002, first_step=100, interval=50)
