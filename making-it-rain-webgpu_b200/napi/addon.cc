@@ -40,6 +40,14 @@ napi_value throw_status(napi_env env, int status, mdb_engine* e) {
   return nullptr;
 }
 
+napi_value throw_message(napi_env env, const std::string& msg) {
+  napi_value message, error;
+  napi_create_string_utf8(env, msg.c_str(), NAPI_AUTO_LENGTH, &message);
+  napi_create_error(env, nullptr, message, &error);
+  napi_throw(env, error);
+  return nullptr;
+}
+
 mdb_engine* engine_of(napi_env env, napi_value v) {
   void* p = nullptr;
   napi_get_value_external(env, v, &p);
@@ -178,6 +186,33 @@ napi_value Create(napi_env env, napi_callback_info info) {
   o.seed = uint32_t(number(env, argv[2], "seed", 0));
   o.verlet_skin = number(env, argv[2], "verletSkin", -1);
   o.max_batch = int32_t(number(env, argv[2], "maxBatch", 100));
+  // RunOptions.integrator, "lfmiddle" or "verlet" (loop.ts:127)
+  o.integrator = MDB_INTEGRATOR_LFMIDDLE;
+  bool has_integrator = false;
+  napi_has_named_property(env, argv[2], "integrator", &has_integrator);
+  if (has_integrator) {
+    char name[32] = {0};
+    size_t len = 0;
+    napi_get_value_string_utf8(env, property(env, argv[2], "integrator"), name, sizeof(name), &len);
+    if (std::strcmp(name, "verlet") == 0) o.integrator = MDB_INTEGRATOR_VERLET;
+    else if (std::strcmp(name, "lfmiddle") != 0)
+      return throw_message(env, std::string("unknown integrator '") + name + "': expected lfmiddle or verlet");
+  }
+  // RunOptions.mesh, a pinned [x, y, z] PME mesh (loop.ts:167); absent = by rule
+  bool has_mesh = false;
+  napi_has_named_property(env, argv[2], "mesh", &has_mesh);
+  if (has_mesh) {
+    napi_value m = property(env, argv[2], "mesh");
+    uint32_t len = 0;
+    if (napi_get_array_length(env, m, &len) == napi_ok)
+      for (uint32_t k = 0; k < 3 && k < len; ++k) {
+        napi_value x;
+        double v = 0;
+        napi_get_element(env, m, k, &x);
+        napi_get_value_double(env, x, &v);
+        o.mesh[k] = int32_t(v);
+      }
+  }
   mdb_engine* e = nullptr;
   const int status = mdb_create(&sys, &st, &o, &e);
   if (status != MDB_OK) {
