@@ -75,6 +75,28 @@ double number(napi_env env, napi_value obj, const char* key, double fallback) {
   return out;
 }
 
+// A boolean member (or a number, non-zero = true); `fallback` when absent.
+bool flag(napi_env env, napi_value obj, const char* key, bool fallback) {
+  bool has = false;
+  napi_has_named_property(env, obj, key, &has);
+  if (!has) return fallback;
+  napi_value v;
+  napi_get_named_property(env, obj, key, &v);
+  napi_valuetype t;
+  napi_typeof(env, v, &t);
+  if (t == napi_boolean) {
+    bool out = fallback;
+    napi_get_value_bool(env, v, &out);
+    return out;
+  }
+  if (t == napi_number) {
+    double out = fallback ? 1.0 : 0.0;
+    napi_get_value_double(env, v, &out);
+    return out != 0.0;
+  }
+  return fallback;
+}
+
 napi_value property(napi_env env, napi_value obj, const char* key) {
   napi_value v = nullptr;
   napi_get_named_property(env, obj, key, &v);
@@ -82,8 +104,11 @@ napi_value property(napi_env env, napi_value obj, const char* key) {
 }
 
 // OpenMMSystem (src/engine/system.ts:161) -> mdb_system_desc.  The typed
-// arrays are borrowed for the duration of the create call only.
-bool fill_system(napi_env env, napi_value sys, mdb_system_desc* d, std::vector<double>& box) {
+// arrays are borrowed for the duration of the create call only.  A force type
+// the engine does not implement is refused by name (`unsupported` holds it),
+// as the reference's parser refuses it, rather than dropped.
+bool fill_system(napi_env env, napi_value sys, mdb_system_desc* d, std::vector<double>& box,
+                 std::string& unsupported) {
   std::memset(d, 0, sizeof(*d));
   size_t n = 0;
   d->masses = typed_array<double>(env, property(env, sys, "masses"), &n);
@@ -118,7 +143,7 @@ bool fill_system(napi_env env, napi_value sys, mdb_system_desc* d, std::vector<d
       d->cutoff = number(env, f, "cutoff", 1.0);
       d->ewald_tolerance = number(env, f, "ewaldTolerance", 5e-4);
       d->alpha = number(env, f, "alpha", 0);
-      d->use_dispersion_correction = number(env, f, "useDispersionCorrection", 1) != 0;
+      d->use_dispersion_correction = flag(env, f, "useDispersionCorrection", true) ? 1 : 0;
       d->charge = typed_array<double>(env, property(env, f, "charge"), &m);
       d->sigma = typed_array<double>(env, property(env, f, "sigma"), &m);
       d->epsilon = typed_array<double>(env, property(env, f, "epsilon"), &m);
@@ -156,6 +181,17 @@ bool fill_system(napi_env env, napi_value sys, mdb_system_desc* d, std::vector<d
       d->barostat_frequency = int32_t(number(env, f, "frequency", 25));
       d->barostat_pressure = number(env, f, "defaultPressure", 1);
       d->barostat_temperature = number(env, f, "defaultTemperature", 300);
+    } else if (!std::strcmp(type, "PositionRestraint")) {
+      // k*periodicdistance(x,y,z,x0,y0,z0)^2 per particle (system.ts:139-150)
+      d->restraint_particle = typed_array<int32_t>(env, property(env, f, "particle"), &m);
+      d->n_restraints = int32_t(m);
+      d->restraint_k = typed_array<double>(env, property(env, f, "k"), &m);
+      d->restraint_x0 = typed_array<double>(env, property(env, f, "x0"), &m);
+      d->restraint_y0 = typed_array<double>(env, property(env, f, "y0"), &m);
+      d->restraint_z0 = typed_array<double>(env, property(env, f, "z0"), &m);
+    } else {
+      unsupported = type;
+      return false;
     }
   }
   (void)box;
@@ -168,7 +204,18 @@ napi_value Create(napi_env env, napi_callback_info info) {
   napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
   mdb_system_desc sys;
   std::vector<double> box;
-  if (!fill_system(env, argv[0], &sys, box)) return throw_status(env, MDB_ERR_INVALID_ARGUMENT, nullptr);
+  std::string unsupported;
+  if (!fill_system(env, argv[0], &sys, box, unsupported)) {
+    if (unsupported.empty()) return throw_status(env, MDB_ERR_INVALID_ARGUMENT, nullptr);
+    napi_value message, error, name;
+    const std::string text = unsupported + " is not implemented by this engine";
+    napi_create_string_utf8(env, text.c_str(), NAPI_AUTO_LENGTH, &message);
+    napi_create_error(env, nullptr, message, &error);
+    napi_create_string_utf8(env, "UnsupportedForce", NAPI_AUTO_LENGTH, &name);
+    napi_set_named_property(env, error, "name", name);
+    napi_throw(env, error);
+    return nullptr;
+  }
   mdb_state_desc st;
   std::memset(&st, 0, sizeof(st));
   size_t n = 0;
