@@ -103,6 +103,27 @@ napi_value property(napi_env env, napi_value obj, const char* key) {
   return v;
 }
 
+// `boxVectors` ([a, b, c] rows, nm) of a System or a State into `out`; false
+// when the object has none.
+bool read_box(napi_env env, napi_value obj, double* out) {
+  bool has = false;
+  napi_has_named_property(env, obj, "boxVectors", &has);
+  if (!has) return false;
+  napi_value bv = property(env, obj, "boxVectors");
+  uint32_t rows = 0;
+  if (napi_get_array_length(env, bv, &rows) != napi_ok || rows != 3) return false;
+  for (uint32_t r = 0; r < 3; ++r) {
+    napi_value row;
+    napi_get_element(env, bv, r, &row);
+    for (uint32_t c = 0; c < 3; ++c) {
+      napi_value x;
+      napi_get_element(env, row, c, &x);
+      napi_get_value_double(env, x, &out[r * 3 + c]);
+    }
+  }
+  return true;
+}
+
 // OpenMMSystem (src/engine/system.ts:161) -> mdb_system_desc.  The typed
 // arrays are borrowed for the duration of the create call only.  A force type
 // the engine does not implement is refused by name (`unsupported` holds it),
@@ -113,16 +134,7 @@ bool fill_system(napi_env env, napi_value sys, mdb_system_desc* d, std::vector<d
   size_t n = 0;
   d->masses = typed_array<double>(env, property(env, sys, "masses"), &n);
   d->n_particles = int32_t(n);
-  napi_value bv = property(env, sys, "boxVectors");
-  for (uint32_t r = 0; r < 3; ++r) {
-    napi_value row;
-    napi_get_element(env, bv, r, &row);
-    for (uint32_t c = 0; c < 3; ++c) {
-      napi_value x;
-      napi_get_element(env, row, c, &x);
-      napi_get_value_double(env, x, &d->box[r * 3 + c]);
-    }
-  }
+  read_box(env, sys, d->box);
   size_t nc = 0;
   d->constraint_p1 = typed_array<int32_t>(env, property(env, sys, "constraintP1"), &nc);
   d->constraint_p2 = typed_array<int32_t>(env, property(env, sys, "constraintP2"), &nc);
@@ -223,7 +235,8 @@ napi_value Create(napi_env env, napi_callback_info info) {
   bool has_v = false;
   napi_has_named_property(env, argv[1], "velocities", &has_v);
   if (has_v) st.velocities = typed_array<double>(env, property(env, argv[1], "velocities"), &n);
-  std::memcpy(st.box, sys.box, sizeof(st.box));
+  // the run's box is the State's (loop.ts:295), the System's default otherwise
+  if (!read_box(env, argv[1], st.box)) std::memcpy(st.box, sys.box, sizeof(st.box));
   mdb_run_options o;
   std::memset(&o, 0, sizeof(o));
   o.time_step = number(env, argv[2], "timeStep", 0.002);
