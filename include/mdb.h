@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MDB_ABI_VERSION 1
+#define MDB_ABI_VERSION 2
 
 typedef enum mdb_status {
   MDB_OK = 0,
@@ -281,6 +281,7 @@ typedef struct mdb_neighbour_stats {
   int64_t inner_tiles;    /* tiles of the inner list the pair kernel reads (= tiles without one) */
   int64_t prunes;         /* inner-list prunes between rebuilds since creation */
   double inner_skin;      /* nm; 0 without an inner list */
+  int32_t tile_atoms;     /* atoms per cluster: 8 (8x8 tiles) or 32 (32x32 tiles) */
 } mdb_neighbour_stats;
 
 typedef struct mdb_engine mdb_engine;

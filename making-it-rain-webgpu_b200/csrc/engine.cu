@@ -1565,6 +1565,7 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   out->inner_tiles = tiles;
   out->prunes = 0;
   out->inner_skin = 0;
+  out->tile_atoms = e->cluster;
   if (e->d.inner) {
     int inner = 0;
     long long prunes = 0;

@@ -14,7 +14,7 @@ from pathlib import Path
 PACKAGE_ROOT = Path(__file__).resolve().parent.parent
 LIBRARY_PATH = PACKAGE_ROOT / "lib" / "libmdb200.so"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # mdb_status
 OK = 0
@@ -227,6 +227,7 @@ class NeighbourStats(C.Structure):
         ("inner_tiles", C.c_int64),
         ("prunes", C.c_int64),
         ("inner_skin", C.c_double),
+        ("tile_atoms", C.c_int32),
     ]
 
 

@@ -324,7 +324,8 @@ class StepLoop:
         self._check(self._lib.mdb_get_neighbour_stats(self._handle, system, C.byref(s)))
         return {"rebuilds": s.rebuilds, "tiles": s.tiles, "tileCapacity": s.tile_capacity,
                 "blocks": s.blocks, "overflowed": bool(s.overflowed), "skin": s.skin,
-                "innerTiles": s.inner_tiles, "prunes": s.prunes, "innerSkin": s.inner_skin}
+                "innerTiles": s.inner_tiles, "prunes": s.prunes, "innerSkin": s.inner_skin,
+                "tileAtoms": s.tile_atoms}
 
     def profile_step(self, repeats: int = 20) -> dict:
         """`StepLoop.profileStep`, loop.ts:705: device ms per stage.  Advances the system."""

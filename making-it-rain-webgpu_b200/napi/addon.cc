@@ -455,7 +455,9 @@ napi_value Barostat(napi_env env, napi_callback_info info) {
   return obj;
 }
 
-// neighbours(handle): {rebuilds, tiles, overflowed}, verletFlags' fields.
+// neighbours(handle): verletFlags' fields (loop.ts:941) -- rebuilds,
+// overflowed, capacity (tiles), skin (nm), byteLength (of the tile list) --
+// plus the tile counts of the outer and inner lists and the prune count.
 napi_value Neighbours(napi_env env, napi_callback_info info) {
   size_t argc = 1;
   napi_value argv[1];
@@ -472,6 +474,17 @@ napi_value Neighbours(napi_env env, napi_callback_info info) {
   napi_set_named_property(env, obj, "tiles", v);
   napi_get_boolean(env, ns.overflowed != 0, &v);
   napi_set_named_property(env, obj, "overflowed", v);
+  napi_create_int64(env, ns.tile_capacity, &v);
+  napi_set_named_property(env, obj, "capacity", v);
+  napi_create_double(env, ns.skin, &v);
+  napi_set_named_property(env, obj, "skin", v);
+  // a tile is its cluster pair (8 B), image shift (16 B) and interaction mask
+  napi_create_int64(env, ns.tile_capacity * (24 + int64_t(ns.tile_atoms) * ns.tile_atoms / 8), &v);
+  napi_set_named_property(env, obj, "byteLength", v);
+  napi_create_int64(env, ns.inner_tiles, &v);
+  napi_set_named_property(env, obj, "innerTiles", v);
+  napi_create_int64(env, ns.prunes, &v);
+  napi_set_named_property(env, obj, "prunes", v);
   return obj;
 }
 

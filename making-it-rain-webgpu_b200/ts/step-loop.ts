@@ -49,7 +49,16 @@ interface MdbAddon {
   setStep(handle: unknown, step: number): void;
   step(handle: unknown): number;
   barostat(handle: unknown): { attempts: number; accepted: number; volumeScale: number };
-  neighbours(handle: unknown): { rebuilds: number; tiles: number; overflowed: boolean };
+  neighbours(handle: unknown): {
+    rebuilds: number;
+    tiles: number;
+    overflowed: boolean;
+    capacity: number;
+    skin: number;
+    byteLength: number;
+    innerTiles: number;
+    prunes: number;
+  };
   memory(handle: unknown): { count: number; totalBytes: number };
   destroy(handle: unknown): { leaked: number };
 }
@@ -182,12 +191,34 @@ export class StepLoop {
     ];
   }
 
-  get barostatStatistics() {
+  /** `StepLoop.barostatStatistics`, loop.ts:572: null when the System has no MonteCarloBarostat. */
+  get barostatStatistics(): { attempts: number; accepted: number; volumeScale: number } | null {
+    if (!this.system.forces.some((f) => f.type === "MonteCarloBarostat")) return null;
     return addon.barostat(this.handle);
   }
 
-  async verletFlags() {
-    return addon.neighbours(this.handle);
+  /**
+   * `StepLoop.verletFlags`, loop.ts:941.  `worstDisplacement` is NaN: the
+   * engine tests each atom's displacement against half the skin on the device
+   * and keeps no maximum.  `capacity` counts cluster-pair tiles.
+   */
+  async verletFlags(): Promise<{
+    readonly rebuilds: number;
+    readonly worstDisplacement: number;
+    readonly overflowed: boolean;
+    readonly capacity: number;
+    readonly skin: number;
+    readonly byteLength: number;
+  }> {
+    const n = addon.neighbours(this.handle);
+    return {
+      rebuilds: n.rebuilds,
+      worstDisplacement: Number.NaN,
+      overflowed: n.overflowed,
+      capacity: n.capacity,
+      skin: n.skin,
+      byteLength: n.byteLength,
+    };
   }
 
   /**
