@@ -357,18 +357,19 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     }
     e->opt.tuning = nullptr;  // the caller's array is not kept
   }
-  int count = 0;
-  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
-    return fail(e, MDB_ERR_NO_DEVICE, "no CUDA device is visible");
-  e->device = e->opt.device;
-  CUDA_TRY(e, cudaSetDevice(e->device));
-
+  // the systems are checked on the host first, so a caller learns what is
+  // wrong with its input (the reference's named errors) on any machine
   e->hs.resize(n);
   for (int s = 0; s < n; ++s) {
     std::string msg;
     const int st = prepare_system(systems[s], states[s], e->opt, e->hs[s], msg);
     if (st) return fail(e, st, n > 1 ? "system " + std::to_string(s) + ": " + msg : msg);
   }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(e, MDB_ERR_NO_DEVICE, "no CUDA device is visible");
+  e->device = e->opt.device;
+  CUDA_TRY(e, cudaSetDevice(e->device));
   // run options (integrate.ts:170 packStepParams)
   RunDev& R = e->run;
   R.dt = float(e->opt.time_step);

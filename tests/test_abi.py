@@ -137,7 +137,8 @@ C_CLIENT = r"""
 #include <string.h>
 #include "mdb.h"
 
-/* A C caller of the library: version, argument checks, and one engine whose
+/* A C caller of the library: version, argument checks, the reference's named
+   errors (found on the host, before any device work), and one engine whose
    creation must stop at the device check on a machine without a GPU. */
 int main(void) {
   if (mdb_abi_version() != MDB_ABI_VERSION) return 1;
@@ -145,6 +146,10 @@ int main(void) {
   if (mdb_create(NULL, NULL, NULL, &e) != MDB_ERR_INVALID_ARGUMENT) return 2;
   static const double masses[3] = {15.99943, 1.007947, 1.007947};
   static const double pos[9] = {1.0, 1.0, 1.0, 1.09572, 1.0, 1.0, 0.97600, 1.09267, 1.0};
+  static const double charge[3] = {-0.834, 0.417, 0.417}, sigma[3] = {0.315, 1.0, 1.0},
+                      epsilon[3] = {0.636, 0.0, 0.0};
+  static const int32_t ex1[3] = {0, 0, 1}, ex2[3] = {1, 2, 2};
+  static const double exq[3] = {0.0, 0.0, 0.0}, exs[3] = {1.0, 1.0, 1.0}, exe[3] = {0.0, 0.0, 0.0};
   mdb_system_desc sys;
   memset(&sys, 0, sizeof sys);
   sys.n_particles = 3;
@@ -160,10 +165,38 @@ int main(void) {
   printf("%d %s\n", rc, mdb_last_error(e));
   if (rc != MDB_ERR_INVALID_ARGUMENT) return 3;
   mdb_destroy(e, NULL);
-  e = NULL;
   opt.time_step = 0.002;
   opt.temperature = 300.0;
   opt.friction = 1.0;
+  rc = mdb_create(&sys, &st, &opt, &e); /* no NonbondedForce */
+  printf("%d %s\n", rc, mdb_last_error(e));
+  if (rc != MDB_ERR_UNSUPPORTED_FORCE) return 8;
+  mdb_destroy(e, NULL);
+  sys.has_nonbonded = 1;
+  sys.cutoff = 1.6; /* more than half the 3 nm box */
+  sys.ewald_tolerance = 5e-4;
+  sys.use_dispersion_correction = 1;
+  sys.charge = charge;
+  sys.sigma = sigma;
+  sys.epsilon = epsilon;
+  sys.n_exceptions = 3;
+  sys.exception_p1 = ex1;
+  sys.exception_p2 = ex2;
+  sys.exception_charge_prod = exq;
+  sys.exception_sigma = exs;
+  sys.exception_epsilon = exe;
+  rc = mdb_create(&sys, &st, &opt, &e);
+  printf("%d %s\n", rc, mdb_last_error(e));
+  if (rc != MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX) return 9;
+  mdb_destroy(e, NULL);
+  sys.cutoff = 1.0;
+  opt.mesh[0] = opt.mesh[1] = opt.mesh[2] = 22; /* 2 x 11: not 2/3/5/7-smooth */
+  rc = mdb_create(&sys, &st, &opt, &e);
+  printf("%d %s\n", rc, mdb_last_error(e));
+  if (rc != MDB_ERR_NOT_SMOOTH) return 10;
+  mdb_destroy(e, NULL);
+  opt.mesh[0] = opt.mesh[1] = opt.mesh[2] = 0;
+  e = NULL;
   rc = mdb_create(&sys, &st, &opt, &e);
   printf("%d %s\n", rc, mdb_last_error(e));
   int64_t leaked = -1;
@@ -176,9 +209,11 @@ int main(void) {
 
 def test_a_c_program_links_the_library(tmp_path):
     """The header is plain C11 (warnings are errors) and a C program links
-    libmdb200.so and gets the documented status codes.  Without a GPU the
-    engine stops at the device check; with one it is created and destroyed
-    (the GPU tests are the ones that run engines)."""
+    libmdb200.so and gets the documented status codes: the reference's named
+    errors for a System without a NonbondedForce, a cutoff past half the box
+    and a mesh that is not 2/3/5/7-smooth come from the host checks, before
+    any device work.  Without a GPU the valid engine stops at the device
+    check; with one it is created and destroyed."""
     import shutil
     import subprocess
 
@@ -200,4 +235,38 @@ def test_a_c_program_links_the_library(tmp_path):
         pytest.skip("a device is visible: the engine was created")
     assert run.returncode == 0, (run.returncode, run.stdout)
     assert "time_step must be positive" in run.stdout
+    assert "NonbondedForce" in run.stdout
+    assert "cutoff does not fit this box" in run.stdout
+    assert "not 2/3/5/7-smooth" in run.stdout
     assert "no CUDA device is visible" in run.stdout
+
+
+def test_named_errors_reach_python_before_any_device_work():
+    """The reference's named errors (system.ts:178, triclinic.ts:179,
+    constraint-clusters.ts:71, fft.ts:24) come from the engine's host checks,
+    so the Python mirror raises them on any machine."""
+    import dataclasses
+
+    import numpy as np
+
+    from mdb200 import steploop, synth
+
+    system, state = synth.water_box(n_waters=100, width=1.5, seed=1, grid=(16, 16, 16))
+    with pytest.raises(steploop.CutoffTooLargeForBox, match="cutoff does not fit this box"):
+        steploop.StepLoop.from_parsed(system, state, steploop.RunOptions())
+
+    system, state = synth.water_box(n_waters=300, width=2.1, seed=5)
+    with pytest.raises(steploop.NotSmooth, match="not 2/3/5/7-smooth"):
+        steploop.StepLoop.from_parsed(system, state, steploop.RunOptions(mesh=(22, 22, 22)))
+
+    # chain the first five waters' oxygens: one constraint cluster of 15 atoms
+    oxygens = np.arange(0, 15, 3, dtype=np.int32)
+    chained = dataclasses.replace(
+        system,
+        constraint_p1=np.concatenate([system.constraint_p1, oxygens[:-1]]).astype(np.int32),
+        constraint_p2=np.concatenate([system.constraint_p2, oxygens[1:]]).astype(np.int32),
+        constraint_distance=np.concatenate([system.constraint_distance,
+                                            np.linalg.norm(state.positions[oxygens[1:]]
+                                                           - state.positions[oxygens[:-1]], axis=1)]))
+    with pytest.raises(steploop.ClusterTooLarge):
+        steploop.StepLoop.from_parsed(chained, state, steploop.RunOptions())
