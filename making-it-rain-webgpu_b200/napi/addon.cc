@@ -246,6 +246,9 @@ napi_value Create(napi_env env, napi_callback_info info) {
   o.seed = uint32_t(number(env, argv[2], "seed", 0));
   o.verlet_skin = number(env, argv[2], "verletSkin", -1);
   o.max_batch = int32_t(number(env, argv[2], "maxBatch", 100));
+  // the CUDA device: an extra member of the options object (the reference's
+  // GPUDevice argument has no counterpart here); 0 when absent
+  o.device = int32_t(number(env, argv[2], "device", 0));
   // RunOptions.integrator, "lfmiddle" or "verlet" (loop.ts:127)
   o.integrator = MDB_INTEGRATOR_LFMIDDLE;
   bool has_integrator = false;
