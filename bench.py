@@ -1,13 +1,21 @@
-"""Benchmark: ns/day of the B200 step engine on the headline workload.
+"""Benchmark: ns/day of the B200 step engine, batched against plain engines.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl mdb|reference]
 
-One "step" is one MD step (forces + LFMiddle + constraints) of the whole
-workload.  With N > 1 (torchrun, one process per GPU) a single-system workload
-runs one independent replica per rank (one system does not shard: replicas
-only) and `value` is the sum over ranks; the 64-system ensemble is split
-between the ranks by longest processing time on atom count, and `value` is
-the whole ensemble's rate.  Both are timed as the max over ranks.
+The default workload is the headline one: 64 independent systems of uneven
+sizes (2,000-30,000 atoms) advanced together by one batched engine, with the
+same systems run one plain engine each beside it (`batched_vs_plain`).  One
+"step" is one MD step (forces + LFMiddle + constraints) of the whole workload.
+With N > 1 (torchrun, one process per GPU) the ensemble is split between the
+ranks by longest processing time on atom count and `value` is the whole
+ensemble's rate; a single-system workload (`--config water-2652 | peptide-12k
+| octa-27k | npt-100k`) runs one independent replica per rank (one system does
+not shard: replicas only) and `value` is the sum over ranks.  Both are timed
+as the max over ranks.
+
+Both arms print the same `config` (the workload, identically described); what
+only the GPU arm measures (the plain engines, the autotuner's choices, stage
+times) is in `batched_vs_plain`, `details` and `roofline`.
 
 Timing: W untimed warm-up steps, then exactly K steps replayed as CUDA-graph
 strides of `--stride` steps, each stride timed with CUDA events recorded on the
@@ -18,7 +26,10 @@ and positions are read back after every stride, wall-clock timed.
 
 `--impl reference` times the reference's own CPU path on the host cores.  The
 reference's CPU path is TypeScript, which cannot run here (no Node), so the
-f64 C++ restatement of it (oracle/) stands in, with every host thread.
+f64 C++ restatement of it (oracle/) stands in, with every host thread.  It
+times exactly K steps after W warm-up steps; for the ensemble each of its
+steps is one MD step of ceil(64 / K) of the systems, taken round-robin, so
+every system is sampled and the run stays within minutes.
 """
 
 from __future__ import annotations
@@ -48,10 +59,11 @@ NS_PER_DAY_PER_STEP_PER_S = TIME_STEP_PS * 86400 / 1000.0
 FLOP_PER_PAIR = 74.0
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate at max SM clock
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_nonbonded launch, from
-# the ncu captures summarised in profiles/nonbonded_octahedron27k.md and
-# profiles/nonbonded_dram_peptide12k.md (each captured with the configuration
-# the autotuner picks; other workloads report null)
+# one ncu capture per workload with the configuration the autotuner picks
+# (other workloads report null)
 NB_TRAFFIC = {"octa-27k": 11175936, "peptide-12k": 5061632}
+# the north star's single-system target, ns/day on the 27k-atom system
+NORTH_STAR_NS_PER_DAY = 1000.0
 
 
 def workload(name: str, seed: int):
@@ -73,9 +85,61 @@ def workload(name: str, seed: int):
 
 
 def default_config() -> str:
-    from mdb200 import synth
+    return "ensemble-64"
 
-    return "peptide-12k" if hasattr(synth, "config_peptide_12k") else "water-2652"
+
+ENSEMBLE_WORKLOAD = ("64 independent systems, 2,000-30,000 atoms log-uniform, cubic or rhombic dodecahedral "
+                     "TIP3P, half with an Ala helix of 10-40 residues where it fits, PME 1.0 nm")
+
+
+def workload_config(config: str, n_gpus: int, stride: int, members=None) -> dict:
+    """The workload as both arms describe it: the same dict from the same
+    arguments, so a line of either arm names the same configuration."""
+    if config == "ensemble-64":
+        from mdb200 import synth
+
+        members = members if members is not None else synth.config_ensemble_64(seed=1)
+        cfg = {"workload": ENSEMBLE_WORKLOAD, "systems": len(members),
+               "atoms": sum(m[0].particle_count for m in members),
+               "aggregate": "system-ns/day summed over the systems",
+               "parallelism": (f"{n_gpus} GPU(s), systems sharded by longest processing time on atom count, no "
+                               "collective during a stride; reference arm: host threads")}
+    elif config == "npt-100k":
+        from mdb200 import synth
+
+        system, _ = synth.config_npt_100k(seed=1)
+        cfg = {"workload": "NPT TIP3P cube 10 nm, 1 bar, 300 K, Monte Carlo volume move every 25 steps",
+               "atoms": system.particle_count,
+               "parallelism": f"{n_gpus} GPU(s), one replica each; reference arm: host threads"}
+    else:
+        _, _, cfg = workload(config, seed=1)
+        cfg["parallelism"] = f"{n_gpus} GPU(s), one replica each; reference arm: host threads"
+    cfg["time_step_ps"] = TIME_STEP_PS
+    cfg["l2"] = (f"GPU arm: flushed (256 MB write) between timed strides of {stride} steps; "
+                 "reference arm: host memory")
+    return cfg
+
+
+def host_cpu() -> dict:
+    """The host's CPU model (lscpu's model name) and logical CPU count."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.lower().startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except (OSError, subprocess.SubprocessError):
+        pass
+    if model is None:
+        try:
+            for line in Path("/proc/cpuinfo").read_text().splitlines():
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+        except OSError:
+            pass
+    return {"model": model, "nproc": os.cpu_count()}
 
 
 class ClockSampler:
@@ -142,59 +206,139 @@ def flush_l2(buffer) -> None:
     buffer.zero_()
 
 
-def cpu_time_oracle(system, state, steps_hint: int, budget_s: float, threads: int, warmup: int = 1):
-    """Steps/s of the f64 CPU restatement (oracle/), a bounded sample after
-    untimed warm-up steps: `warmup` of them, but no more than fit in about ten
-    seconds (and never fewer than min(warmup, 3)).  Returns (steps/s, timed
-    steps, seconds, warm-up steps)."""
+def cpu_time_oracle(system, state, steps: int, threads: int, warmup: int):
+    """The f64 CPU restatement (oracle/) on one system: `warmup` untimed MD
+    steps, then exactly `steps` timed ones.  Returns (steps/s, seconds)."""
     from oracle import oracle as orc
     from mdb200.system import State
 
-    t = time.perf_counter()
-    p, v, step = orc.run(system, state, 1, seed=1, threads=threads)
-    one = time.perf_counter() - t
-    w = min(warmup, max(3, 1 + int(10.0 / max(one, 1e-6))))
-    if w > 1:
-        p, v, step = orc.run(system, State(positions=p, box=state.box, velocities=v, step=step), w - 1, seed=1,
-                             threads=threads)
-    n = max(1, min(steps_hint, int(budget_s / max(one, 1e-6))))
+    p, v, step = orc.run(system, state, max(1, warmup), seed=1, threads=threads)
     st = State(positions=p, box=state.box, velocities=v, step=step)
     t = time.perf_counter()
-    orc.run(system, st, n, seed=1, threads=threads)
+    orc.run(system, st, steps, seed=1, threads=threads)
     elapsed = time.perf_counter() - t
-    return n / elapsed, n, elapsed, max(1, w)
+    return steps / elapsed, elapsed
 
 
-def cpu_rate(config: str, steps_hint: int, budget_s: float, threads: int, warmup: int = 1):
-    """ns/day of the oracle on the workload, a description of the sample, and
-    the warm-up steps taken.  For the ensemble: one step of every system,
-    summed into one ensemble step, after `warmup` (at most 3) steps of its
-    smallest system."""
+def cpu_steps_in_budget(system, state, budget_s: float, threads: int, limit: int = 1000) -> int:
+    """How many MD steps of the oracle fit in `budget_s` seconds (at least 1),
+    from the time of one step."""
+    from oracle import oracle as orc
+
+    t = time.perf_counter()
+    orc.run(system, state, 1, seed=1, threads=threads)
+    one = time.perf_counter() - t
+    return max(1, min(limit, int(budget_s / max(one, 1e-6))))
+
+
+class EnsembleSampler:
+    """The oracle on the ensemble, one system at a time, as a CPU runs it: a
+    sampler step is one MD step of `per` systems taken round-robin (each
+    system advancing from its own last state), so K steps with per =
+    ceil(64 / K) sample every system.  Summed system-ns/day = (system-steps
+    timed) / seconds x ns-per-step; each system advances at 1 / (sum of every
+    system's step time) while the others wait, which this rate estimates."""
+
+    def __init__(self, members, threads: int, per: int):
+        self.members = members
+        self.states = [m[1] for m in members]
+        self.threads = threads
+        self.per = per
+        self.cursor = 0
+
+    def step(self) -> None:
+        from oracle import oracle as orc
+        from mdb200.system import State
+
+        for _ in range(self.per):
+            i = self.cursor % len(self.members)
+            self.cursor += 1
+            system, st = self.members[i][0], self.states[i]
+            p, v, step = orc.run(system, st, 1, seed=1, threads=self.threads)
+            self.states[i] = State(positions=p, box=st.box, velocities=v, step=step)
+
+    def timed(self, steps: int, budget_s: float | None = None) -> tuple[int, float]:
+        """Up to `steps` sampler steps (fewer once `budget_s` is spent); returns
+        (steps taken, seconds)."""
+        t0 = time.perf_counter()
+        done = 0
+        while done < steps:
+            self.step()
+            done += 1
+            if budget_s is not None and time.perf_counter() - t0 >= budget_s:
+                break
+        return done, time.perf_counter() - t0
+
+
+def cpu_baseline(config: str, budget_s: float, threads: int) -> tuple[float, str]:
+    """ns/day of the oracle on a bounded sample of the workload (about
+    `budget_s` seconds), and a description of the sample."""
     if config == "ensemble-64":
         from mdb200 import synth
-        from oracle import oracle as orc
 
         members = synth.config_ensemble_64(seed=1)
-        w = max(1, min(warmup, 3))
-        small = min(members, key=lambda m: m[0].particle_count)
-        orc.run(small[0], small[1], w, seed=1, threads=threads)
-        elapsed = 0.0
-        for system, state, _ in members:
-            t = time.perf_counter()
-            orc.run(system, state, 1, seed=1, threads=threads)
-            elapsed += time.perf_counter() - t
-        value = len(members) / elapsed * NS_PER_DAY_PER_STEP_PER_S
-        return value, 1, elapsed, (f"one MD step of each of the {len(members)} systems ({elapsed:.1f} s), "
-                                   f"system-ns/day summed, after {w} warm-up steps of the smallest"), w
+        sampler = EnsembleSampler(members, threads, per=1)
+        sampler.step()  # warm-up: the first system
+        n, elapsed = sampler.timed(len(members), budget_s)
+        value = n / elapsed * NS_PER_DAY_PER_STEP_PER_S
+        return value, (f"one MD step each of {n} of the {len(members)} systems, round-robin, in {elapsed:.1f} s "
+                       "after one warm-up step; system-ns/day summed over the ensemble")
     if config == "npt-100k":
         from mdb200 import synth
 
         system, state = synth.config_npt_100k(seed=1)
     else:
         system, state, _ = workload(config, seed=1)
-    sps, n, elapsed, w = cpu_time_oracle(system, state, steps_hint, budget_s, threads, warmup)
-    return (sps * NS_PER_DAY_PER_STEP_PER_S, n, elapsed,
-            f"{n} MD steps of the same workload in {elapsed:.1f} s after {w} warm-up steps", w)
+    n = cpu_steps_in_budget(system, state, budget_s, threads)
+    sps, elapsed = cpu_time_oracle(system, state, n, threads, warmup=1)
+    return (sps * NS_PER_DAY_PER_STEP_PER_S,
+            f"{n} MD steps of the same workload in {elapsed:.1f} s after 1 warm-up step"
+            + (" (volume moves left out)" if config == "npt-100k" else ""))
+
+
+def reference_arm(config: str, args) -> None:
+    """The reference's CPU path (the f64 restatement) on every host thread:
+    exactly --steps timed steps after --warmup untimed ones, one JSON line."""
+    threads = os.cpu_count() or 1
+    stride = min(args.stride, args.steps)
+    if config == "ensemble-64":
+        from mdb200 import synth
+
+        members = synth.config_ensemble_64(seed=1)
+        per = max(1, -(-len(members) // args.steps))
+        sampler = EnsembleSampler(members, threads, per)
+        for _ in range(args.warmup):
+            sampler.step()
+        n, elapsed = sampler.timed(args.steps)
+        value = n * per / elapsed * NS_PER_DAY_PER_STEP_PER_S
+        sample = (f"each step one MD step of {per} of the {len(members)} systems, round-robin "
+                  f"({n * per} system-steps in {elapsed:.1f} s after {args.warmup} warm-up steps); "
+                  "system-ns/day summed over the ensemble")
+        cfg = workload_config(config, args.gpus, stride, members)
+        scaling = "strong"
+    else:
+        if config == "npt-100k":
+            from mdb200 import synth
+
+            system, state = synth.config_npt_100k(seed=1)
+        else:
+            system, state, _ = workload(config, seed=1)
+        sps, elapsed = cpu_time_oracle(system, state, args.steps, threads, args.warmup)
+        n = args.steps
+        value = sps * NS_PER_DAY_PER_STEP_PER_S
+        sample = (f"{n} MD steps of the same workload in {elapsed:.1f} s after {args.warmup} warm-up steps"
+                  + (" (volume moves left out)" if config == "npt-100k" else ""))
+        cfg = workload_config(config, args.gpus, stride)
+        scaling = "weak"
+    print(json.dumps({
+        "impl": "reference", "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": args.gpus,
+        "steps": n, "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
+        "scaling": scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port", "host_cpu": host_cpu(),
+                         "sample": sample + " (f64 C++ restatement of src/reference; the TypeScript original "
+                                            "needs Node, absent here)"},
+        "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
 
 
 def main() -> None:
@@ -223,23 +367,8 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        threads = os.cpu_count() or 1
-        value, n, elapsed, sample, warm = cpu_rate(config, args.steps, min(args.cpu_budget * 6, 240.0), threads,
-                                                   args.warmup)
-        cfg = {"workload": config} if config in ("ensemble-64", "npt-100k") else workload(config, seed=1)[2]
-        print(json.dumps({
-            "impl": "reference", "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": args.gpus,
-            "steps": n, "warmup": warm, "ms_per_step": 1000.0 * elapsed / n, "higher_is_better": True,
-            "scaling": "strong" if config == "ensemble-64" else "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {**cfg, "parallelism": "host threads", "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port",
-                             "sample": sample + " (f64 C++ restatement of src/reference; the TypeScript "
-                                                "original needs Node, absent here)"},
-            "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }))
+        if rank == 0:
+            reference_arm(config, args)
         return
 
     import torch
@@ -355,6 +484,7 @@ def main() -> None:
                 "launches_per_step": prof["launches_per_step"]}
 
     scaling = "weak"  # single systems run as one replica per rank
+    extra: dict = {}
     if config == "ensemble-64":
         from mdb200 import shard, synth
 
@@ -400,21 +530,18 @@ def main() -> None:
         plain_value = 1000.0 / plain_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
         plain_tuned_value = 1000.0 / plain_tuned_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
         e2e_s, h2d, d2h = end_to_end(loop, states)
-        cfg = {"workload": f"{n_total} independent systems, 2,000-30,000 atoms log-uniform, cubic or rhombic "
-                           "dodecahedral TIP3P, half with an Ala helix of 10-40 residues where it fits",
-               "systems": n_total, "atoms": sum(m[0].particle_count for m in members),
-               "systems_per_rank": len(systems), "atoms_per_rank": sum(s.particle_count for s in systems),
-               "sharding": "longest-processing-time on atom count, no collective during a stride"
-                           if world > 1 else "one GPU",
-               "aggregate": "system-ns/day summed over the systems",
-               "plain_engine_ns_per_day": plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
-               "plain_engine": "one engine per system, the library's default list settings",
-               "batched_over_plain": value / plain_value,
-               "plain_engine_tuned_ns_per_day": plain_tuned_value,
-               "batched_over_plain_tuned": value / plain_tuned_value,
-               "autotuner": {str(b): {k: round(v, 4) if isinstance(v, float) else v for k, v in r.items()}
-                             for b, r in buckets.items()}}
-        result_loop, n_atoms = loop, cfg["atoms"]
+        cfg = workload_config(config, world, stride, members)
+        extra["batched_vs_plain"] = {
+            "batched_ns_per_day": value, "plain_engine_ns_per_day": plain_value,
+            "batched_over_plain": value / plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
+            "plain_engine": "one engine per system, the library's default list settings, timed the same way",
+            "plain_engine_tuned_ns_per_day": plain_tuned_value, "batched_over_plain_tuned": value / plain_tuned_value}
+        extra["details"] = {
+            "systems_per_rank": len(systems), "atoms_per_rank": sum(s.particle_count for s in systems),
+            "steps_per_s": steps_per_s,
+            "autotuner": {str(b): {k: round(v, 4) if isinstance(v, float) else v for k, v in r.items()}
+                          for b, r in buckets.items()}}
+        result_loop = loop
         e2e_value = args.steps / e2e_s * n_total * NS_PER_DAY_PER_STEP_PER_S
         system, state = systems[0], states[0]
     elif config == "npt-100k":
@@ -454,34 +581,36 @@ def main() -> None:
         attempts = after["attempts"] - before["attempts"]
         exact_proposals = after["exactEvaluations"] - before["exactEvaluations"] - attempts
         plain_attempts = plain_stats["attempts"] - plain_before["attempts"]
-        cfg = {"workload": "NPT TIP3P cube 10 nm, 1 bar, 300 K, Monte Carlo volume move every "
-                           f"{frequency} steps, screened by the device-trained network; the plain and the "
-                           f"screened barostat both timed from the state after the {args.surrogate_attempts * frequency}"
-                           " training steps",
-               "atoms": system.particle_count,
-               "autotuner": {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()},
-               "plain_barostat_ns_per_day": plain_value, "screened_over_plain": value / plain_value,
-               "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
-                             "active": after["surrogateActive"], "rms_kj_mol": after["surrogateRms"],
-                             "attempts_timed": attempts,
-                             "exact_per_attempt": (after["exactEvaluations"] - before["exactEvaluations"])
-                                                  / max(1, attempts),
-                             "screened_timed": after["screened"] - before["screened"],
-                             "plain_exact_per_attempt": (plain_stats["exactEvaluations"]
-                                                         - plain_before["exactEvaluations"])
-                                                        / max(1, plain_attempts),
-                             "attempts_per_ps": attempts / (args.steps * TIME_STEP_PS),
-                             "stage1_acceptance": exact_proposals / max(1, attempts),
-                             "stage2_acceptance": (after["accepted"] - before["accepted"]) / max(1, exact_proposals),
-                             "plain_acceptance": (plain_stats["accepted"] - plain_before["accepted"])
-                                                 / max(1, plain_attempts),
-                             "mean_volume_nm3": float(np.mean(volumes)) if volumes else None,
-                             "plain_mean_volume_nm3": float(np.mean(plain_volumes)) if plain_volumes else None}}
+        cfg = workload_config(config, world, stride)
+        extra["screened_vs_plain"] = {
+            "screened_ns_per_day": value, "plain_barostat_ns_per_day": plain_value,
+            "screened_over_plain": value / plain_value,
+            "timing": f"the plain and the screened barostat both timed from the state after the "
+                      f"{args.surrogate_attempts * frequency} training steps"}
+        extra["details"] = {
+            "steps_per_s": steps_per_s,
+            "autotuner": {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()},
+            "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
+                          "active": after["surrogateActive"], "rms_kj_mol": after["surrogateRms"],
+                          "attempts_timed": attempts,
+                          "exact_per_attempt": (after["exactEvaluations"] - before["exactEvaluations"])
+                                               / max(1, attempts),
+                          "screened_timed": after["screened"] - before["screened"],
+                          "plain_exact_per_attempt": (plain_stats["exactEvaluations"]
+                                                      - plain_before["exactEvaluations"])
+                                                     / max(1, plain_attempts),
+                          "attempts_per_ps": attempts / (args.steps * TIME_STEP_PS),
+                          "stage1_acceptance": exact_proposals / max(1, attempts),
+                          "stage2_acceptance": (after["accepted"] - before["accepted"]) / max(1, exact_proposals),
+                          "plain_acceptance": (plain_stats["accepted"] - plain_before["accepted"])
+                                              / max(1, plain_attempts),
+                          "mean_volume_nm3": float(np.mean(volumes)) if volumes else None,
+                          "plain_mean_volume_nm3": float(np.mean(plain_volumes)) if plain_volumes else None}}
         e2e_s, h2d, d2h = end_to_end(loop, [state])
         e2e_value = args.steps / e2e_s * NS_PER_DAY_PER_STEP_PER_S * world
-        result_loop, n_atoms = loop, system.particle_count
+        result_loop = loop
     else:
-        system, state, cfg = workload(config, seed=1 + rank)
+        system, state, _ = workload(config, seed=1 + rank)
         # the library's autotuner picks tile shape, skin and sort cell for this
         # system (untimed, like graph capture); the timed run uses its choice
         if args.tuning:
@@ -490,7 +619,6 @@ def main() -> None:
                     "inner_skin": v[4] if len(v) > 4 else 0.0, "candidates": 0, "source": "--tuning"}
         else:
             best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=600)
-        cfg["autotuner"] = {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
                                    tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"],
                                             best["prune_tiles"], best["inner_skin"])])
@@ -500,31 +628,35 @@ def main() -> None:
         value = steps_per_s * NS_PER_DAY_PER_STEP_PER_S * world
         e2e_s, h2d, d2h = end_to_end(loop, [state])
         e2e_value = args.steps / e2e_s * NS_PER_DAY_PER_STEP_PER_S * world
-        result_loop, n_atoms = loop, system.particle_count
+        cfg = workload_config(config, world, stride)
+        extra["details"] = {"steps_per_s": steps_per_s,
+                            "autotuner": {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}}
+        if config == "octa-27k":
+            per_replica = value / world
+            extra["north_star"] = {"target_ns_per_day": NORTH_STAR_NS_PER_DAY, "ns_per_day": per_replica,
+                                   "met": per_replica >= NORTH_STAR_NS_PER_DAY,
+                                   "what": "one 27k-atom system on one B200 (replicas count once)"}
+        result_loop = loop
 
     roof = roofline(result_loop)
     result = {
         "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_s * 1000.0 / args.steps, "higher_is_better": True,
         "scaling": scaling, "vs_baseline": None, "dtype": "f32 pair math, int64 fixed-point accumulation",
-        "data": "synthetic",
-        "config": {**cfg, "time_step_ps": TIME_STEP_PS, "steps_per_s": steps_per_s * world,
-                   "parallelism": ("single GPU" if world == 1 else
-                                   f"ensemble sharded over {world} GPUs" if scaling == "strong" else
-                                   f"replicas x{world}"),
-                   "l2": f"flushed (256 MB write) between timed strides of {stride} steps"},
+        "data": "synthetic", "config": cfg,
         "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps},
         "gpu_launches": int(roof.pop("launches_per_step")) * args.steps,
         "roofline": roof,
         "clocks": clock_summary,
+        **extra,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cpu_value, _, _, sample, _ = cpu_rate(config, 1000, args.cpu_budget, threads)
-        one_value, _, _, one_sample, _ = cpu_rate(config, 1000, args.cpu_budget / 2, 1)
+        cpu_value, sample = cpu_baseline(config, args.cpu_budget, threads)
+        one_value, one_sample = cpu_baseline(config, args.cpu_budget / 2, 1)
         result["cpu_baseline"] = {
-            "value": cpu_value, "unit": "ns/day", "cores": threads, "kind": "port",
+            "value": cpu_value, "unit": "ns/day", "cores": threads, "kind": "port", "host_cpu": host_cpu(),
             "sample": sample + " (f64 C++ restatement of src/reference, OpenMP over all host threads)",
             "single_thread": {"value": one_value, "cores": 1,
                               "sample": one_sample + " (one thread, like the reference's single JS thread)"}}
@@ -535,7 +667,6 @@ def main() -> None:
         import torch.distributed as dist
 
         dist.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()

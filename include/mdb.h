@@ -395,14 +395,20 @@ int mdb_get_neighbour_stats(mdb_engine* engine, int32_t system,
  *   box        host, 9 doubles; mesh host, 3 ints; alpha in nm^-1
  *   stream     a cudaStream_t, or NULL for the default stream
  *
- * Limits: at most 262,144 mesh points (64^3) and 128 points per axis, each
- * axis 2/3/5/7-smooth; larger meshes return MDB_ERR_CAPACITY and non-smooth
- * ones MDB_ERR_NOT_SMOOTH, before any device work.  The array (about 5.3 MB)
- * stays resident on every device that loads the library until the process
- * exits.  The first call on a device looks up the array's device address;
- * make that first call before any stream capture.  Every call shares the
- * array and leaves its contents behind (the charge grid is cleared at the
- * start of each call); calls whose device work overlaps race on it.
+ * Limits: at most 262,144 mesh points (64^3) and 128 points per axis, at
+ * least 5 points per axis (the order-5 spline's span), each axis
+ * 2/3/5/7-smooth; larger meshes return MDB_ERR_CAPACITY, shorter axes
+ * MDB_ERR_INVALID_ARGUMENT and non-smooth ones MDB_ERR_NOT_SMOOTH, before any
+ * device work.  The array (about 5.3 MB) stays resident on every device that
+ * loads the library until the process exits.  A call on a stream that is not
+ * capturing looks up the array's device address (so after cudaDeviceReset the
+ * next such call finds the reloaded array); a call inside a stream capture
+ * reuses the address the last call outside one found, so make the first call
+ * on a device, and the first after a device reset, before any stream capture.
+ * Every call shares the array and leaves its contents behind (the charge grid
+ * is cleared at the start of each call); calls whose device work overlaps
+ * race on it.  A CUDA error pending from the caller's earlier work is
+ * reported as MDB_ERR_DEVICE and left pending; this call then does nothing.
  */
 int mdb_reciprocal_noalloc(int32_t n, const double* positions, const double* charges,
                            const double box[9], double alpha, const int32_t mesh[3],

@@ -665,8 +665,8 @@ void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
 // size, so this path never calls cudaMalloc, cudaFree or any allocating
 // library routine.
 //
-// Limits: at most kNoAllocMaxMeshPoints mesh points (64^3) and
-// kNoAllocMaxAxis points per axis.  Every call uses the same array and leaves
+// Limits: at most kNoAllocMaxMeshPoints mesh points (64^3), kNoAllocMaxAxis
+// points per axis and at least kPmeOrder.  Every call uses the same array and leaves
 // its contents behind; the charge grid is cleared at the start of each call.
 // Two calls whose device work overlaps (different streams, or different host
 // threads on one device) race on the array and must be serialised by the
@@ -940,20 +940,25 @@ __global__ void k_na_energy(NaPtrs p, int count, double* energy) {
   }
 }
 
-// The scratch array's device address, looked up once per device with that
-// device current.  In host code `g_noalloc_scratch` names a host-side stand-in,
-// never device memory, so kernels must be given this address instead.
+// The scratch array's device address, looked up with the device current.  In
+// host code `g_noalloc_scratch` names a host-side stand-in, never device
+// memory, so kernels must be given this address instead.  A call on a stream
+// that is not capturing looks the address up again (cheap), so a device reset,
+// which reloads the module at a new address, is picked up by the next such
+// call; a call inside a stream capture uses the address the last call outside
+// one found, and fails if there is none yet.
 std::mutex g_noalloc_mutex;
 std::array<unsigned char*, 64> g_noalloc_address{};
 
-int noalloc_scratch(int device, unsigned char** out) {
+int noalloc_scratch(int device, bool capturing, unsigned char** out) {
   if (device < 0 || device >= int(g_noalloc_address.size())) return MDB_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_address[device]) {
+  if (!capturing) {
     void* ptr = nullptr;
     if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || ptr == nullptr) return MDB_ERR_DEVICE;
     g_noalloc_address[device] = static_cast<unsigned char*>(ptr);
   }
+  if (!g_noalloc_address[device]) return MDB_ERR_INVALID_ARGUMENT;
   *out = g_noalloc_address[device];
   return MDB_OK;
 }
@@ -969,7 +974,9 @@ extern "C" int mdb_reciprocal_noalloc(int32_t n, const double* positions, const 
     return MDB_ERR_INVALID_ARGUMENT;
   long long points = 1;
   for (int k = 0; k < 3; ++k) {
-    if (mesh[k] < 2 || mesh[k] > kNoAllocMaxAxis) return MDB_ERR_CAPACITY;
+    // an order-5 spline spans 5 mesh points, wrapped once into the mesh
+    if (mesh[k] < kPmeOrder) return MDB_ERR_INVALID_ARGUMENT;
+    if (mesh[k] > kNoAllocMaxAxis) return MDB_ERR_CAPACITY;
     points *= mesh[k];
   }
   if (points > kNoAllocMaxMeshPoints) return MDB_ERR_CAPACITY;
@@ -993,8 +1000,15 @@ extern "C" int mdb_reciprocal_noalloc(int32_t n, const double* positions, const 
 
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return MDB_ERR_NO_DEVICE;
+  // An error left by the caller's earlier work is theirs: report it without
+  // consuming it, so that only this call's own launches set what
+  // cudaGetLastError returns below.
+  if (cudaPeekAtLastError() != cudaSuccess) return MDB_ERR_DEVICE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &capture) != cudaSuccess) return MDB_ERR_DEVICE;
   unsigned char* base = nullptr;
-  const int status = noalloc_scratch(device, &base);
+  const int status = noalloc_scratch(device, capture != cudaStreamCaptureStatusNone, &base);
   if (status != MDB_OK) return status;
   NaPtrs p;
   p.grid = reinterpret_cast<unsigned long long*>(base + kNaGrid);
@@ -1004,7 +1018,6 @@ extern "C" int mdb_reciprocal_noalloc(int32_t n, const double* positions, const 
   p.twiddles = reinterpret_cast<float2*>(base + kNaTwiddles);
   p.partials = reinterpret_cast<double*>(base + kNaPartials);
 
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int lines = std::max(1, 2048 / mesh[2]);
   const int z_blocks = int((mesh[0] * mesh[1] + lines - 1) / lines);
   const int tiles = (S.kzh + 15) / 16;

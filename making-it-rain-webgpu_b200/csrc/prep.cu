@@ -229,6 +229,14 @@ int prepare_system(const mdb_system_desc& in, const mdb_state_desc& state, const
       error = msg.str();
       return MDB_ERR_INVALID_ARGUMENT;
     }
+    // The order-5 spline of an atom touches 5 consecutive mesh points, wrapped
+    // once into the mesh; an axis shorter than that would wrap past its end.
+    if (g < kPmeOrder) {
+      msg << "mesh size " << g << " is below the " << kPmeOrder << " points the order-" << kPmeOrder
+          << " B-spline spans";
+      error = msg.str();
+      return MDB_ERR_INVALID_ARGUMENT;
+    }
     h.grid[k] = g;
   }
 

@@ -1,28 +1,33 @@
 """Write ff14sb_subset.json: the AMBER ff14SB residues and parameters the
 synthetic peptide workloads use.
 
+  python making-it-rain-webgpu_b200/mdb200/data/make_forcefield.py <making-it-rain-webgpu checkout>
+
 Reads OpenMM's force-field XML as the reference project vendors it
-(vendor/ffxml/protein.ff14SB.xml, MIT-licensed, from OpenMM) from
-/root/reference, and keeps only what the builders in mdb200/peptide.py need:
-the ALA, GLY, LYS, GLU, ACE and NME templates, the atom types they use, and
-every bond, angle, proper/improper torsion and Lennard-Jones entry whose types
-are among those (or wildcards).  Run it where the reference is mounted; the
-JSON it writes is committed next to this script.
+(vendor/ffxml/protein.ff14SB.xml, MIT-licensed, from OpenMM) from the given
+checkout of the reference, and keeps only what the builders in
+mdb200/peptide.py need: the ALA, GLY, LYS, GLU, ACE and NME templates, the
+atom types they use, and every bond, angle, proper/improper torsion and
+Lennard-Jones entry whose types are among those (or wildcards).  The JSON it
+writes is committed next to this script.
 """
 
 from __future__ import annotations
 
+import argparse
 import json
 import xml.etree.ElementTree as ET
 from pathlib import Path
 
-SOURCE = Path("/root/reference/vendor/ffxml/protein.ff14SB.xml")
+FFXML = Path("vendor/ffxml/protein.ff14SB.xml")  # inside the reference checkout
 OUT = Path(__file__).resolve().parent / "ff14sb_subset.json"
 RESIDUES = ("ALA", "GLY", "LYS", "GLU", "ACE", "NME")
 
 
 def main() -> None:
-    root = ET.parse(SOURCE).getroot()
+    ap = argparse.ArgumentParser(description="write ff14sb_subset.json from the reference's vendored ff14SB")
+    ap.add_argument("reference", type=Path, help="root of a making-it-rain-webgpu checkout")
+    root = ET.parse(ap.parse_args().reference / FFXML).getroot()
     types = {t.get("name"): {"class": t.get("class"), "element": t.get("element"), "mass": float(t.get("mass"))}
              for t in root.find("AtomTypes")}
     residues = {}

@@ -1,8 +1,10 @@
 """Regenerate the golden fixtures in this folder from the reference's own tests.
 
-Run in a container where the reference project is mounted (read-only) at
-/root/reference.  Every value written here is read out of the reference's
-committed test data or test source, as text; nothing is computed.
+  python tests/golden/make_golden.py <making-it-rain-webgpu checkout>
+
+The argument is the root of a checkout of the reference project (read only).
+Every value written here is read out of the reference's committed test data
+or test source, as text; nothing is computed.
 
   nonbonded.json   test/fixtures/nonbonded-{system,state}.xml and
                    nonbonded-facts.json: OpenMM 8.4 PME and Ewald group
@@ -17,12 +19,13 @@ committed test data or test source, as text; nothing is computed.
 
 from __future__ import annotations
 
+import argparse
 import json
 import re
 import xml.etree.ElementTree as ET
 from pathlib import Path
 
-REFERENCE = Path("/root/reference")
+REFERENCE = Path(".")  # set by main() from the command line
 OUT = Path(__file__).resolve().parent
 
 
@@ -93,6 +96,10 @@ def triclinic() -> dict:
 
 
 def main() -> None:
+    global REFERENCE
+    ap = argparse.ArgumentParser(description="regenerate the golden fixtures from the reference's tests")
+    ap.add_argument("reference", type=Path, help="root of a making-it-rain-webgpu checkout")
+    REFERENCE = ap.parse_args().reference
     for name, make in (("nonbonded", nonbonded), ("random_kat", random_kat), ("erf", erf_table),
                        ("fixed_words", fixed_words), ("triclinic", triclinic)):
         path = OUT / f"{name}.json"

@@ -270,3 +270,25 @@ def test_named_errors_reach_python_before_any_device_work():
                                                            - state.positions[oxygens[:-1]], axis=1)]))
     with pytest.raises(steploop.ClusterTooLarge):
         steploop.StepLoop.from_parsed(chained, state, steploop.RunOptions())
+
+
+def test_mesh_axes_shorter_than_the_spline_are_refused_before_device_work(lib):
+    """An order-5 B-spline spans five mesh points, wrapped once into the mesh,
+    so an axis of fewer than five points is refused on the host: by the engine
+    (as an invalid argument) and by the allocation-free reciprocal-space entry
+    point, before either touches a device."""
+    import numpy as np
+
+    from mdb200 import abi, steploop, synth
+
+    system, state = synth.water_box(n_waters=300, width=2.1, seed=5)
+    with pytest.raises(steploop.EngineError, match="below the 5 points"):
+        steploop.StepLoop.from_parsed(system, state, steploop.RunOptions(mesh=(24, 3, 24)))
+
+    box = np.ascontiguousarray((np.eye(3) * 3.0).reshape(9))
+    dummy = C.c_void_p(1)  # never dereferenced: the size check comes first
+    for axes in ((3, 16, 16), (16, 4, 16), (16, 16, 2)):
+        mesh = (C.c_int32 * 3)(*axes)
+        status = lib.mdb_reciprocal_noalloc(1, dummy, dummy, box.ctypes.data_as(C.POINTER(C.c_double)), 3.0, mesh,
+                                            dummy, dummy, None)
+        assert status == abi.ERR_INVALID_ARGUMENT, (axes, status)
