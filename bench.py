@@ -178,12 +178,18 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self, start: float, end: float) -> dict:
-        """Samples taken between `start` and `end` (perf_counter seconds)."""
+        """Samples taken between `start` and `end` (perf_counter seconds).  A
+        timed region shorter than the 200 ms sampling period may hold none:
+        then the samples within 0.5 s either side of it stand in, and
+        `window` says so."""
+        inside = [(t, line) for t, line in self.lines if start <= t <= end]
+        window = "timed region"
+        if not inside:
+            inside = [(t, line) for t, line in self.lines if start - 0.5 <= t <= end + 0.5]
+            window = "within 0.5 s of the timed region (shorter than the sampling period)"
         sm, mx, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for stamp, line in self.lines:
-            if not start <= stamp <= end:
-                continue
+        for stamp, line in inside:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -199,7 +205,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         loaded = [v for v in sm if v > 0.5 * max(sm)] or sm
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": window}
 
 
 def flush_l2(buffer) -> None:
@@ -354,6 +360,10 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default=None,
                     help="skin,sort_cell,tile_atoms,prune_tiles[,inner_skin]: skip the autotuner (profiling runs)")
+    ap.add_argument("--phase-launches", action="store_true",
+                    help="list build as separate kernel launches, one per phase (profiling runs)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="ensemble: skip the plain per-system engines (profiling runs)")
     ap.add_argument("--surrogate-attempts", type=int, default=2000,
                     help="npt-100k: exact attempts the screening network learns from (2,000 = 50,000 steps)")
     args = ap.parse_args()
@@ -422,7 +432,7 @@ def main() -> None:
                 on_stride(loop)
         barrier()
         t1 = time.perf_counter()
-        time.sleep(0.3)  # let the sampler flush the last line of the region
+        time.sleep(0.7)  # let the sampler record a line after the region
         clocks.__exit__(None, None, None)
         return max_over_ranks(device_ms / 1000.0), clocks.summary(t0, t1)
 
@@ -516,26 +526,34 @@ def main() -> None:
             return max_over_ranks(total)
 
         # the plain engine as a user gets it: the library's default list settings
-        plain_ms = plain_engines([None] * len(systems))
+        plain_ms = None if args.no_plain else plain_engines([None] * len(systems))
         # autotuner per size bucket (untimed), then one batched engine
-        tuning, buckets = steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=400)
+        if args.tuning:
+            fixed = tuple(float(x) for x in args.tuning.split(","))
+            fixed = (fixed[0], fixed[1], int(fixed[2]), int(fixed[3])) + fixed[4:]
+            tuning, buckets = [fixed] * len(systems), {"all": {"source": "--tuning " + args.tuning}}
+        else:
+            tuning, buckets = steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=400)
         # the plain engines again with the batch's tuning, to separate the gain of
         # batching from the autotuner's
-        plain_tuned_ms = plain_engines(tuning)
-        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride, tuning=tuning)
+        plain_tuned_ms = None if args.no_plain else plain_engines(tuning)
+        opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride, tuning=tuning,
+                                   phase_launches=args.phase_launches)
         loop = steploop.StepLoop.batch(systems, states, opts)
         total_s, clock_summary = timed(loop)
         steps_per_s = args.steps / total_s
         value = steps_per_s * n_total * NS_PER_DAY_PER_STEP_PER_S
-        plain_value = 1000.0 / plain_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
-        plain_tuned_value = 1000.0 / plain_tuned_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
         e2e_s, h2d, d2h = end_to_end(loop, states)
         cfg = workload_config(config, world, stride, members)
-        extra["batched_vs_plain"] = {
-            "batched_ns_per_day": value, "plain_engine_ns_per_day": plain_value,
-            "batched_over_plain": value / plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
-            "plain_engine": "one engine per system, the library's default list settings, timed the same way",
-            "plain_engine_tuned_ns_per_day": plain_tuned_value, "batched_over_plain_tuned": value / plain_tuned_value}
+        if plain_ms is not None:
+            plain_value = 1000.0 / plain_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
+            plain_tuned_value = 1000.0 / plain_tuned_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
+            extra["batched_vs_plain"] = {
+                "batched_ns_per_day": value, "plain_engine_ns_per_day": plain_value,
+                "batched_over_plain": value / plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
+                "plain_engine": "one engine per system, the library's default list settings, timed the same way",
+                "plain_engine_tuned_ns_per_day": plain_tuned_value,
+                "batched_over_plain_tuned": value / plain_tuned_value}
         extra["details"] = {
             "systems_per_rank": len(systems), "atoms_per_rank": sum(s.particle_count for s in systems),
             "steps_per_s": steps_per_s,
@@ -621,7 +639,8 @@ def main() -> None:
             best = steploop.autotune(system, state, steploop.RunOptions(device=local), steps=600)
         opts = steploop.RunOptions(seed=7 + rank, device=local, max_batch=args.stride,
                                    tuning=[(best["verlet_skin"], best["sort_cell"], best["tile_atoms"],
-                                            best["prune_tiles"], best["inner_skin"])])
+                                            best["prune_tiles"], best["inner_skin"])],
+                                   phase_launches=args.phase_launches)
         loop = steploop.StepLoop.from_parsed(system, state, opts)
         total_s, clock_summary = timed(loop)
         steps_per_s = args.steps / total_s

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MDB_ABI_VERSION 2
+#define MDB_ABI_VERSION 3
 
 typedef enum mdb_status {
   MDB_OK = 0,
@@ -190,6 +190,10 @@ typedef struct mdb_run_options {
   int32_t surrogate_attempts;  /* > 0: each barostat learns a screening network from that many exact
                                   attempts, then screens proposals by delayed acceptance; 0 = plain
                                   barostat (no reference counterpart) */
+  int32_t tile_row_capacity;   /* starting capacity of the tile list, tiles per cluster; 0 = the
+                                  default.  A list that needs more is grown and rebuilt before any step
+                                  uses it (no reference counterpart: the reference's list has a fixed
+                                  capacity and an overflow pass, src/gpu/loop.ts:380-392) */
 } mdb_run_options;
 
 /*
@@ -274,14 +278,16 @@ typedef struct mdb_profile {
 typedef struct mdb_neighbour_stats {
   int64_t rebuilds;
   int64_t tiles;          /* cluster-pair tiles in the current list */
-  int64_t tile_capacity;
-  int64_t blocks;         /* 32-atom clusters */
-  int32_t overflowed;     /* a table ran out of room since creation */
+  int64_t tile_capacity;  /* tiles the list can hold at its current size */
+  int64_t blocks;         /* clusters of tile_atoms atoms (rows of the tile list) */
+  int32_t overflowed;     /* 1 if the list has outgrown its capacity since creation (it was then grown
+                             and rebuilt before any step used it) */
   double skin;            /* nm */
   int64_t inner_tiles;    /* tiles of the inner list the pair kernel reads (= tiles without one) */
   int64_t prunes;         /* inner-list prunes between rebuilds since creation */
   double inner_skin;      /* nm; 0 without an inner list */
   int32_t tile_atoms;     /* atoms per cluster: 8 (8x8 tiles) or 32 (32x32 tiles) */
+  int64_t list_grown;     /* times the list was grown after an overflow */
 } mdb_neighbour_stats;
 
 typedef struct mdb_engine mdb_engine;
@@ -374,6 +380,18 @@ int mdb_potential(mdb_engine* engine, int32_t system, const double* positions,
                   double* forces, mdb_energies* energies);
 
 /* ---- statistics ------------------------------------------------------------ */
+
+/*
+ * The cell grid the list was built on: divisions per axis of the spatial
+ * sort's fractional cells and each cell's extent along the box's diagonal, nm.
+ * Replaces `StepLoop.cellGeometry()`, src/gpu/loop.ts:894 (whose cells are the
+ * neighbour search's; here they are the finer cells of the sort that orders
+ * the clusters).
+ */
+int mdb_get_cell_geometry(const mdb_engine* engine, int32_t system, int32_t divisions[3], double extent[3]);
+
+/* Kernel launches one step makes.  Replaces `StepLoop.passesPerStep`, loop.ts:1105. */
+int mdb_get_passes_per_step(const mdb_engine* engine, int32_t* out);
 
 int mdb_get_barostat_stats(const mdb_engine* engine, int32_t system,
                            mdb_barostat_stats* out);

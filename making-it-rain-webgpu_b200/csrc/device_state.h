@@ -74,8 +74,10 @@ struct Dev {
   int2* tiles;
   unsigned int* masks;
   int* tile_count;   // per system
+  int* tile_need;    // per system: tiles the last rebuild found (above tile_cap: it overflowed)
   int* tile_prefix;  // S+1
   int tile_cap_total; // sum of the systems' tile capacities
+  int* halt;          // set when a list overflowed: the integrator stops advancing until the host rebuilds
 
   // inner list: the outer list's tiles that have a pair inside cutoff + inner
   // skin, in each system's region of the same capacity; the pair kernel's list

@@ -44,8 +44,10 @@ namespace {
 constexpr double kCellWidth = 0.25;  // nm, fractional cells of the spatial sort
 constexpr int kDefaultCluster = 8;   // atoms per cluster of the tile list
 constexpr double kDefaultInnerSkin = -1.0;  // nm; <= 0: no inner list unless a tuning asks for one
-// Capacity of the dense tile list, per cluster: about three times the mean
-// row at a 0.2 nm skin in water (~120 tiles for 8-atom clusters, ~90 for 32).
+// Starting capacity of the dense tile list, per cluster: about 1.7 times the
+// mean row of water at a 0.5 nm skin (~230 tiles for 8-atom clusters) and
+// twice that at a 0.2 nm skin (~90 for 32).  A list that needs more stops the
+// integrator and is grown and rebuilt by the host (grow_tile_list).
 int row_cap_for(int cluster) { return cluster == 8 ? 384 : 192; }
 constexpr int kFftTile = 8;  // kz columns per y- and x-pass CTA
 // the exact stage switches the screening network off once its running RMS
@@ -112,6 +114,7 @@ struct mdb_engine {
   double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel
   std::vector<double> sort_cell;   // per system, nm
   std::vector<double> inner_skin;  // per system, nm; <= 0: that system's inner list is its outer list
+  int64_t list_grown = 0;          // times an overflowing list was grown and rebuilt
 };
 
 namespace {
@@ -151,6 +154,40 @@ int upload(mdb_engine* e, const char* label, T*& out, const std::vector<T>& host
   int st = alloc(e, label, out, host.size());
   if (st) return st;
   if (!host.empty()) CUDA_TRY(e, cudaMemcpy(out, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return MDB_OK;
+}
+
+// Free one of the engine's allocations and forget it.
+void release(mdb_engine* e, void* ptr) {
+  if (!ptr) return;
+  for (size_t k = 0; k < e->allocs.size(); ++k)
+    if (e->allocs[k].ptr == ptr) {
+      cudaFree(ptr);
+      e->allocs.erase(e->allocs.begin() + long(k));
+      return;
+    }
+}
+
+// The tile-list arrays, sized by the systems' tile capacities (tile_cap):
+// tiles, their interaction-mask words (C * C / 32 a tile), shifts and
+// survival flags for the fill pass's raw list and for the list the pair
+// kernel reads, and the inner list's copies.
+int alloc_tile_list(mdb_engine* e) {
+  Dev& d = e->d;
+  const size_t n = size_t(d.tile_cap_total), words = size_t(e->cluster * e->cluster / 32);
+  int st = MDB_OK;
+  if ((st = alloc(e, "tiles", d.tiles, n))) return st;
+  if ((st = alloc(e, "tile masks", d.masks, n * words))) return st;
+  if ((st = alloc(e, "tile image shifts", d.tile_shift, n))) return st;
+  if ((st = alloc(e, "raw tiles", d.raw_tiles, n))) return st;
+  if ((st = alloc(e, "raw tile masks", d.raw_masks, n * words))) return st;
+  if ((st = alloc(e, "raw tile shifts", d.raw_shift, n))) return st;
+  if ((st = alloc(e, "tile survives", d.tile_alive, n))) return st;
+  if (d.inner) {
+    if ((st = alloc(e, "inner tiles", d.in_tiles, n))) return st;
+    if ((st = alloc(e, "inner tile masks", d.in_masks, n * words))) return st;
+    if ((st = alloc(e, "inner tile shifts", d.in_shift, n))) return st;
+  }
   return MDB_OK;
 }
 
@@ -243,6 +280,8 @@ void fill_box(const HostSystem& h, SysDev& S, bool keep_shift) {
   S.pme_pref = float(kOne4PiEps0 * 2 * 3.14159265358979323846 / vol);
 }
 
+int request_rebuild(mdb_engine* e, int s);
+
 int check_device_status(mdb_engine* e) {
   cudaError_t err = cudaStreamSynchronize(e->s0);
   if (err != cudaSuccess) return fail(e, MDB_ERR_DEVICE, std::string("device: ") + cudaGetErrorString(err));
@@ -251,7 +290,15 @@ int check_device_status(mdb_engine* e) {
   int any = 0;
   for (int f : flags) any |= f;
   if (any & kErrTileCapacity) return fail(e, MDB_ERR_CAPACITY, "the cluster-pair tile list ran out of room");
-  if (any & kErrTimeout) return fail(e, MDB_ERR_TIMEOUT, "a bounded device wait gave up");
+  if (any & kErrTimeout) {
+    // the list kernel's grid barrier gave up: its count holds the blocks that
+    // arrived; clear it and the bit so the next list build starts afresh
+    CUDA_TRY(e, cudaMemset(e->d.list_barrier, 0, 2 * sizeof(unsigned int)));
+    for (int& f : flags) f &= ~kErrTimeout;
+    CUDA_TRY(e, cudaMemcpy(e->d.err, flags.data(), sizeof(int) * e->d.S, cudaMemcpyHostToDevice));
+    request_rebuild(e, -1);
+    return fail(e, MDB_ERR_TIMEOUT, "a bounded device wait gave up");
+  }
   if (any & kErrRange) return fail(e, MDB_ERR_RANGE, "a value left the fixed-point range: the run diverged");
   return MDB_OK;
 }
@@ -322,6 +369,53 @@ int request_rebuild(mdb_engine* e, int s) {
   const int one = 1;
   CUDA_TRY(e, cudaMemcpy(e->d.rebuild_now, now.data(), sizeof(int) * e->d.S, cudaMemcpyHostToDevice));
   CUDA_TRY(e, cudaMemcpy(e->d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+  return MDB_OK;
+}
+
+// A list that needed more tiles than its system's capacity stopped the
+// integrator (the halt word) at the step whose rebuild overflowed.  Grow every
+// such system's capacity to half again what it needed (at least double),
+// reallocate the list, drop the captured graphs (they hold the old arrays),
+// clear the halt and the capacity bits, and ask for a rebuild of every system.
+int grow_tile_list(mdb_engine* e) {
+  Dev& d = e->d;
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  CUDA_TRY(e, cudaStreamSynchronize(e->s1));
+  CUDA_TRY(e, cudaStreamSynchronize(e->s2));
+  std::vector<int> need(d.S), err(d.S);
+  CUDA_TRY(e, cudaMemcpy(need.data(), d.tile_need, sizeof(int) * d.S, cudaMemcpyDeviceToHost));
+  CUDA_TRY(e, cudaMemcpy(err.data(), d.err, sizeof(int) * d.S, cudaMemcpyDeviceToHost));
+  long long total = 0;
+  for (int s = 0; s < d.S; ++s) {
+    SysDev& S = e->sd[s];
+    const long long most = (long long)S.n_blocks * (S.n_blocks + 1) / 2;
+    if (need[s] > S.tile_cap)
+      S.tile_cap = int(std::min<long long>(most, std::max<long long>(need[s] + need[s] / 2, 2ll * S.tile_cap)));
+    S.tile_off = int(total);
+    total += S.tile_cap;
+    err[s] &= ~kErrTileCapacity;
+  }
+  if (total > std::numeric_limits<int>::max()) return fail(e, MDB_ERR_CAPACITY, "the tile list cannot grow further");
+  for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+  e->graphs.clear();
+  for (void* p : {(void*)d.tiles, (void*)d.masks, (void*)d.tile_shift, (void*)d.raw_tiles, (void*)d.raw_masks,
+                  (void*)d.raw_shift, (void*)d.tile_alive, (void*)d.in_tiles, (void*)d.in_masks, (void*)d.in_shift})
+    release(e, p);
+  d.tile_cap_total = int(total);
+  if (const int st = alloc_tile_list(e)) return st;
+  CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(d.sys), e->sd.data(), sizeof(SysDev) * d.S, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemcpy(d.err, err.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice));
+  CUDA_TRY(e, cudaMemset(d.halt, 0, sizeof(int)));
+  e->list_grown += 1;
+  return request_rebuild(e, -1);
+}
+
+// Whether a list overflowed (the integrator has stopped): one 4-byte read.
+int list_halted(mdb_engine* e, bool* halted) {
+  int h = 0;
+  CUDA_TRY(e, cudaMemcpyAsync(&h, e->d.halt, sizeof(int), cudaMemcpyDeviceToHost, e->s0));
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  *halted = h != 0;
   return MDB_OK;
 }
 
@@ -425,7 +519,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     S.n_cells = S.cdim[0] * S.cdim[1] * S.cdim[2];
     S.cell_off = cells;
     const long long all_pairs = (long long)S.n_blocks * (S.n_blocks + 1) / 2;
-    S.tile_cap = int(std::min<long long>(all_pairs, (long long)S.n_blocks * row_cap_for(e->cluster)));
+    const long long row_cap = e->opt.tile_row_capacity > 0 ? e->opt.tile_row_capacity : row_cap_for(e->cluster);
+    S.tile_cap = int(std::min<long long>(all_pairs, (long long)S.n_blocks * row_cap));
     S.tile_off = tiles;
     S.energy_base = s * kECount;
     S.cut2 = float(h.cutoff * h.cutoff);
@@ -687,13 +782,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.cell_sys = tmp_i;
   TRY(upload(e, "cell order map", tmp_i, cell_map));
   d.cell_map = tmp_i;
-  TRY(alloc(e, "tiles", d.tiles, tiles));
-  TRY(alloc(e, "tile masks", d.masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
-  TRY(alloc(e, "tile image shifts", d.tile_shift, tiles));
-  TRY(alloc(e, "raw tiles", d.raw_tiles, tiles));
-  TRY(alloc(e, "raw tile masks", d.raw_masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
-  TRY(alloc(e, "raw tile shifts", d.raw_shift, tiles));
-  TRY(alloc(e, "tile survives", d.tile_alive, tiles));
+  if (const int st_ = alloc_tile_list(e)) return st_;
   TRY(alloc(e, "surviving tiles per row", d.row_alive, blocks));
   TRY(alloc(e, "surviving tiles start", d.alive_start, blocks));
   TRY(alloc(e, "fold translations", d.fold, slots));
@@ -703,9 +792,6 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "inner prune count", d.prune_count, n));
   TRY(alloc(e, "inner prune ticket", d.inner_ticket, 1));
   if (d.inner) {
-    TRY(alloc(e, "inner tiles", d.in_tiles, tiles));
-    TRY(alloc(e, "inner tile masks", d.in_masks, size_t(tiles) * (e->cluster * e->cluster / 32)));
-    TRY(alloc(e, "inner tile shifts", d.in_shift, tiles));
     TRY(alloc(e, "inner tile count", d.in_count, n));
     TRY(alloc(e, "inner tile prefix", d.in_prefix, n + 1));
     TRY(alloc(e, "prune reference.x", d.prx, atoms));
@@ -715,6 +801,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     TRY(alloc(e, "prune cluster bounds hi", d.cb_hi, blocks));
   }
   TRY(alloc(e, "tile count", d.tile_count, n));
+  TRY(alloc(e, "tile need", d.tile_need, n));
+  TRY(alloc(e, "list halt", d.halt, 1));
   TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
   TRY(alloc(e, "rebuild flag", d.rebuild_flag, n));
   TRY(alloc(e, "rebuild now", d.rebuild_now, n));
@@ -833,13 +921,21 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   CUDA_TRY(e, cudaEventCreate(&e->t1));
   CUDA_TRY(e, cudaDeviceSynchronize());
 
-  // first list and the first COM velocity, by the phase kernels
+  // first list and the first COM velocity, by the phase kernels (a list that
+  // overflows its starting capacity is grown and built again)
   if (const int st = request_rebuild(e, -1)) return st;
-  launch_rebuild_sort(d, e->s0);
-  launch_wrap(d, e->s0);
-  launch_rebuild_tiles(d, e->s0);
-  launch_inner_prune(d, e->s0);
-  launch_momentum(d, e->s0);
+  for (int attempt = 0;; ++attempt) {
+    launch_rebuild_sort(e->d, e->s0);
+    launch_wrap(e->d, e->s0);
+    launch_rebuild_tiles(e->d, e->s0);
+    launch_inner_prune(e->d, e->s0);
+    CUDA_TRY(e, cudaGetLastError());
+    bool halted = false;
+    if (const int st = list_halted(e, &halted)) return st;
+    if (!halted || attempt == 4) break;
+    if (const int st = grow_tile_list(e)) return st;
+  }
+  launch_momentum(e->d, e->s0);
   CUDA_TRY(e, cudaGetLastError());
   int status = check_device_status(e);
   if (status) return status;
@@ -869,7 +965,14 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
   const HostSystem& h = e->hs[s];
   const SysDev& S = e->sd[s];
   CUDA_TRY(e, cudaMemsetAsync(d.energy, 0, sizeof(unsigned long long) * d.S * kECount, e->s0));
-  list_kernels(e, e->s0);
+  // the list first: one that overflows is grown and built again before any force
+  for (int attempt = 0;; ++attempt) {
+    list_kernels(e, e->s0);
+    bool halted = false;
+    if (const int st = list_halted(e, &halted)) return st;
+    if (!halted || attempt == 4) break;
+    if (const int st = grow_tile_list(e)) return st;
+  }
   launch_pme(d, true, e->s0);
   launch_listed(d, true, e->s0);
   launch_nonbonded(d, true, e->s0);
@@ -1273,6 +1376,7 @@ int run(mdb_engine* e, int64_t steps) {
   for (const auto& h : e->hs)
     if (h.barostat_frequency > 0) freq = freq == 0 ? h.barostat_frequency : std::min(freq, h.barostat_frequency);
   int64_t remaining = steps;
+  int stalled = 0;
   while (remaining > 0) {
     int64_t chunk = std::min<int64_t>(remaining, e->opt.max_batch);
     if (freq > 0) {
@@ -1282,8 +1386,23 @@ int run(mdb_engine* e, int64_t steps) {
           until = std::min<int64_t>(until, std::max<int64_t>(1, e->hs[s].barostat_frequency - e->baro[s].step));
       chunk = until;
     }
+    const int64_t before = e->step;
     int st = run_steps(e, chunk);
     if (st) return st;
+    // a list that overflowed stopped the integrator at the step whose rebuild
+    // overflowed: grow it, rebuild, and run the steps that did not happen
+    bool halted = false;
+    if ((st = list_halted(e, &halted))) return st;
+    if (halted) {
+      long long now = 0;
+      CUDA_TRY(e, cudaMemcpy(&now, e->d.step, sizeof(long long), cudaMemcpyDeviceToHost));
+      e->step = now;
+      chunk = now - before;
+      if (chunk == 0 && ++stalled > 4) return fail(e, MDB_ERR_CAPACITY, "the tile list kept overflowing");
+      if ((st = grow_tile_list(e))) return st;
+    } else {
+      stalled = 0;
+    }
     remaining -= chunk;
     if (freq > 0) {
       for (size_t s = 0; s < e->hs.size(); ++s) {
@@ -1301,6 +1420,17 @@ int run(mdb_engine* e, int64_t steps) {
 }
 
 bool bad_system(const mdb_engine* e, int32_t s) { return !e || s < 0 || s >= int32_t(e->hs.size()); }
+
+// Kernels one graph-replayed step launches: the list kernels (one cooperative
+// launch, or 5 sort + 1 wrap + 6 tile-list kernels, 3 more when rebuilds
+// prune), the inner-list kernel, PME (spread, 3 transform passes or 5 without
+// the plane kernels, gather), listed, nonbonded, integrator.
+int launches_per_step(const mdb_engine* e) {
+  const Dev& d = e->d;
+  return (e->coop_list ? 1 : 5 + 1 + 6 + (d.prune ? 3 : 0)) + (d.inner ? 1 : 0) +
+         (d.n_fft_z ? (d.fft_planes ? 5 : 7) : 0) +
+         (d.n_bonds + d.n_angles + d.n_torsions + d.n_exceptions + d.n_restraints > 0 ? 1 : 0) + 1 + 1;
+}
 
 }  // namespace
 
@@ -1549,6 +1679,21 @@ int mdb_get_barostat_stats(const mdb_engine* e, int32_t s, mdb_barostat_stats* o
   return MDB_OK;
 }
 
+int mdb_get_cell_geometry(const mdb_engine* e, int32_t s, int32_t divisions[3], double extent[3]) {
+  if (bad_system(e, s) || !divisions || !extent) return MDB_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 3; ++k) {
+    divisions[k] = e->sd[s].cdim[k];
+    extent[k] = e->hs[s].box[k * 4] / e->sd[s].cdim[k];
+  }
+  return MDB_OK;
+}
+
+int mdb_get_passes_per_step(const mdb_engine* e, int32_t* out) {
+  if (!e || !out) return MDB_ERR_INVALID_ARGUMENT;
+  *out = launches_per_step(e);
+  return MDB_OK;
+}
+
 int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) {
   if (bad_system(e, s) || !out) return MDB_ERR_INVALID_ARGUMENT;
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
@@ -1561,7 +1706,8 @@ int mdb_get_neighbour_stats(mdb_engine* e, int32_t s, mdb_neighbour_stats* out) 
   out->tiles = tiles;
   out->tile_capacity = e->sd[s].tile_cap;
   out->blocks = e->sd[s].n_blocks;
-  out->overflowed = (err & kErrTileCapacity) ? 1 : 0;
+  out->overflowed = (err & kErrTileCapacity) || e->list_grown > 0 ? 1 : 0;
+  out->list_grown = e->list_grown;
   out->skin = e->skin[s];
   out->inner_tiles = tiles;
   out->prunes = 0;
@@ -1656,10 +1802,7 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
   // 6 tile-list kernels, 3 more when rebuilds prune), the inner-list kernel,
   // PME (spread, 3 transform passes or 5 without the plane kernels, gather),
   // listed, nonbonded, integrator
-  out->launches_per_step = (e->coop_list ? 1 : 5 + 1 + 6 + (d.prune ? 3 : 0)) + (d.inner ? 1 : 0) +
-                           (d.n_fft_z ? (d.fft_planes ? 5 : 7) : 0) +
-                           (d.n_bonds + d.n_angles + d.n_torsions + d.n_exceptions + d.n_restraints > 0 ? 1 : 0) +
-                           1 + 1;
+  out->launches_per_step = launches_per_step(e);
   CUDA_TRY(e, cudaMemsetAsync(d.fx, 0, sizeof(long long) * d.n_slots, st));
   CUDA_TRY(e, cudaMemsetAsync(d.fy, 0, sizeof(long long) * d.n_slots, st));
   CUDA_TRY(e, cudaMemsetAsync(d.fz, 0, sizeof(long long) * d.n_slots, st));

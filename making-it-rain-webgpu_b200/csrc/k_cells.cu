@@ -493,7 +493,15 @@ __device__ void phase_tiles_scan(const Dev& d) {
     const SysDev& S = d.sys[s];
     const int total = block_exclusive_scan(d.tile_cnt + S.block_off, d.tile_start + S.block_off, S.n_blocks);
     if (threadIdx.x == 0) {
-      if (total > S.tile_cap) atomicOr(&d.err[s], kErrTileCapacity);
+      // a list that needs more tiles than the system's capacity is cut there,
+      // and the engine's halt word stops the integrator, so no step runs on
+      // the cut list: the host grows the capacity to `tile_need` and rebuilds
+      // before it runs the remaining steps
+      d.tile_need[s] = total;
+      if (total > S.tile_cap) {
+        atomicOr(&d.err[s], kErrTileCapacity);
+        atomicExch(d.halt, 1);
+      }
       d.tile_count[s] = total < S.tile_cap ? total : S.tile_cap;
     }
   }

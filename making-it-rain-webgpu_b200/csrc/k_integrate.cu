@@ -519,6 +519,17 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   const int b = blockIdx.x;
   const int s = d.iblk_sys[b];
   const SysDev& S = d.sys[s];
+  if (*d.halt) {
+    // a list overflowed this step (every block sees the same word): the
+    // forces came from a cut list, so nothing advances; only the force
+    // slots are cleared for the next step, which the host runs after it has
+    // grown and rebuilt the list
+    for (int e = threadIdx.x; e < d.iblk_natom[b]; e += kThreads) {
+      const int gs = S.slot_off + d.rank[d.iatom[d.iblk_atom0[b] + e]];
+      d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;
+    }
+    return;
+  }
   const RunDev& R = d.run;
   const long long step = d.step[s];
   const bool com = S.com_freq > 0 && (step % S.com_freq) == 0;

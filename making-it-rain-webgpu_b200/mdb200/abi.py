@@ -14,7 +14,7 @@ from pathlib import Path
 PACKAGE_ROOT = Path(__file__).resolve().parent.parent
 LIBRARY_PATH = PACKAGE_ROOT / "lib" / "libmdb200.so"
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # mdb_status
 OK = 0
@@ -135,6 +135,7 @@ class RunOptions(C.Structure):
         ("flags", C.c_int32),
         ("tuning", C.POINTER(Tuning)),
         ("surrogate_attempts", C.c_int32),
+        ("tile_row_capacity", C.c_int32),
     ]
 
 
@@ -228,6 +229,7 @@ class NeighbourStats(C.Structure):
         ("prunes", C.c_int64),
         ("inner_skin", C.c_double),
         ("tile_atoms", C.c_int32),
+        ("list_grown", C.c_int64),
     ]
 
 
@@ -260,6 +262,8 @@ EXPORTS = {
     "mdb_potential": (C.c_int, [_E, C.c_int32, _dp, _dp, C.POINTER(Energies)]),
     "mdb_get_barostat_stats": (C.c_int, [_E, C.c_int32, C.POINTER(BarostatStats)]),
     "mdb_get_neighbour_stats": (C.c_int, [_E, C.c_int32, C.POINTER(NeighbourStats)]),
+    "mdb_get_cell_geometry": (C.c_int, [_E, C.c_int32, _ip, C.POINTER(C.c_double)]),
+    "mdb_get_passes_per_step": (C.c_int, [_E, _ip]),
     "mdb_memory_report": (C.c_int, [_E, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "mdb_profile_step": (C.c_int, [_E, C.c_int32, C.POINTER(Profile)]),
     "mdb_mlp_gradient": (C.c_int, [C.POINTER(C.c_float)] * 3 + [C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),

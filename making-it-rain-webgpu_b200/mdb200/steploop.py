@@ -5,7 +5,8 @@ relative to the reference project root) and its `Report` (loop.ts:173-199):
 `create` / `from_parsed`, `run`, `report`, `potential`, `positions`,
 `velocities`, `set_positions`, `set_velocities`, `set_box`,
 `advance_step_count`, `steps`, `barostat_statistics`, `mesh`,
-`box_vectors`, `verlet_flags`, `destroy`.  The per-group evaluators
+`box_vectors`, `verlet_flags`, `cell_geometry`, `passes_per_step`,
+`profile_step`, `destroy`.  The per-group evaluators
 `evaluateDirectSpace` / `evaluateReciprocalSpace` / `evaluateBondedForce`
 become `evaluate()`.  Failures raise the reference's named errors.
 
@@ -81,6 +82,9 @@ class RunOptions:
     # > 0: each barostat learns a screening network from that many exact
     # attempts, then screens proposals by delayed acceptance
     surrogate_attempts: int = 0
+    # starting capacity of the tile list, tiles per cluster; 0 = default
+    # (a list that needs more is grown and rebuilt before a step uses it)
+    tile_row_capacity: int = 0
 
     def to_c(self) -> abi.RunOptions:
         o = abi.RunOptions()
@@ -97,6 +101,7 @@ class RunOptions:
         o.flags = ((0 if self.graphs else abi.FLAG_NO_GRAPH) | (abi.FLAG_ALWAYS_REBUILD if self.always_rebuild else 0)
                    | (abi.FLAG_PHASE_LAUNCHES if self.phase_launches else 0))
         o.surrogate_attempts = int(self.surrogate_attempts)
+        o.tile_row_capacity = int(self.tile_row_capacity)
         if self.tuning is not None:
             arr = (abi.Tuning * len(self.tuning))(*[abi.Tuning(float(t[0]), float(t[1]),
                                                                int(t[2]) if len(t) > 2 else 0,
@@ -325,7 +330,23 @@ class StepLoop:
         return {"rebuilds": s.rebuilds, "tiles": s.tiles, "tileCapacity": s.tile_capacity,
                 "blocks": s.blocks, "overflowed": bool(s.overflowed), "skin": s.skin,
                 "innerTiles": s.inner_tiles, "prunes": s.prunes, "innerSkin": s.inner_skin,
-                "tileAtoms": s.tile_atoms}
+                "tileAtoms": s.tile_atoms, "listGrown": s.list_grown}
+
+    def cell_geometry(self, system: int = 0) -> dict:
+        """`StepLoop.cellGeometry()`, loop.ts:894: the divisions of the cell
+        grid the list was built on and each cell's extent along the box's
+        diagonal (nm)."""
+        div = (C.c_int32 * 3)()
+        ext = (C.c_double * 3)()
+        self._check(self._lib.mdb_get_cell_geometry(self._handle, system, div, ext))
+        return {"divisions": tuple(div), "extent": tuple(ext)}
+
+    @property
+    def passes_per_step(self) -> int:
+        """`StepLoop.passesPerStep`, loop.ts:1105: kernel launches one step makes."""
+        n = C.c_int32()
+        self._check(self._lib.mdb_get_passes_per_step(self._handle, C.byref(n)))
+        return n.value
 
     def profile_step(self, repeats: int = 20) -> dict:
         """`StepLoop.profileStep`, loop.ts:705: device ms per stage.  Advances the system."""

@@ -491,6 +491,45 @@ napi_value Neighbours(napi_env env, napi_callback_info info) {
   return obj;
 }
 
+// cellGeometry(handle): {divisions, extent}, `StepLoop.cellGeometry()` (loop.ts:894).
+napi_value CellGeometry(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  int32_t div[3] = {0, 0, 0};
+  double ext[3] = {0, 0, 0};
+  const int status = mdb_get_cell_geometry(e, 0, div, ext);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_value obj, divisions, extent, v;
+  napi_create_object(env, &obj);
+  napi_create_array_with_length(env, 3, &divisions);
+  napi_create_array_with_length(env, 3, &extent);
+  for (uint32_t k = 0; k < 3; ++k) {
+    napi_create_int32(env, div[k], &v);
+    napi_set_element(env, divisions, k, v);
+    napi_create_double(env, ext[k], &v);
+    napi_set_element(env, extent, k, v);
+  }
+  napi_set_named_property(env, obj, "divisions", divisions);
+  napi_set_named_property(env, obj, "extent", extent);
+  return obj;
+}
+
+// passesPerStep(handle): kernel launches one step makes (loop.ts:1105).
+napi_value PassesPerStep(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  mdb_engine* e = engine_of(env, argv[0]);
+  int32_t n = 0;
+  const int status = mdb_get_passes_per_step(e, &n);
+  if (status != MDB_OK) return throw_status(env, status, e);
+  napi_value v;
+  napi_create_int32(env, n, &v);
+  return v;
+}
+
 // memory(handle): {count, totalBytes}, the engine's device allocations for
 // `report_pool()` (every allocation is a named one; there is no scratch pool).
 napi_value Memory(napi_env env, napi_callback_info info) {
@@ -544,6 +583,8 @@ napi_value Init(napi_env env, napi_value exports) {
       {"step", nullptr, Step, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"barostat", nullptr, Barostat, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"neighbours", nullptr, Neighbours, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"cellGeometry", nullptr, CellGeometry, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"passesPerStep", nullptr, PassesPerStep, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"memory", nullptr, Memory, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"destroy", nullptr, Destroy, nullptr, nullptr, nullptr, napi_default, nullptr},
   };

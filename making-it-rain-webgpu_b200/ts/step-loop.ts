@@ -59,6 +59,8 @@ interface MdbAddon {
     innerTiles: number;
     prunes: number;
   };
+  cellGeometry(handle: unknown): { divisions: number[]; extent: number[] };
+  passesPerStep(handle: unknown): number;
   memory(handle: unknown): { count: number; totalBytes: number };
   destroy(handle: unknown): { leaked: number };
 }
@@ -219,6 +221,16 @@ export class StepLoop {
       skin: n.skin,
       byteLength: n.byteLength,
     };
+  }
+
+  /** `StepLoop.cellGeometry()`, loop.ts:894: the cell grid the list was built on. */
+  cellGeometry(): { readonly divisions: readonly number[]; readonly extent: readonly number[] } {
+    return addon.cellGeometry(this.handle);
+  }
+
+  /** `StepLoop.passesPerStep`, loop.ts:1105: kernel launches one step makes. */
+  get passesPerStep(): number {
+    return addon.passesPerStep(this.handle);
   }
 
   /**

@@ -54,7 +54,7 @@ def test_fixture_groups_and_forces(mdb, oracle):
     assert abs(e["direct_group"] - want["direct_group"]) <= 1e-4 * abs(want["direct_group"])
     err = rel_rms(f, wf)
     print("fixture force rel RMS", err)
-    assert err < 2e-6, err
+    assert err <= FORCE_REL_RMS, err
     loop.destroy()
 
 
@@ -343,3 +343,64 @@ def test_inner_list_on_a_small_cell_changes_nothing(mdb):
     print("small cell: whole list", f0, "inner list", f1)
     assert f1["prunes"] > 10 and f1["innerTiles"] < 0.9 * f1["tiles"]
     assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+
+
+def test_tile_list_overflow_is_grown_and_rebuilt(mdb, oracle, peptide):
+    """The reference never loses a pair when its list overflows
+    (src/gpu/loop.ts:380-392).  Here a list that outgrows its capacity stops
+    the integrator at that step; the host grows the list, rebuilds it and runs
+    the remaining steps, so no step runs on a cut list.  The engine starts
+    from a tiny capacity on the peptide box expanded by 25% per axis (molecule
+    centres scaled, as the barostat moves them), so its list is grown while
+    the engine is created; then it is given the real box and positions back,
+    half again as dense as the capacity was grown for, so the first rebuild of
+    the next run overflows mid-stride.  The forces match the oracle both times
+    and the step count is exact."""
+    from mdb200.system import State
+
+    system, state = peptide
+    scale = 1.25
+    dilute = State(positions=oracle.scale_molecules(system, state.positions, scale),
+                   box=np.asarray(state.box) * scale, velocities=state.velocities, step=state.step)
+    loop = make_loop(mdb, system, dilute, seed=4, tile_row_capacity=16)
+    flags = loop.verlet_flags()
+    print("after creation", flags)
+    assert flags["listGrown"] >= 1 and flags["overflowed"]
+    e, f = loop.evaluate()
+    want, wf = oracle.potential(system, dilute.positions, box=dilute.box, grid=(50, 50, 50), threads=8)
+    err, change = force_error_allowing_cutoff_shell(oracle, system, dilute.positions, dilute.box, f, wf)
+    print("grown list: force rel RMS", err)
+    assert err <= FORCE_REL_RMS, err
+    assert e["pairs_within_cutoff"] == want["pairs_within_cutoff"] + change
+    loop.set_box(state.box)
+    loop.set_positions(state.positions)
+    grown = loop.verlet_flags()["listGrown"]
+    loop.run(5)
+    assert loop.steps == state.step + 5
+    flags = loop.verlet_flags()
+    print("back at the real density, after 5 steps", flags)
+    assert flags["listGrown"] > grown
+    e2, f2 = loop.evaluate()
+    pos, box = loop.positions(), loop.box_vectors()
+    want2, wf2 = oracle.potential(system, pos, box=box, grid=(50, 50, 50), threads=8)
+    err2, change2 = force_error_allowing_cutoff_shell(oracle, system, pos, box, f2, wf2)
+    print("after the mid-run growth: force rel RMS", err2)
+    assert err2 <= FORCE_REL_RMS, err2
+    assert e2["pairs_within_cutoff"] == want2["pairs_within_cutoff"] + change2
+    loop.destroy()
+
+
+def test_cell_geometry_and_passes_per_step(mdb, water):
+    """`cellGeometry()` (loop.ts:894) gives the sort grid the list was built on
+    -- divisions of the 3.0 nm box into cells of at least the 0.25 nm sort
+    width, and their extent -- and `passesPerStep` (loop.ts:1105) the launches
+    of one step, the same count the stage profile reports."""
+    system, state = water
+    loop = make_loop(mdb, system, state)
+    cg = loop.cell_geometry()
+    assert cg["divisions"] == (12, 12, 12)
+    assert np.allclose(cg["extent"], 0.25)
+    passes = loop.passes_per_step
+    assert 8 <= passes <= 30
+    assert loop.profile_step(repeats=2)["launches_per_step"] == passes
+    loop.destroy()

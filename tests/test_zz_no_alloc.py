@@ -10,7 +10,8 @@ system whose charges are all farther apart than the cutoff, so the engine's
 forces are the reciprocal forces alone and `reciprocal_mesh` is the mesh sum):
 the same per-point arithmetic, so the force bits are equal and the energy
 agrees to 1e-12.  It also checks each
-result against the f64 oracle at the force and reciprocal-energy tolerances.
+result against the f64 oracle at the PME force and reciprocal-energy
+tolerances.
 
 This file is collected last on purpose: it must pass on its own in a fresh
 process and after every other test.
@@ -26,7 +27,11 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-FORCE_REL_RMS = 1.1e-6
+# Against the f64 oracle: these forces are the reciprocal forces alone, which
+# the f32 mesh arithmetic carries to a few 1e-6; the bound is the one the
+# oracle's own PME forces are pinned to against OpenMM (1e-5 relative RMS).
+# The engine's 1.1e-6 bound is on whole forces, where direct space dominates.
+RECIPROCAL_FORCE_REL_RMS = 1e-5
 ENERGY_REL = 1e-5
 MESH = (32, 32, 32)
 
@@ -92,8 +97,8 @@ def test_noalloc_reciprocal_matches_the_engine_twice(oracle):
         # split of the spectrum, so the energy may differ in its last bits
         assert np.array_equal(got_f, want_forces), (call, np.abs(got_f - want_forces).max())
         assert abs(got_e - want_energy) <= 1e-12 * abs(want_energy), (call, got_e, want_energy)
-        # and against the f64 oracle, at the force bound and the reciprocal-group tolerance
-        assert err <= FORCE_REL_RMS, (call, err)
+        # and against the f64 oracle, at the PME force bound and the reciprocal-group tolerance
+        assert err <= RECIPROCAL_FORCE_REL_RMS, (call, err)
         assert abs(got_e - want["reciprocal_mesh"]) <= ENERGY_REL * abs(want["reciprocal_mesh"]), (call, got_e)
 
 
