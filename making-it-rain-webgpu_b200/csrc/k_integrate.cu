@@ -245,20 +245,22 @@ template <int NC>
 __device__ bool rattle_star(const long long* x, const long long* y, const long long* z, float* vx, float* vy,
                             float* vz, const float* im, float tol) {
   constexpr int NA = NC + 1;
-  double v[NA][3], w[NA];
+  double v[NA][3];
 #pragma unroll
   for (int k = 0; k < NA; ++k) {
     v[k][0] = vx[k]; v[k][1] = vy[k]; v[k][2] = vz[k];
-    w[k] = im[k];
   }
-  double rv[NC][3], rl[NC], rm[NC], delta[NC];
+  // the reference bond vectors are f32 values (from_fixed) and the inverse
+  // masses f32: kept as f32 and widened where used, to save registers
+  float rv[NC][3];
+  double rl[NC], rm[NC], delta[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     rv[c][0] = from_fixed(x[0] - x[c + 1]);
     rv[c][1] = from_fixed(y[0] - y[c + 1]);
     rv[c][2] = from_fixed(z[0] - z[c + 1]);
-    rl[c] = rv[c][0] * rv[c][0] + rv[c][1] * rv[c][1] + rv[c][2] * rv[c][2];
-    const double sum = w[0] + w[c + 1];
+    rl[c] = double(rv[c][0]) * rv[c][0] + double(rv[c][1]) * rv[c][1] + double(rv[c][2]) * rv[c][2];
+    const double sum = double(im[0]) + double(im[c + 1]);
     rm[c] = sum == 0.0 ? 0.0 : 0.5 / sum;
   }
   bool ok = false;
@@ -277,8 +279,8 @@ __device__ bool rattle_star(const long long* x, const long long* y, const long l
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const double dr = rv[c][k] * delta[c];
-        v[0][k] += dr * w[0];
-        v[c + 1][k] -= dr * w[c + 1];
+        v[0][k] += dr * double(im[0]);
+        v[c + 1][k] -= dr * double(im[c + 1]);
       }
   }
 #pragma unroll
@@ -293,21 +295,20 @@ template <int NC>
 __device__ bool shake_star(const long long* x, const long long* y, const long long* z, const float* im,
                            const float* dist, float3* dp, float tol) {
   constexpr int NA = NC + 1;
-  double q[NA][3], w[NA];
+  double q[NA][3];
 #pragma unroll
   for (int k = 0; k < NA; ++k) {
     q[k][0] = dp[k].x; q[k][1] = dp[k].y; q[k][2] = dp[k].z;
-    w[k] = im[k];
   }
-  double rv[NC][3], rm[NC], d2[NC], delta[NC];
+  float rv[NC][3];  // f32 values (from_fixed), widened where used
+  double rm[NC], delta[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     rv[c][0] = from_fixed(x[0] - x[c + 1]);
     rv[c][1] = from_fixed(y[0] - y[c + 1]);
     rv[c][2] = from_fixed(z[0] - z[c + 1]);
-    const double sum = w[0] + w[c + 1];
+    const double sum = double(im[0]) + double(im[c + 1]);
     rm[c] = sum == 0.0 ? 0.0 : 0.5 / sum;
-    d2[c] = double(dist[c]) * dist[c];
   }
   const double lo = 1.0 - 2.0 * tol + double(tol) * tol, hi = 1.0 + 2.0 * tol + double(tol) * tol;
   bool ok = false;
@@ -315,12 +316,13 @@ __device__ bool shake_star(const long long* x, const long long* y, const long lo
     int conv = 0;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
+      const double d2 = double(dist[c]) * dist[c];
       const double ex = rv[c][0] + q[0][0] - q[c + 1][0], ey = rv[c][1] + q[0][1] - q[c + 1][1],
                    ez = rv[c][2] + q[0][2] - q[c + 1][2];
       const double l2 = ex * ex + ey * ey + ez * ez;
       const double proj = ex * rv[c][0] + ey * rv[c][1] + ez * rv[c][2];
-      delta[c] = proj == 0.0 ? 0.0 : rm[c] * (d2[c] - l2) / proj;
-      conv += (l2 >= lo * d2[c] && l2 <= hi * d2[c]);
+      delta[c] = proj == 0.0 ? 0.0 : rm[c] * (d2 - l2) / proj;
+      conv += (l2 >= lo * d2 && l2 <= hi * d2);
     }
     if (conv == NC) { ok = true; break; }
 #pragma unroll
@@ -328,8 +330,8 @@ __device__ bool shake_star(const long long* x, const long long* y, const long lo
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const double dr = rv[c][k] * delta[c];
-        q[0][k] += dr * w[0];
-        q[c + 1][k] -= dr * w[c + 1];
+        q[0][k] += dr * double(im[0]);
+        q[c + 1][k] -= dr * double(im[c + 1]);
       }
   }
 #pragma unroll
@@ -409,6 +411,7 @@ struct Stage {
   long long tx[kIntegrateTable], ty[kIntegrateTable], tz[kIntegrateTable];  // unconstrained drift
   long long cx[kIntegrateTable], cy[kIntegrateTable], cz[kIntegrateTable];  // constrained drift
   float vx[kIntegrateTable], vy[kIntegrateTable], vz[kIntegrateTable], im[kIntegrateTable];
+  float rx[kIntegrateTable], ry[kIntegrateTable], rz[kIntegrateTable];     // drift residuals
 };
 
 constexpr int kPerThread = kIntegrateTable / kThreads;
@@ -539,49 +542,35 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   const float dt = R.dt;
   const bool lfm = R.integrator == 0;
 
-  int atom[kPerThread], slot[kPerThread], fw[kPerThread];
-  long long px[kPerThread], py[kPerThread], pz[kPerThread];
-  float vx[kPerThread], vy[kPerThread], vz[kPerThread], rx[kPerThread], ry[kPerThread], rz[kPerThread];
-  float im[kPerThread], n0[kPerThread], n1[kPerThread], n2[kPerThread];
+  // Every phase keeps its per-atom state in the shared table, not in
+  // registers across the barriers, so the kernel needs few registers and
+  // many blocks fit on an SM; an atom phase reads its atom's index again.
 
-  // ---- atoms: load, clear the force slot, COM removal, kick, noise draw
+  // ---- atoms: load, clear the force slot, COM removal, kick
 #pragma unroll
   for (int j = 0; j < kPerThread; ++j) {
     const int e = threadIdx.x + j * kThreads;
-    atom[j] = -1;
     if (e >= natom) continue;
     const int a = d.iatom[atom0 + e];
-    atom[j] = a;
-    px[j] = d.px[a]; py[j] = d.py[a]; pz[j] = d.pz[a];
-    vx[j] = d.vx[a]; vy[j] = d.vy[a]; vz[j] = d.vz[a];
-    rx[j] = d.rx[a]; ry[j] = d.ry[a]; rz[j] = d.rz[a];
-    im[j] = d.invm[a];
+    float vx = d.vx[a], vy = d.vy[a], vz = d.vz[a];
+    const float im = d.invm[a];
     const int gs = S.slot_off + d.rank[a];
-    slot[j] = gs;
-    fw[j] = d.fold[gs];
     const float fx = from_fixed(static_cast<long long>(d.fx[gs]));
     const float fy = from_fixed(static_cast<long long>(d.fy[gs]));
     const float fz = from_fixed(static_cast<long long>(d.fz[gs]));
     d.fx[gs] = 0ull; d.fy[gs] = 0ull; d.fz[gs] = 0ull;  // consumer clears
-    if (com && im[j] > 0.f) { vx[j] -= vc.x; vy[j] -= vc.y; vz[j] -= vc.z; }
-    n0[j] = n1[j] = n2[j] = 0.f;
-    if (im[j] != 0.f) {
+    if (com && im > 0.f) { vx -= vc.x; vy -= vc.y; vz -= vc.z; }
+    if (im != 0.f) {
       if (lfm) {
-        vx[j] += dt * im[j] * fx; vy[j] += dt * im[j] * fy; vz[j] += dt * im[j] * fz;
-        if (R.draw_noise) {
-          const unsigned p = static_cast<unsigned>(a - S.atom_off);
-          const uint2 key = make_uint2(R.seed, kThermostatDomain);
-          const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
-          const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
-          n0[j] = g0.x; n1[j] = g0.y; n2[j] = g1.x;
-        }
+        vx += dt * im * fx; vy += dt * im * fy; vz += dt * im * fz;
       } else {
-        vx[j] += im[j] * fx * dt; vy[j] += im[j] * fy * dt; vz[j] += im[j] * fz * dt;
+        vx += im * fx * dt; vy += im * fy * dt; vz += im * fz * dt;
       }
     }
-    sh.x[e] = px[j]; sh.y[e] = py[j]; sh.z[e] = pz[j];
-    sh.vx[e] = vx[j]; sh.vy[e] = vy[j]; sh.vz[e] = vz[j];
-    sh.im[e] = im[j];
+    sh.x[e] = d.px[a]; sh.y[e] = d.py[a]; sh.z[e] = d.pz[a];
+    sh.vx[e] = vx; sh.vy[e] = vy; sh.vz[e] = vz;
+    sh.rx[e] = d.rx[a]; sh.ry[e] = d.ry[a]; sh.rz[e] = d.rz[a];
+    sh.im[e] = im;
   }
   __syncthreads();
 
@@ -590,32 +579,46 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   if (lfm && threadIdx.x < nunit) unit_velocities(sh, units[threadIdx.x], R.tolerance, bad);
   __syncthreads();
 
-  // ---- atoms: drift (fixed point, residual feedback) with the thermostat between the halves
+  // ---- atoms: drift (fixed point, residual feedback) with the thermostat
+  // between the halves; the thermostatted velocity and the new residual go
+  // back to the table (the position constraints read neither)
   const float half = 0.5f * dt;
 #pragma unroll
   for (int j = 0; j < kPerThread; ++j) {
     const int e = threadIdx.x + j * kThreads;
-    if (atom[j] < 0) continue;
+    if (e >= natom) continue;
+    const float im = sh.im[e];
     long long tx = 0, ty = 0, tz = 0;
-    if (im[j] != 0.f) {
-      vx[j] = sh.vx[e]; vy[j] = sh.vy[e]; vz[j] = sh.vz[e];
+    if (im != 0.f) {
+      float vx = sh.vx[e], vy = sh.vy[e], vz = sh.vz[e];
+      float rx = sh.rx[e], ry = sh.ry[e], rz = sh.rz[e];
       if (lfm) {
-        const float noise = R.noise_scale * sqrtf(R.kt * im[j]);
+        float n0 = 0.f, n1 = 0.f, n2 = 0.f;
+        if (R.draw_noise) {
+          const unsigned p = static_cast<unsigned>(d.iatom[atom0 + e] - S.atom_off);
+          const uint2 key = make_uint2(R.seed, kThermostatDomain);
+          const float2 g0 = normal_pair(make_uint2(p * 2u, static_cast<unsigned>(step)), key);
+          const float2 g1 = normal_pair(make_uint2(p * 2u + 1u, static_cast<unsigned>(step)), key);
+          n0 = g0.x; n1 = g0.y; n2 = g1.x;
+        }
+        const float noise = R.noise_scale * sqrtf(R.kt * im);
         float lo;
-        tx = displace(vx[j] * half + rx[j], lo);
-        vx[j] = R.velocity_scale * vx[j] + noise * n0[j];
-        tx += displace(vx[j] * half + lo, rx[j]);
-        ty = displace(vy[j] * half + ry[j], lo);
-        vy[j] = R.velocity_scale * vy[j] + noise * n1[j];
-        ty += displace(vy[j] * half + lo, ry[j]);
-        tz = displace(vz[j] * half + rz[j], lo);
-        vz[j] = R.velocity_scale * vz[j] + noise * n2[j];
-        tz += displace(vz[j] * half + lo, rz[j]);
+        tx = displace(vx * half + rx, lo);
+        vx = R.velocity_scale * vx + noise * n0;
+        tx += displace(vx * half + lo, rx);
+        ty = displace(vy * half + ry, lo);
+        vy = R.velocity_scale * vy + noise * n1;
+        ty += displace(vy * half + lo, ry);
+        tz = displace(vz * half + rz, lo);
+        vz = R.velocity_scale * vz + noise * n2;
+        tz += displace(vz * half + lo, rz);
       } else {
-        tx = displace(vx[j] * dt + rx[j], rx[j]);
-        ty = displace(vy[j] * dt + ry[j], ry[j]);
-        tz = displace(vz[j] * dt + rz[j], rz[j]);
+        tx = displace(vx * dt + rx, rx);
+        ty = displace(vy * dt + ry, ry);
+        tz = displace(vz * dt + rz, rz);
       }
+      sh.vx[e] = vx; sh.vy[e] = vy; sh.vz[e] = vz;
+      sh.rx[e] = rx; sh.ry[e] = ry; sh.rz[e] = rz;
     }
     sh.tx[e] = tx; sh.ty[e] = ty; sh.tz[e] = tz;
   }
@@ -632,42 +635,46 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
 #pragma unroll
   for (int j = 0; j < kPerThread; ++j) {
     const int e = threadIdx.x + j * kThreads;
-    const int a = atom[j];
-    if (a < 0) continue;
+    if (e >= natom) continue;
+    const int a = d.iatom[atom0 + e];
+    const float im = sh.im[e];
     const long long cx = sh.cx[e], cy = sh.cy[e], cz = sh.cz[e];
-    if (im[j] != 0.f) {
+    long long px = sh.x[e], py = sh.y[e], pz = sh.z[e];
+    float vx = sh.vx[e], vy = sh.vy[e], vz = sh.vz[e];
+    if (im != 0.f) {
       if (lfm) {
-        vx[j] += idt * from_fixed(cx - sh.tx[e]);
-        vy[j] += idt * from_fixed(cy - sh.ty[e]);
-        vz[j] += idt * from_fixed(cz - sh.tz[e]);
+        vx += idt * from_fixed(cx - sh.tx[e]);
+        vy += idt * from_fixed(cy - sh.ty[e]);
+        vz += idt * from_fixed(cz - sh.tz[e]);
       } else {
-        vx[j] = idt * from_fixed(cx);
-        vy[j] = idt * from_fixed(cy);
-        vz[j] = idt * from_fixed(cz);
+        vx = idt * from_fixed(cx);
+        vy = idt * from_fixed(cy);
+        vz = idt * from_fixed(cz);
       }
-      px[j] += cx; py[j] += cy; pz[j] += cz;
-      d.px[a] = px[j]; d.py[a] = py[j]; d.pz[a] = pz[j];
-      d.vx[a] = vx[j]; d.vy[a] = vy[j]; d.vz[a] = vz[j];
-      d.rx[a] = rx[j]; d.ry[a] = ry[j]; d.rz[a] = rz[j];
-      const double m = 1.0 / im[j];
-      mom[0] += m * vx[j]; mom[1] += m * vy[j]; mom[2] += m * vz[j];
-      bad |= !isfinite(vx[j] + vy[j] + vz[j]);
+      px += cx; py += cy; pz += cz;
+      d.px[a] = px; d.py[a] = py; d.pz[a] = pz;
+      d.vx[a] = vx; d.vy[a] = vy; d.vz[a] = vz;
+      d.rx[a] = sh.rx[e]; d.ry[a] = sh.ry[e]; d.rz[a] = sh.rz[e];
+      const double m = 1.0 / im;
+      mom[0] += m * vx; mom[1] += m * vy; mom[2] += m * vz;
+      bad |= !isfinite(vx + vy + vz);
     } else if (com) {
-      d.vx[a] = vx[j]; d.vy[a] = vy[j]; d.vz[a] = vz[j];
+      d.vx[a] = vx; d.vy[a] = vy; d.vz[a] = vz;
     }
     {
       // the next step's pair coordinates under this list's fold, so the list
       // kernel need not wrap again unless a rebuild or a prune is due
+      const int gs = S.slot_off + d.rank[a];
       long long na, nb, nc;
-      unpack_fold(fw[j], na, nb, nc);
-      d.pc[slot[j]] = pair_coordinate(S, px[j], py[j], pz[j], na, nb, nc);
+      unpack_fold(d.fold[gs], na, nb, nc);
+      d.pc[gs] = pair_coordinate(S, px, py, pz, na, nb, nc);
     }
-    const float ex = from_fixed(px[j] - d.refx[a]), ey = from_fixed(py[j] - d.refy[a]),
-                ez = from_fixed(pz[j] - d.refz[a]);
+    const float ex = from_fixed(px - d.refx[a]), ey = from_fixed(py - d.refy[a]),
+                ez = from_fixed(pz - d.refz[a]);
     moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
     if (d.inner) {
-      const float qx = from_fixed(px[j] - d.prx[a]), qy = from_fixed(py[j] - d.pry[a]),
-                  qz = from_fixed(pz[j] - d.prz[a]);
+      const float qx = from_fixed(px - d.prx[a]), qy = from_fixed(py - d.pry[a]),
+                  qz = from_fixed(pz - d.prz[a]);
       strayed |= qx * qx + qy * qy + qz * qz > S.half_inner2;
     }
   }
