@@ -90,16 +90,24 @@ def default_config() -> str:
 
 ENSEMBLE_WORKLOAD = ("64 independent systems, 2,000-30,000 atoms log-uniform, cubic or rhombic dodecahedral "
                      "TIP3P, half with an Ala helix of 10-40 residues where it fits, PME 1.0 nm")
+NPT_ENSEMBLE_WORKLOAD = ENSEMBLE_WORKLOAD + ", NPT: Monte Carlo volume move every 25 steps at 1 bar, 300 K"
+ENSEMBLES = ("ensemble-64", "npt-ensemble-64")
+
+
+def ensemble_members(config: str):
+    """The 64 systems of an ensemble workload (NVT, or with a barostat each)."""
+    from mdb200 import synth
+
+    return synth.config_npt_ensemble_64(seed=1) if config == "npt-ensemble-64" else synth.config_ensemble_64(seed=1)
 
 
 def workload_config(config: str, n_gpus: int, stride: int, members=None) -> dict:
     """The workload as both arms describe it: the same dict from the same
     arguments, so a line of either arm names the same configuration."""
-    if config == "ensemble-64":
-        from mdb200 import synth
-
-        members = members if members is not None else synth.config_ensemble_64(seed=1)
-        cfg = {"workload": ENSEMBLE_WORKLOAD, "systems": len(members),
+    if config in ENSEMBLES:
+        members = members if members is not None else ensemble_members(config)
+        cfg = {"workload": NPT_ENSEMBLE_WORKLOAD if config == "npt-ensemble-64" else ENSEMBLE_WORKLOAD,
+               "systems": len(members),
                "atoms": sum(m[0].particle_count for m in members),
                "aggregate": "system-ns/day summed over the systems",
                "parallelism": (f"{n_gpus} GPU(s), systems sharded by longest processing time on atom count, no "
@@ -279,16 +287,15 @@ class EnsembleSampler:
 def cpu_baseline(config: str, budget_s: float, threads: int) -> tuple[float, str]:
     """ns/day of the oracle on a bounded sample of the workload (about
     `budget_s` seconds), and a description of the sample."""
-    if config == "ensemble-64":
-        from mdb200 import synth
-
-        members = synth.config_ensemble_64(seed=1)
+    if config in ENSEMBLES:
+        members = ensemble_members(config)
         sampler = EnsembleSampler(members, threads, per=1)
         sampler.step()  # warm-up: the first system
         n, elapsed = sampler.timed(len(members), budget_s)
         value = n / elapsed * NS_PER_DAY_PER_STEP_PER_S
         return value, (f"one MD step each of {n} of the {len(members)} systems, round-robin, in {elapsed:.1f} s "
-                       "after one warm-up step; system-ns/day summed over the ensemble")
+                       "after one warm-up step; system-ns/day summed over the ensemble"
+                       + (" (volume moves left out)" if config == "npt-ensemble-64" else ""))
     if config == "npt-100k":
         from mdb200 import synth
 
@@ -307,10 +314,8 @@ def reference_arm(config: str, args) -> None:
     exactly --steps timed steps after --warmup untimed ones, one JSON line."""
     threads = os.cpu_count() or 1
     stride = min(args.stride, args.steps)
-    if config == "ensemble-64":
-        from mdb200 import synth
-
-        members = synth.config_ensemble_64(seed=1)
+    if config in ENSEMBLES:
+        members = ensemble_members(config)
         per = max(1, -(-len(members) // args.steps))
         sampler = EnsembleSampler(members, threads, per)
         for _ in range(args.warmup):
@@ -319,7 +324,8 @@ def reference_arm(config: str, args) -> None:
         value = n * per / elapsed * NS_PER_DAY_PER_STEP_PER_S
         sample = (f"each step one MD step of {per} of the {len(members)} systems, round-robin "
                   f"({n * per} system-steps in {elapsed:.1f} s after {args.warmup} warm-up steps); "
-                  "system-ns/day summed over the ensemble")
+                  "system-ns/day summed over the ensemble"
+                  + (" (volume moves left out)" if config == "npt-ensemble-64" else ""))
         cfg = workload_config(config, args.gpus, stride, members)
         scaling = "strong"
     else:
@@ -364,13 +370,15 @@ def main() -> None:
                     help="list build as separate kernel launches, one per phase (profiling runs)")
     ap.add_argument("--no-plain", action="store_true",
                     help="ensemble: skip the plain per-system engines (profiling runs)")
+    ap.add_argument("--ensemble-surrogate-attempts", type=int, default=1280,
+                    help="npt-ensemble-64: exact attempts, pooled over the 64 systems, the network learns from")
     ap.add_argument("--surrogate-attempts", type=int, default=2000,
                     help="npt-100k: exact attempts the screening network learns from (2,000 = 50,000 steps)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     config = args.config or default_config()
     if args.steps is None:
-        args.steps = {"ensemble-64": 400, "npt-100k": 2000}.get(config, 12000)
+        args.steps = {"ensemble-64": 400, "npt-ensemble-64": 400, "npt-100k": 2000}.get(config, 12000)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -561,6 +569,107 @@ def main() -> None:
                           for b, r in buckets.items()}}
         result_loop = loop
         e2e_value = args.steps / e2e_s * n_total * NS_PER_DAY_PER_STEP_PER_S
+        system, state = systems[0], states[0]
+    elif config == "npt-ensemble-64":
+        from mdb200 import shard, synth
+
+        members = ensemble_members(config)
+        share = shard.rank_share([m[0].particle_count for m in members], rank, world)
+        systems = [members[i][0] for i in share]
+        states = [members[i][1] for i in share]
+        n_total = len(members)
+        scaling = "strong"
+        frequency = systems[0].barostat[2]
+
+        def baro_sum(lp) -> dict:
+            """Barostat statistics summed over the engine's systems (the
+            network's figures are the engine's one network)."""
+            out = {}
+            for k in range(len(systems)):
+                st = lp.barostat_statistics(k)
+                for key in ("attempts", "accepted", "screened", "exactEvaluations"):
+                    out[key] = out.get(key, 0) + st[key]
+                for key in ("trainingSamples", "surrogateActive", "surrogateDisabled", "surrogateRms"):
+                    out[key] = st[key]
+            return out
+
+        # the list tuning per size bucket, from the same systems without their
+        # barostats (the list does not depend on them); untimed
+        if args.tuning:
+            fixed = tuple(float(x) for x in args.tuning.split(","))
+            fixed = (fixed[0], fixed[1], int(fixed[2]), int(fixed[3])) + fixed[4:]
+            tuning, buckets = [fixed] * len(systems), {"all": {"source": "--tuning " + args.tuning}}
+        else:
+            nvt = synth.config_ensemble_64(seed=1)
+            tuning, buckets = steploop.tune_by_bucket([nvt[i][0] for i in share], [nvt[i][1] for i in share],
+                                                      steploop.RunOptions(device=local), steps=400)
+        plain_steps = max(4, min(args.steps, 200) // frequency) * frequency
+        plain_ms = None
+        if not args.no_plain:
+            # the plain engine as a user gets it: one engine per system, its own
+            # plain barostat, the library's default list settings
+            total = 0.0
+            for sy, st in zip(systems, states):
+                one = steploop.StepLoop.from_parsed(sy, st, steploop.RunOptions(seed=7 + rank, device=local,
+                                                                               max_batch=args.stride))
+                one.run(max(args.warmup, frequency))
+                flush_l2(flush)
+                torch.cuda.synchronize()
+                total += one.run_timed(plain_steps) / plain_steps
+                one.destroy()
+            plain_ms = max_over_ranks(total)
+        # one batched engine with plain barostats, the batch's tuning
+        bp = steploop.StepLoop.batch(systems, states, steploop.RunOptions(seed=7 + rank, device=local,
+                                                                         max_batch=args.stride, tuning=tuning))
+        bp_before = baro_sum(bp)
+        bp_s, _ = timed(bp)
+        bp_stats = baro_sum(bp)
+        bp.destroy()
+        # one batched engine whose barostats screen with one network learnt
+        # from their pooled exact attempts (the learning is untimed)
+        loop = steploop.StepLoop.batch(systems, states, steploop.RunOptions(
+            seed=7 + rank, device=local, max_batch=args.stride, tuning=tuning,
+            surrogate_attempts=args.ensemble_surrogate_attempts))
+        t_train = time.perf_counter()
+        rounds = -(-args.ensemble_surrogate_attempts // len(systems))
+        loop.run(rounds * frequency)
+        t_train = time.perf_counter() - t_train
+        before = baro_sum(loop)
+        total_s, clock_summary = timed(loop)
+        after = baro_sum(loop)
+        steps_per_s = args.steps / total_s
+        value = steps_per_s * n_total * NS_PER_DAY_PER_STEP_PER_S
+        bp_value = args.steps / bp_s * n_total * NS_PER_DAY_PER_STEP_PER_S
+        e2e_s, h2d, d2h = end_to_end(loop, states)
+        e2e_value = args.steps / e2e_s * n_total * NS_PER_DAY_PER_STEP_PER_S
+        cfg = workload_config(config, world, stride, members)
+        attempts = after["attempts"] - before["attempts"]
+        exact_props = after["exactEvaluations"] - before["exactEvaluations"] - attempts
+        bp_attempts = bp_stats["attempts"] - bp_before["attempts"]
+        extra["npt_batched_vs_plain"] = {
+            "batched_screened_ns_per_day": value, "batched_plain_barostat_ns_per_day": bp_value,
+            "batched_screened_over_batched_plain": value / bp_value,
+            "plain": f"one engine per system with its own plain Monte Carlo barostat, the library's default list "
+                     f"settings, {plain_steps} steps each"}
+        if plain_ms is not None:
+            plain_value = 1000.0 / plain_ms * n_total * NS_PER_DAY_PER_STEP_PER_S
+            extra["npt_batched_vs_plain"].update({
+                "plain_engine_ns_per_day": plain_value, "plain_engine_ms_per_all_systems_step": plain_ms,
+                "batched_screened_over_plain": value / plain_value, "batched_plain_over_plain": bp_value / plain_value})
+        extra["details"] = {
+            "systems_per_rank": len(systems), "atoms_per_rank": sum(x.particle_count for x in systems),
+            "steps_per_s": steps_per_s,
+            "autotuner": {str(b): {k: round(v, 4) if isinstance(v, float) else v for k, v in r.items()}
+                          for b, r in buckets.items()},
+            "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
+                          "active": after["surrogateActive"], "disabled": after["surrogateDisabled"],
+                          "rms_kj_mol": after["surrogateRms"], "attempts_timed": attempts,
+                          "exact_per_attempt": (after["exactEvaluations"] - before["exactEvaluations"])
+                                               / max(1, attempts),
+                          "stage1_acceptance": exact_props / max(1, attempts),
+                          "stage2_acceptance": (after["accepted"] - before["accepted"]) / max(1, exact_props),
+                          "plain_acceptance": (bp_stats["accepted"] - bp_before["accepted"]) / max(1, bp_attempts)}}
+        result_loop = loop
         system, state = systems[0], states[0]
     elif config == "npt-100k":
         from mdb200 import synth

@@ -187,9 +187,9 @@ typedef struct mdb_run_options {
   int32_t device;              /* CUDA device ordinal */
   int32_t flags;               /* MDB_FLAG_* */
   const mdb_tuning* tuning;    /* NULL, or one entry per system of the engine (no reference counterpart) */
-  int32_t surrogate_attempts;  /* > 0: each barostat learns a screening network from that many exact
-                                  attempts, then screens proposals by delayed acceptance; 0 = plain
-                                  barostat (no reference counterpart) */
+  int32_t surrogate_attempts;  /* > 0: the engine's barostats learn one screening network from that many
+                                  exact attempts (pooled over the engine's systems), then screen proposals
+                                  by delayed acceptance; 0 = plain barostat (no reference counterpart) */
   int32_t tile_row_capacity;   /* starting capacity of the tile list, tiles per cluster; 0 = the
                                   default.  A list that needs more is grown and rebuilt before any step
                                   uses it (no reference counterpart: the reference's list has a fixed
@@ -239,7 +239,7 @@ typedef struct mdb_barostat_stats {
   /* delayed-acceptance screening (no reference counterpart) */
   int64_t screened;          /* proposals rejected by the network stage alone */
   int64_t exact_evaluations; /* exact potential evaluations the attempts made */
-  int64_t training_samples;  /* exact attempts the network learned from */
+  int64_t training_samples;  /* exact attempts the network learned from (all systems of the engine) */
   int32_t surrogate_active;  /* 1 while proposals are screened */
   int32_t surrogate_disabled;/* 1 when the exact stage found the network too inaccurate */
   double surrogate_rms;      /* running RMS of (predicted - exact) potential change, kJ/mol */
@@ -329,7 +329,10 @@ int mdb_system_count(const mdb_engine* engine, int32_t* out);
 /*
  * Advance every system by `steps` steps.  Replaces `StepLoop.run(n)`,
  * loop.ts:651, including the barostat attempts it makes between batches
- * (loop.ts:662-685).
+ * (loop.ts:662-685).  Systems whose barostats are due at the same step attempt
+ * together: one evaluation of the engine for their current energies and one
+ * for their proposals; each draws from its own counter, so its moves are the
+ * ones it makes alone.
  */
 int mdb_run(mdb_engine* engine, int64_t steps);
 

@@ -231,6 +231,24 @@ __device__ __forceinline__ unsigned int row_bits(const unsigned int* masks, long
   return (masks[ti * (C * C / 32) + (l >> 2)] >> ((l & 3) * 8)) & 0xFFu;
 }
 
+// A tile's lattice image, kept beside its shift in the tile's int4 (w): bit
+// 0 asks for the per-pair minimum image, bits 1-30 hold the image's lattice
+// counts (three signed 10-bit values), from which the shift in pair-coordinate
+// units follows for any box -- so a small box change (a barostat move) can
+// keep the list and recompute the shifts.
+__host__ __device__ __forceinline__ int tile_flags(bool per_pair, int na, int nb, int nc) {
+  return (per_pair ? 1 : 0) | ((na & 1023) << 1) | ((nb & 1023) << 11) | ((nc & 1023) << 21);
+}
+__device__ __forceinline__ bool tile_per_pair(int w) { return (w & 1) != 0; }
+__device__ __forceinline__ int4 tile_shift_for(const SysDev& S, int w) {
+  const int na = (w << 21) >> 22, nb = (w << 11) >> 22, nc = (w << 1) >> 22;
+  const unsigned sx = unsigned(na) * unsigned(S.pc_box[0]) + unsigned(nb) * unsigned(S.pc_box[3]) +
+                      unsigned(nc) * unsigned(S.pc_box[6]);
+  const unsigned sy = unsigned(nb) * unsigned(S.pc_box[4]) + unsigned(nc) * unsigned(S.pc_box[7]);
+  const unsigned sz = unsigned(nc) * unsigned(S.pc_box[8]);
+  return make_int4(int(sx), int(sy), int(sz), w);
+}
+
 // Minimum image of a pair-coordinate difference (int32 at 2^pc_shift per nm).
 template <bool TRICLINIC>
 __device__ __forceinline__ void min_image(const SysDev& S, int& dx, int& dy, int& dz) {

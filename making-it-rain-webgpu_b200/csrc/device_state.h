@@ -167,6 +167,7 @@ void launch_integrate(const Dev& d, cudaStream_t s);
 void launch_momentum(const Dev& d, cudaStream_t s);
 void launch_scale_molecules(const Dev& d, int first_mol, int n_mol, double scale, cudaStream_t st);
 void launch_restore_positions(const Dev& d, int atom_off, int n, cudaStream_t st);
+void launch_after_box_change(const Dev& d, int s, int n_slots, int tile_cap, cudaStream_t st);
 int molecular_offset_blocks(int n_mol);
 void launch_molecular_offsets(const Dev& d, int first_mol, int n_mol, int slot_off, double* partials,
                               cudaStream_t st);

@@ -77,6 +77,8 @@ struct Surrogate {
   float* t = nullptr;             // device: normalised targets
   float* y = nullptr;             // device: inference outputs
   float* loss = nullptr;          // device: per-minibatch losses of the last epoch
+  float* xi = nullptr;            // device: inference inputs, two rows per system
+  float* yi = nullptr;            // device: inference outputs
   double final_loss = 0;
 };
 
@@ -85,7 +87,6 @@ struct BarostatState {
   int64_t attempts = 0, accepted = 0, step = 0, draw = 0;
   int64_t screened = 0, exact = 0;
   int window_attempts = 0, window_accepted = 0;
-  Surrogate net;
 };
 
 }  // namespace
@@ -97,6 +98,9 @@ struct mdb_engine {
   std::vector<HostSystem> hs;
   std::vector<SysDev> sd;
   std::vector<BarostatState> baro;
+  // the barostats' screening network, one for every system of the engine:
+  // it learns from the pooled exact attempts of all of them
+  Surrogate net;
   Dev d{};
   std::vector<Allocation> allocs;
   cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
@@ -111,10 +115,12 @@ struct mdb_engine {
   bool prune = true;               // rebuilds drop tiles with no pair inside cutoff + skin
   std::vector<double> skin;        // per system, nm
   std::vector<int> mol_first, mol_count;  // per system: its molecules in d.mol_off
-  double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel
+  double* mol_partials = nullptr;          // 9 per block of the molecular-offset kernel, systems one after another
+  std::vector<int> mol_part_off;           // per system: its first block in mol_partials
   std::vector<double> sort_cell;   // per system, nm
   std::vector<double> inner_skin;  // per system, nm; <= 0: that system's inner list is its outer list
   int64_t list_grown = 0;          // times an overflowing list was grown and rebuilt
+  std::vector<std::array<double, 9>> box_at_rebuild;  // per system: the box when a box change last asked for a rebuild
 };
 
 namespace {
@@ -459,6 +465,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     const int st = prepare_system(systems[s], states[s], e->opt, e->hs[s], msg);
     if (st) return fail(e, st, n > 1 ? "system " + std::to_string(s) + ": " + msg : msg);
   }
+  e->box_at_rebuild.resize(n);
+  for (int s = 0; s < n; ++s) e->box_at_rebuild[s] = e->hs[s].box;
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
     return fail(e, MDB_ERR_NO_DEVICE, "no CUDA device is visible");
@@ -704,8 +712,9 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     tiles += S.tile_cap;
     e->baro[s].volume_scale = 0.01 * box_volume(h.box.data());
     e->baro[s].step = 0;
-    e->baro[s].net.target = std::max(0, e->opt.surrogate_attempts);
   }
+
+  e->net.target = std::max(0, e->opt.surrogate_attempts);
 
   // ---- device tables ----
   Dev& d = e->d;
@@ -876,9 +885,13 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     d.mol_off = tmp;
     TRY(upload(e, "molecule atoms", tmp, mol_atoms));
     d.mol_atoms = tmp;
-    int most = 1;
-    for (int s = 0; s < n; ++s) most = std::max(most, molecular_offset_blocks(e->mol_count[s]));
-    TRY(alloc(e, "molecular virial partials", e->mol_partials, size_t(most) * 9));
+    int total_blocks = 0;
+    e->mol_part_off.assign(n, 0);
+    for (int s = 0; s < n; ++s) {
+      e->mol_part_off[s] = total_blocks;
+      total_blocks += molecular_offset_blocks(e->mol_count[s]);
+    }
+    TRY(alloc(e, "molecular virial partials", e->mol_partials, size_t(total_blocks) * 9));
   }
   UnitDev* u_dev = nullptr;
   TRY(upload(e, "integration units", u_dev, units));
@@ -960,10 +973,13 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   return MDB_OK;
 }
 
-int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinetic = true) {
+// Energies by group (and the virials) of several systems from one evaluation
+// of the whole engine -- the systems' terms come out of the same launches --
+// and, for the first of them, the forces.  `kinetic`: also the kinetic energy
+// from the velocities as they are.
+int evaluate_many(mdb_engine* e, const std::vector<int>& systems, double* forces, mdb_energies* out,
+                  bool kinetic) {
   const Dev& d = e->d;
-  const HostSystem& h = e->hs[s];
-  const SysDev& S = e->sd[s];
   CUDA_TRY(e, cudaMemsetAsync(d.energy, 0, sizeof(unsigned long long) * d.S * kECount, e->s0));
   // the list first: one that overflows is grown and built again before any force
   for (int attempt = 0;; ++attempt) {
@@ -979,15 +995,15 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
   CUDA_TRY(e, cudaGetLastError());
   int st = check_device_status(e);
   if (st) return st;
-  std::vector<double> mol_part;
   if (out) {
-    launch_molecular_offsets(d, e->mol_first[s], e->mol_count[s], S.slot_off, e->mol_partials, e->s0);
+    for (int s : systems)
+      launch_molecular_offsets(d, e->mol_first[s], e->mol_count[s], e->sd[s].slot_off,
+                               e->mol_partials + size_t(e->mol_part_off[s]) * 9, e->s0);
     CUDA_TRY(e, cudaGetLastError());
-    mol_part.resize(size_t(molecular_offset_blocks(e->mol_count[s])) * 9);
     CUDA_TRY(e, cudaStreamSynchronize(e->s0));  // s0 does not order with the legacy stream
-    CUDA_TRY(e, cudaMemcpy(mol_part.data(), e->mol_partials, sizeof(double) * mol_part.size(), cudaMemcpyDeviceToHost));
   }
-  if (forces) {
+  if (forces && !systems.empty()) {
+    const SysDev& S = e->sd[systems[0]];
     std::vector<unsigned long long> f[3];
     std::vector<int> order(S.n_slots);
     for (auto& v : f) v.resize(S.n_slots);
@@ -1003,68 +1019,74 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
     }
   }
   if (out) {
-    std::memset(out, 0, sizeof(*out));
-    std::vector<unsigned long long> en(kECount);
-    CUDA_TRY(e, cudaMemcpy(en.data(), d.energy + S.energy_base, sizeof(long long) * kECount, cudaMemcpyDeviceToHost));
-    auto val = [&](int k) { return double((long long)en[k]) / 4294967296.0; };
-    std::vector<double> mesh(e->n_mesh_items);
+    std::vector<unsigned long long> en(size_t(d.S) * kECount);
+    CUDA_TRY(e, cudaMemcpy(en.data(), d.energy, sizeof(long long) * en.size(), cudaMemcpyDeviceToHost));
+    std::vector<double> mesh(e->n_mesh_items), mesh_vir(size_t(e->n_mesh_items) * 6);
     CUDA_TRY(e, cudaMemcpy(mesh.data(), d.mesh_partial, sizeof(double) * e->n_mesh_items, cudaMemcpyDeviceToHost));
-    std::vector<double> mesh_vir(size_t(e->n_mesh_items) * 6);
     CUDA_TRY(e, cudaMemcpy(mesh_vir.data(), d.mesh_virial, sizeof(double) * mesh_vir.size(), cudaMemcpyDeviceToHost));
-    double em = 0, wm[6] = {0, 0, 0, 0, 0, 0};
-    for (int k = 0; k < e->n_mesh_items; ++k)
-      if (e->fft_x_sys[k] == s) {
-        em += mesh[k];
-        for (int c = 0; c < 6; ++c) wm[c] += mesh_vir[size_t(k) * 6 + c];
+    for (size_t i = 0; i < systems.size(); ++i) {
+      const int s = systems[i];
+      const HostSystem& h = e->hs[s];
+      const SysDev& S = e->sd[s];
+      mdb_energies& o = out[i];
+      std::memset(&o, 0, sizeof(o));
+      std::vector<double> mol_part(size_t(molecular_offset_blocks(e->mol_count[s])) * 9);
+      CUDA_TRY(e, cudaMemcpy(mol_part.data(), e->mol_partials + size_t(e->mol_part_off[s]) * 9,
+                             sizeof(double) * mol_part.size(), cudaMemcpyDeviceToHost));
+      auto val = [&](int k) { return double((long long)en[size_t(S.energy_base) + k]) / 4294967296.0; };
+      double em = 0, wm[6] = {0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < e->n_mesh_items; ++k)
+        if (e->fft_x_sys[k] == s) {
+          em += mesh[k];
+          for (int c = 0; c < 6; ++c) wm[c] += mesh_vir[size_t(k) * 6 + c];
+        }
+      o.bond = val(kEBond);
+      o.angle = val(kEAngle);
+      o.torsion = val(kETorsion);
+      o.restraint = val(kERestraint);
+      o.direct_coulomb = val(kECoulomb);
+      o.direct_lj = val(kELj);
+      o.exclusion_correction = val(kEExclusion);
+      o.exceptions = val(kEException);
+      o.pairs_within_cutoff = double(static_cast<long long>(en[size_t(S.energy_base) + kEPairs]));
+      o.dispersion = h.dispersion_energy;
+      o.reciprocal_mesh = em;
+      o.self_energy = h.self_energy;
+      o.net_charge = h.net_charge_energy;
+      o.direct_group = o.direct_coulomb + o.direct_lj + o.exclusion_correction + o.exceptions + o.dispersion;
+      o.reciprocal_group = o.reciprocal_mesh + o.self_energy + o.net_charge;
+      // virial: pairs, exceptions and bonded terms from the device accumulators,
+      // the mesh sum's from the FP64 partials, and the 1/V corrections on the
+      // diagonal (restraints are left out: their anchors do not scale)
+      for (int k = 0; k < 9; ++k) o.virial[k] = val(kEVirial0 + k);
+      const int sym[6][2] = {{0, 0}, {4, 4}, {8, 8}, {1, 3}, {2, 6}, {5, 7}};
+      for (int c = 0; c < 6; ++c) {
+        o.virial[sym[c][0]] += wm[c];
+        if (sym[c][1] != sym[c][0]) o.virial[sym[c][1]] += wm[c];
       }
-    out->bond = val(kEBond);
-    out->angle = val(kEAngle);
-    out->torsion = val(kETorsion);
-    out->restraint = val(kERestraint);
-    out->direct_coulomb = val(kECoulomb);
-    out->direct_lj = val(kELj);
-    out->exclusion_correction = val(kEExclusion);
-    out->exceptions = val(kEException);
-    out->pairs_within_cutoff = double(static_cast<long long>(en[kEPairs]));
-    out->dispersion = h.dispersion_energy;
-    out->reciprocal_mesh = em;
-    out->self_energy = h.self_energy;
-    out->net_charge = h.net_charge_energy;
-    out->direct_group = out->direct_coulomb + out->direct_lj + out->exclusion_correction + out->exceptions +
-                        out->dispersion;
-    out->reciprocal_group = out->reciprocal_mesh + out->self_energy + out->net_charge;
-    // virial: pairs, exceptions and bonded terms from the device accumulators,
-    // the mesh sum's from the FP64 partials, and the 1/V corrections on the
-    // diagonal (restraints are left out: their anchors do not scale)
-    for (int k = 0; k < 9; ++k) out->virial[k] = val(kEVirial0 + k);
-    const int sym[6][2] = {{0, 0}, {4, 4}, {8, 8}, {1, 3}, {2, 6}, {5, 7}};
-    for (int c = 0; c < 6; ++c) {
-      out->virial[sym[c][0]] += wm[c];
-      if (sym[c][1] != sym[c][0]) out->virial[sym[c][1]] += wm[c];
-    }
-    for (int a = 0; a < 3; ++a) out->virial[4 * a] += out->dispersion + out->net_charge;
-    // the molecular virial: minus the atoms' offsets from their molecule's centre
-    for (int c = 0; c < 9; ++c) {
-      double corr = 0;
-      for (size_t b = 0; b < mol_part.size() / 9; ++b) corr += mol_part[b * 9 + c];
-      out->molecular_virial[c] = out->virial[c] - corr;
-    }
-    out->potential = out->bond + out->angle + out->torsion + out->restraint + out->direct_group +
-                     out->reciprocal_group;
-    // kinetic energy from the velocities as they are (kinetic.ts:31)
-    if (kinetic) {
-      std::vector<float> v[3];
-      for (auto& x : v) x.resize(h.n);
-      CUDA_TRY(e, cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
-      CUDA_TRY(e, cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
-      CUDA_TRY(e, cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
-      double ke = 0;
-      for (int a = 0; a < h.n; ++a)
-        if (h.mass[a] > 0)
-          ke += h.mass[a] * (double(v[0][a]) * v[0][a] + double(v[1][a]) * v[1][a] + double(v[2][a]) * v[2][a]);
-      out->kinetic = 0.5 * ke;
-      out->degrees_of_freedom = h.dof;
-      out->temperature = h.dof > 0 ? 2 * out->kinetic / (h.dof * kBoltzmann) : 0;
+      for (int a = 0; a < 3; ++a) o.virial[4 * a] += o.dispersion + o.net_charge;
+      // the molecular virial: minus the atoms' offsets from their molecule's centre
+      for (int c = 0; c < 9; ++c) {
+        double corr = 0;
+        for (size_t b = 0; b < mol_part.size() / 9; ++b) corr += mol_part[b * 9 + c];
+        o.molecular_virial[c] = o.virial[c] - corr;
+      }
+      o.potential = o.bond + o.angle + o.torsion + o.restraint + o.direct_group + o.reciprocal_group;
+      // kinetic energy from the velocities as they are (kinetic.ts:31)
+      if (kinetic) {
+        std::vector<float> v[3];
+        for (auto& x : v) x.resize(h.n);
+        CUDA_TRY(e, cudaMemcpy(v[0].data(), d.vx + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
+        CUDA_TRY(e, cudaMemcpy(v[1].data(), d.vy + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
+        CUDA_TRY(e, cudaMemcpy(v[2].data(), d.vz + S.atom_off, sizeof(float) * h.n, cudaMemcpyDeviceToHost));
+        double ke = 0;
+        for (int a = 0; a < h.n; ++a)
+          if (h.mass[a] > 0)
+            ke += h.mass[a] * (double(v[0][a]) * v[0][a] + double(v[1][a]) * v[1][a] + double(v[2][a]) * v[2][a]);
+        o.kinetic = 0.5 * ke;
+        o.degrees_of_freedom = h.dof;
+        o.temperature = h.dof > 0 ? 2 * o.kinetic / (h.dof * kBoltzmann) : 0;
+      }
     }
   }
   // the step loop expects cleared accumulators
@@ -1073,6 +1095,10 @@ int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinet
   CUDA_TRY(e, cudaMemsetAsync(d.fz, 0, sizeof(long long) * d.n_slots, e->s0));
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   return MDB_OK;
+}
+
+int evaluate(mdb_engine* e, int s, double* forces, mdb_energies* out, bool kinetic = true) {
+  return evaluate_many(e, std::vector<int>{s}, forces, out, kinetic);
 }
 
 int get_positions(mdb_engine* e, int s, double* out) {
@@ -1121,11 +1147,46 @@ int set_box(mdb_engine* e, int s, const double* box) {
   if (h.cutoff > 0.5 * std::min({widths[0], widths[1], widths[2]}))
     return fail(e, MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX, "the cutoff does not fit the new box");
   std::copy(reduced, reduced + 9, h.box.begin());
+  std::copy(reduced, reduced + 9, e->box_at_rebuild[s].begin());
   update_box_constants(h);
   fill_box(h, e->sd[s], true);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys) + s, &e->sd[s], sizeof(SysDev), cudaMemcpyHostToDevice));
   return request_rebuild(e, s);
+}
+
+// A volume move's box change (or its undo) that keeps the tile list: the
+// tiles' shifts follow the new box from their lattice counts, the pair
+// coordinates follow the scaled positions, and a device displacement test asks
+// for a rebuild only if some atom has gone half the skin from the list's
+// reference (k_after_box_change).  A rebuild is still asked for when the
+// pair-coordinate scale changes or the box has drifted by more than 1% per
+// axis since the engine last asked for one on a box change: the tiles'
+// per-pair flags were set for the box the list was built in.
+int move_box(mdb_engine* e, int s, const double* box) {
+  HostSystem& h = e->hs[s];
+  double reduced[9];
+  if (!reduce_box(box, reduced)) return fail(e, MDB_ERR_INVALID_ARGUMENT, "degenerate box");
+  double widths[3];
+  perpendicular_widths(reduced, widths);
+  if (h.cutoff > 0.5 * std::min({widths[0], widths[1], widths[2]}))
+    return fail(e, MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX, "the cutoff does not fit the new box");
+  std::copy(reduced, reduced + 9, h.box.begin());
+  update_box_constants(h);
+  const int shift = e->sd[s].pc_shift;
+  fill_box(h, e->sd[s], true);
+  bool rebuild = e->sd[s].pc_shift != shift;
+  for (int k = 0; k < 3; ++k)
+    rebuild |= std::fabs(reduced[4 * k] / e->box_at_rebuild[s][4 * k] - 1.0) > 0.01;
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys) + s, &e->sd[s], sizeof(SysDev), cudaMemcpyHostToDevice));
+  if (rebuild) {
+    std::copy(reduced, reduced + 9, e->box_at_rebuild[s].begin());
+    return request_rebuild(e, s);
+  }
+  launch_after_box_change(e->d, s, e->sd[s].n_slots, e->sd[s].tile_cap, e->s0);
+  CUDA_TRY(e, cudaGetLastError());
+  return MDB_OK;
 }
 
 // ---- the barostat's screening network (no reference counterpart) ----------
@@ -1180,6 +1241,8 @@ int surrogate_alloc(mdb_engine* e, Surrogate& net, int samples) {
   TRY(alloc(e, "surrogate targets", net.t, std::max(samples, 2)));
   TRY(alloc(e, "surrogate outputs", net.y, 2));
   TRY(alloc(e, "surrogate losses", net.loss, samples / kMlpBatch + 2));
+  TRY(alloc(e, "surrogate inference inputs", net.xi, size_t(e->d.S) * 2 * kMlpIn));
+  TRY(alloc(e, "surrogate inference outputs", net.yi, size_t(e->d.S) * 2));
 #undef TRY
   return MDB_OK;
 }
@@ -1238,133 +1301,192 @@ int surrogate_train(mdb_engine* e, Surrogate& net, uint32_t seed, int epochs) {
   return MDB_OK;
 }
 
-// Predicted potential change (kJ/mol) of a move dlnV from a state with these
-// energies and box, by one device forward pass.
-int surrogate_predict(mdb_engine* e, Surrogate& net, const HostSystem& h, const mdb_energies& en,
-                      const double* box, double dlnv, double* out) {
-  double f[kMlpIn];
-  surrogate_features(en, h, box, dlnv, f);
-  float x[kMlpIn];
-  for (int k = 0; k < kMlpIn; ++k) x[k] = float((f[k] - net.mu[k]) / net.sd[k]);
-  CUDA_TRY(e, cudaMemcpyAsync(net.x, x, sizeof(x), cudaMemcpyHostToDevice, e->s0));
-  launch_mlp_forward(net.dev.w_bf16, net.x, 1, net.y, e->s0);
-  float y = 0;
-  CUDA_TRY(e, cudaMemcpyAsync(&y, net.y, sizeof(float), cudaMemcpyDeviceToHost, e->s0));
+// Predicted potential changes (kJ/mol) of moves dlnv[i] from states with
+// energies en[i] and boxes box[i] of systems sys[i], by one device forward
+// pass over all of them.
+int surrogate_predict(mdb_engine* e, Surrogate& net, const std::vector<int>& sys, const mdb_energies* en,
+                      const std::vector<std::array<double, 9>>& box, const std::vector<double>& dlnv,
+                      std::vector<double>& out) {
+  const int n = int(sys.size());
+  out.assign(n, 0.0);
+  if (n == 0) return MDB_OK;
+  std::vector<float> x(size_t(n) * kMlpIn);
+  for (int i = 0; i < n; ++i) {
+    double f[kMlpIn];
+    surrogate_features(en[i], e->hs[sys[i]], box[i].data(), dlnv[i], f);
+    for (int k = 0; k < kMlpIn; ++k) x[size_t(i) * kMlpIn + k] = float((f[k] - net.mu[k]) / net.sd[k]);
+  }
+  std::vector<float> y(n);
+  CUDA_TRY(e, cudaMemcpyAsync(net.xi, x.data(), sizeof(float) * x.size(), cudaMemcpyHostToDevice, e->s0));
+  launch_mlp_forward(net.dev.w_bf16, net.xi, n, net.yi, e->s0);
+  CUDA_TRY(e, cudaMemcpyAsync(y.data(), net.yi, sizeof(float) * n, cudaMemcpyDeviceToHost, e->s0));
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  *out = first_order_change(en, dlnv) + (double(y) * net.sd_t + net.mu_t) * std::max(1, h.n) * dlnv * dlnv;
+  for (int i = 0; i < n; ++i)
+    out[i] = first_order_change(en[i], dlnv[i]) +
+             (double(y[i]) * net.sd_t + net.mu_t) * std::max(1, e->hs[sys[i]].n) * dlnv[i] * dlnv[i];
   return MDB_OK;
 }
 
+// threefry2x32([draw, seed], [BAROSTAT_DOMAIN, 0]) (loop.ts:614-622): the
+// barostat's next uniform number, one counter per system.
+double barostat_uniform(BarostatState& b, uint32_t seed) {
+  uint32_t c0 = uint32_t(b.draw++), c1 = seed, k0 = 0x6a09e667u, k1 = 0;
+  static const int rot[8] = {13, 15, 26, 6, 17, 29, 16, 24};
+  const uint32_t ks[3] = {k0, k1, 0x1bd11bdau ^ k0 ^ k1};
+  uint32_t x0 = c0 + ks[0], x1 = c1 + ks[1];
+  for (int r = 0; r < 20; ++r) {
+    x0 += x1;
+    x1 = ((x1 << rot[r % 8]) | (x1 >> (32 - rot[r % 8]))) ^ x0;
+    if ((r + 1) % 4 == 0) {
+      const uint32_t inj = uint32_t((r + 1) / 4);
+      x0 += ks[inj % 3];
+      x1 += ks[(inj + 1) % 3] + inj;
+    }
+  }
+  return (double(x0 >> 9) + 0.5) * std::ldexp(1.0, -23);
+}
+
 // Box and positions of a volume move, on the device: back up, scale every
-// molecule's centre, set the box (which requests the list rebuild).
+// molecule's centre, move the box (the list is kept unless an atom went too far).
 int apply_volume_move(mdb_engine* e, int s, double scale) {
   launch_scale_molecules(e->d, e->mol_first[s], e->mol_count[s], scale, e->s0);
   CUDA_TRY(e, cudaGetLastError());
   double nb[9];
   for (int i = 0; i < 9; ++i) nb[i] = e->hs[s].box[i] * scale;
-  return set_box(e, s, nb);
+  return move_box(e, s, nb);
 }
 
 int undo_volume_move(mdb_engine* e, int s, const std::array<double, 9>& old_box) {
   launch_restore_positions(e->d, e->sd[s].atom_off, e->sd[s].n_atoms, e->s0);
   CUDA_TRY(e, cudaGetLastError());
-  return set_box(e, s, old_box.data());
+  return move_box(e, s, old_box.data());
 }
 
-// One Monte Carlo volume move (src/gpu/loop.ts:602-641, src/reference/barostat.ts:210-274).
-// With a trained screening network the move goes through delayed acceptance
-// (Christen & Fox 2005): stage 1 accepts with a1 = min(1, exp(-w~/kT)) from
-// the network's predicted change, and only then is the exact energy of the
-// proposal computed; stage 2 accepts with min(1, exp(-w/kT) a1(y->x)/a1(x->y)),
-// the reverse move's stage-1 probability evaluated with the network at the
-// proposal, so the chain keeps the exact NPT distribution.
-int barostat_attempt(mdb_engine* e, int s) {
-  HostSystem& h = e->hs[s];
-  BarostatState& b = e->baro[s];
-  Surrogate& net = b.net;
-  mdb_energies e0{};
-  int st = evaluate(e, s, nullptr, &e0, false);
+// One Monte Carlo volume move for each system in `due` (src/gpu/loop.ts:602-641,
+// src/reference/barostat.ts:210-274), all of them together: one evaluation of
+// the engine gives every system's current energy, the moves are proposed and
+// applied, and one more evaluation gives the proposals' energies.  Each
+// system draws from its own counter, so a system's moves are the ones it
+// would make alone.  With a trained screening network the moves go through
+// delayed acceptance (Christen & Fox 2005): stage 1 accepts with
+// a1 = min(1, exp(-w~/kT)) from the network's predicted change, and only the
+// systems that pass go on to the exact energy; stage 2 accepts with
+// min(1, exp(-w/kT) a1(y->x)/a1(x->y)), the reverse move's stage-1
+// probability evaluated with the network at the proposal, so every chain
+// keeps the exact NPT distribution.
+int barostat_round(mdb_engine* e, const std::vector<int>& due) {
+  Surrogate& net = e->net;
+  const int n = int(due.size());
+  std::vector<mdb_energies> e0(n);
+  int st = evaluate_many(e, due, nullptr, e0.data(), false);
   if (st) return st;
-  auto uniform = [&]() {
-    // threefry2x32([draw, seed], [BAROSTAT_DOMAIN, 0]) (loop.ts:614-622)
-    uint32_t c0 = uint32_t(b.draw++), c1 = e->opt.seed, k0 = 0x6a09e667u, k1 = 0;
-    static const int rot[8] = {13, 15, 26, 6, 17, 29, 16, 24};
-    const uint32_t ks[3] = {k0, k1, 0x1bd11bdau ^ k0 ^ k1};
-    uint32_t x0 = c0 + ks[0], x1 = c1 + ks[1];
-    for (int r = 0; r < 20; ++r) {
-      x0 += x1;
-      x1 = ((x1 << rot[r % 8]) | (x1 >> (32 - rot[r % 8]))) ^ x0;
-      if ((r + 1) % 4 == 0) {
-        const uint32_t inj = uint32_t((r + 1) / 4);
-        x0 += ks[inj % 3];
-        x1 += ks[(inj + 1) % 3] + inj;
-      }
-    }
-    return (double(x0 >> 9) + 0.5) * std::ldexp(1.0, -23);
+  struct Move {
+    std::array<double, 9> old_box;
+    double volume, dv, scale, dlnv, volume_term, kT, a1 = 1.0;
+    bool exact = true;
   };
-  const std::array<double, 9> old_box = h.box;
-  const double volume = box_volume(h.box.data());
-  const double dv = b.volume_scale * 2 * (uniform() - 0.5);
-  const double nv = volume + dv;
-  const double scale = std::cbrt(nv / volume);
-  const double dlnv = std::log(nv / volume);
-  const double pressure = h.barostat_pressure * 0.06022140762081242;
-  const double kT = kBoltzmann * h.barostat_temperature;
-  const double volume_term = pressure * dv - double(h.molecules.size()) * kT * dlnv;
-  const bool screen = net.active && !net.disabled;
-  double a1 = 1.0, du_pred = 0.0;
-  if (screen) {
-    if ((st = surrogate_predict(e, net, h, e0, old_box.data(), dlnv, &du_pred))) return st;
-    a1 = std::min(1.0, std::exp(-(du_pred + volume_term) / kT));
+  std::vector<Move> mv(n);
+  for (int i = 0; i < n; ++i) {
+    const int s = due[i];
+    HostSystem& h = e->hs[s];
+    BarostatState& b = e->baro[s];
+    Move& m = mv[i];
+    m.old_box = h.box;
+    m.volume = box_volume(h.box.data());
+    m.dv = b.volume_scale * 2 * (barostat_uniform(b, e->opt.seed) - 0.5);
+    const double nv = m.volume + m.dv;
+    m.scale = std::cbrt(nv / m.volume);
+    m.dlnv = std::log(nv / m.volume);
+    m.kT = kBoltzmann * h.barostat_temperature;
+    m.volume_term = h.barostat_pressure * 0.06022140762081242 * m.dv - double(h.molecules.size()) * m.kT * m.dlnv;
   }
-  b.attempts++;
-  b.window_attempts++;
-  bool accepted = false;
-  if (screen && !(uniform() < a1)) {
-    b.screened++;  // rejected by the network alone: no exact evaluation
-  } else {
-    if ((st = apply_volume_move(e, s, scale))) return st;
-    mdb_energies e1{};
-    if ((st = evaluate(e, s, nullptr, &e1, false))) return st;
-    b.exact++;
-    const double du = e1.potential - e0.potential;
-    const double w = du + volume_term;
+  const bool screen = net.active && !net.disabled;
+  std::vector<double> du_pred;
+  if (screen) {
+    std::vector<std::array<double, 9>> boxes(n);
+    std::vector<double> dl(n);
+    for (int i = 0; i < n; ++i) {
+      boxes[i] = mv[i].old_box;
+      dl[i] = mv[i].dlnv;
+    }
+    if ((st = surrogate_predict(e, net, due, e0.data(), boxes, dl, du_pred))) return st;
+  }
+  std::vector<int> exact_sys;
+  std::vector<int> exact_idx;
+  for (int i = 0; i < n; ++i) {
+    BarostatState& b = e->baro[due[i]];
+    Move& m = mv[i];
+    b.attempts++;
+    b.window_attempts++;
     if (screen) {
-      double du_rev = 0.0;
-      if ((st = surrogate_predict(e, net, h, e1, h.box.data(), -dlnv, &du_rev))) return st;
-      const double a1_rev = std::min(1.0, std::exp(-(du_rev - volume_term) / kT));
-      const double a2 = std::min(1.0, std::exp(-w / kT) * a1_rev / a1);
-      accepted = uniform() < a2;
+      m.a1 = std::min(1.0, std::exp(-(du_pred[i] + m.volume_term) / m.kT));
+      m.exact = barostat_uniform(b, e->opt.seed) < m.a1;
+      if (!m.exact) b.screened++;  // rejected by the network alone: no exact evaluation
+    }
+    if (m.exact) {
+      if ((st = apply_volume_move(e, due[i], m.scale))) return st;
+      exact_sys.push_back(due[i]);
+      exact_idx.push_back(i);
+    }
+  }
+  std::vector<mdb_energies> e1(exact_sys.size());
+  if (!exact_sys.empty() && (st = evaluate_many(e, exact_sys, nullptr, e1.data(), false))) return st;
+  std::vector<double> du_rev;
+  if (screen && !exact_sys.empty()) {
+    std::vector<std::array<double, 9>> boxes(exact_sys.size());
+    std::vector<double> dl(exact_sys.size());
+    for (size_t k = 0; k < exact_sys.size(); ++k) {
+      boxes[k] = e->hs[exact_sys[k]].box;
+      dl[k] = -mv[exact_idx[k]].dlnv;
+    }
+    if ((st = surrogate_predict(e, net, exact_sys, e1.data(), boxes, dl, du_rev))) return st;
+  }
+  bool train = false;
+  for (size_t k = 0; k < exact_sys.size(); ++k) {
+    const int s = exact_sys[k], i = exact_idx[k];
+    HostSystem& h = e->hs[s];
+    BarostatState& b = e->baro[s];
+    Move& m = mv[i];
+    b.exact++;
+    const double du = e1[k].potential - e0[i].potential;
+    const double w = du + m.volume_term;
+    bool accepted = false;
+    if (screen) {
+      const double a1_rev = std::min(1.0, std::exp(-(du_rev[k] - m.volume_term) / m.kT));
+      const double a2 = std::min(1.0, std::exp(-w / m.kT) * a1_rev / m.a1);
+      accepted = barostat_uniform(b, e->opt.seed) < a2;
       // the exact stage checks the network's prediction
-      const double err = du_pred - du;
+      const double err = du_pred[i] - du;
       net.err2 = net.checked == 0 ? err * err : 0.98 * net.err2 + 0.02 * err * err;
-      if (++net.checked >= 50 && std::sqrt(net.err2) > kSurrogateMaxRmsKT * kT) net.disabled = true;
+      if (++net.checked >= 50 && std::sqrt(net.err2) > kSurrogateMaxRmsKT * m.kT) net.disabled = true;
     } else {
-      accepted = !(w > 0 && uniform() > std::exp(-w / kT));
+      accepted = !(w > 0 && barostat_uniform(b, e->opt.seed) > std::exp(-w / m.kT));
       if (net.target > 0 && !net.active) {
         double f[kMlpIn];
-        surrogate_features(e0, h, old_box.data(), dlnv, f);
+        surrogate_features(e0[i], h, m.old_box.data(), m.dlnv, f);
         for (double v : f) net.feats.push_back(float(v));
         // what the first-order term misses, per atom like the energy features
-        net.delta_u.push_back((du - first_order_change(e0, dlnv)) / std::max(1, h.n));
-        net.dlnv.push_back(dlnv);
-        if (int(net.delta_u.size()) >= net.target) {
-          if ((st = surrogate_train(e, net, e->opt.seed, 300))) return st;
-        }
+        net.delta_u.push_back((du - first_order_change(e0[i], m.dlnv)) / std::max(1, h.n));
+        net.dlnv.push_back(m.dlnv);
+        train |= int(net.delta_u.size()) >= net.target;
       }
     }
-    if (!accepted && (st = undo_volume_move(e, s, old_box))) return st;
+    if (accepted) {
+      b.accepted++;
+      b.window_accepted++;
+    } else if ((st = undo_volume_move(e, s, m.old_box))) {
+      return st;
+    }
   }
-  if (accepted) {
-    b.accepted++;
-    b.window_accepted++;
-  }
-  if (b.window_attempts >= 10) {
+  if (train && (st = surrogate_train(e, net, e->opt.seed, 300))) return st;
+  for (int i = 0; i < n; ++i) {
+    BarostatState& b = e->baro[due[i]];
+    if (b.window_attempts < 10) continue;
     if (b.window_accepted < 0.25 * b.window_attempts) {
       b.volume_scale /= 1.1;
       b.window_attempts = b.window_accepted = 0;
     } else if (b.window_accepted > 0.75 * b.window_attempts) {
-      b.volume_scale = std::min(b.volume_scale * 1.1, volume * 0.3);
+      b.volume_scale = std::min(b.volume_scale * 1.1, mv[i].volume * 0.3);
       b.window_attempts = b.window_accepted = 0;
     }
   }
@@ -1405,6 +1527,7 @@ int run(mdb_engine* e, int64_t steps) {
     }
     remaining -= chunk;
     if (freq > 0) {
+      std::vector<int> due;
       for (size_t s = 0; s < e->hs.size(); ++s) {
         auto& h = e->hs[s];
         auto& b = e->baro[s];
@@ -1412,8 +1535,9 @@ int run(mdb_engine* e, int64_t steps) {
         b.step += chunk;  // barostat.ts:129 barostatActsAfterSteps
         if (b.step < h.barostat_frequency) continue;
         b.step -= h.barostat_frequency;
-        if ((st = barostat_attempt(e, int(s)))) return st;
+        due.push_back(int(s));
       }
+      if (!due.empty() && (st = barostat_round(e, due))) return st;
     }
   }
   return check_device_status(e);
@@ -1670,7 +1794,7 @@ int mdb_get_barostat_stats(const mdb_engine* e, int32_t s, mdb_barostat_stats* o
   // the current state's energy every attempt, the proposal's when not screened
   out->exact_evaluations = e->baro[s].attempts + e->baro[s].exact;
   out->screened = e->baro[s].screened;
-  const Surrogate& net = e->baro[s].net;
+  const Surrogate& net = e->net;
   out->surrogate_active = net.active && !net.disabled ? 1 : 0;
   out->surrogate_disabled = net.disabled ? 1 : 0;
   out->training_samples = int64_t(net.delta_u.size());

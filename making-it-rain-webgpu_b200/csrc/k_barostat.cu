@@ -95,6 +95,55 @@ __global__ void __launch_bounds__(kThreads) k_molecular_offsets(Dev d, int first
   }
 }
 
+// After the box of system s changed by a small amount (a volume move or its
+// undo, positions scaled or restored): its slots' pair coordinates from the
+// new positions under the list's folds, its tiles' shifts from their lattice
+// counts and the new box, and the integrator's displacement tests -- half the
+// skin from the list's reference positions, half the inner skin from the last
+// prune's -- which here ask the list kernels for a rebuild or a prune
+// directly.  So the list survives the move unless an atom went too far.
+__global__ void __launch_bounds__(kThreads) k_after_box_change(Dev d, int s) {
+  const SysDev& S = d.sys[s];
+  const int n_tiles = min(d.tile_count[s], S.tile_cap);
+  const int n_inner = d.inner ? min(d.in_count[s], S.tile_cap) : 0;
+  const int n = max(S.n_slots, max(n_tiles, n_inner));
+  bool moved = false, strayed = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i < S.n_slots) {
+      const int gs = S.slot_off + i;
+      const int a = d.order[gs];
+      if (a >= 0) {
+        const long long x = d.px[a], y = d.py[a], z = d.pz[a];
+        long long na, nb, nc;
+        unpack_fold(d.fold[gs], na, nb, nc);
+        d.pc[gs] = pair_coordinate(S, x, y, z, na, nb, nc);
+        const float ex = from_fixed(x - d.refx[a]), ey = from_fixed(y - d.refy[a]), ez = from_fixed(z - d.refz[a]);
+        moved |= ex * ex + ey * ey + ez * ez > S.half_skin2;
+        if (d.inner) {
+          const float qx = from_fixed(x - d.prx[a]), qy = from_fixed(y - d.pry[a]), qz = from_fixed(z - d.prz[a]);
+          strayed |= qx * qx + qy * qy + qz * qz > S.half_inner2;
+        }
+      }
+    }
+    if (i < n_tiles) {
+      const long long t = static_cast<long long>(S.tile_off) + i;
+      d.tile_shift[t] = tile_shift_for(S, d.tile_shift[t].w);
+    }
+    if (i < n_inner) {
+      const long long t = static_cast<long long>(S.tile_off) + i;
+      d.in_shift[t] = tile_shift_for(S, d.in_shift[t].w);
+    }
+  }
+  if (moved) {
+    atomicExch(&d.rebuild_now[s], 1);
+    atomicExch(d.any_rebuild, 1);
+  }
+  if (strayed) {
+    atomicExch(&d.prune_now[s], 1);
+    atomicExch(d.any_prune, 1);
+  }
+}
+
 int blocks_for(int n) { return std::max(1, std::min((n + kThreads - 1) / kThreads, 148 * 8)); }
 
 }  // namespace
@@ -108,6 +157,10 @@ int molecular_offset_blocks(int n_mol) { return std::max(1, std::min((n_mol + kT
 void launch_molecular_offsets(const Dev& d, int first_mol, int n_mol, int slot_off, double* partials,
                               cudaStream_t st) {
   k_molecular_offsets<<<molecular_offset_blocks(n_mol), kThreads, 0, st>>>(d, first_mol, n_mol, slot_off, partials);
+}
+
+void launch_after_box_change(const Dev& d, int s, int n_slots, int tile_cap, cudaStream_t st) {
+  k_after_box_change<<<blocks_for(std::max(n_slots, tile_cap)), kThreads, 0, st>>>(d, s);
 }
 
 void launch_restore_positions(const Dev& d, int atom_off, int n, cudaStream_t st) {

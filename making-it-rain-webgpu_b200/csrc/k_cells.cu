@@ -327,7 +327,9 @@ __device__ __forceinline__ bool boxes_near(const SysDev& S, float4 li, float4 hi
 }
 
 // The lattice shift (in pair-coordinate units, applied to J) of the image
-// that brings box J nearest box I, as boxes_near finds it.  w = 1 when that
+// that brings box J nearest box I, as boxes_near finds it; w carries that
+// image's lattice counts (so a box change can recompute the shift without a
+// rebuild) and the per-pair flag, set when that
 // one image might not hold every pair of the tile within the cutoff: when
 // 2 (|h_I| + |h_J|) + list + cutoff reaches the cell's narrowest width (h the
 // half-diagonals), another image of some pair could come inside the cutoff,
@@ -380,7 +382,7 @@ __device__ __forceinline__ int4 tile_image(const SysDev& S, float4 li, float4 hi
   const float ej = 0.5f * sqrtf((hj.x - lj.x) * (hj.x - lj.x) + (hj.y - lj.y) * (hj.y - lj.y) +
                                 (hj.z - lj.z) * (hj.z - lj.z));
   const bool per_pair = 2.f * (ei + ej) + sqrtf(S.list2) + sqrtf(S.cut2) >= S.min_width;
-  return make_int4(int(sx), int(sy), int(sz), per_pair ? 1 : 0);
+  return make_int4(int(sx), int(sy), int(sz), tile_flags(per_pair, na, nb, nc));
 }
 
 // Position of the k-th (from 0) set bit of m, or -1.
@@ -535,7 +537,7 @@ __device__ void phase_tiles_prune(const Dev& d) {
       mask = (mask >> l) | (mask << ((C - l) & (C - 1)));  // bit k <-> j = l + k (mod C)
       const int4 pi = d.pc[tile.x * C + l];
       int4 pj = d.pc[tile.y * C + l];
-      if (!sh.w) {
+      if (!tile_per_pair(sh.w)) {
         pj.x = int(unsigned(pj.x) + unsigned(sh.x));
         pj.y = int(unsigned(pj.y) + unsigned(sh.y));
         pj.z = int(unsigned(pj.z) + unsigned(sh.z));
@@ -545,7 +547,7 @@ __device__ void phase_tiles_prune(const Dev& d) {
       for (int k = 0; k < C; ++k) {
         int dx = int(unsigned(pj.x) - unsigned(pi.x)), dy = int(unsigned(pj.y) - unsigned(pi.y)),
             dz = int(unsigned(pj.z) - unsigned(pi.z));
-        if (sh.w) {
+        if (tile_per_pair(sh.w)) {
           if (S.triclinic) min_image<true>(S, dx, dy, dz);
           else min_image<false>(S, dx, dy, dz);
         }
@@ -682,7 +684,7 @@ __device__ bool tile_within_reach<8>(const Dev& d, const SysDev& S, long long ti
   const int2 tile = __ldcg(&d.tiles[ti]);
   const int4 sh = __ldcg(&d.tile_shift[ti]);
   const float inv = S.pc_inv;
-  if (sh.w) {
+  if (tile_per_pair(sh.w)) {
     if (!S.prune_per_pair) return true;
     // per-pair images (small cells): the pair kernel's own minimum image of each pair
     const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
@@ -752,7 +754,7 @@ __device__ bool tile_within_reach<32>(const Dev& d, const SysDev& S, long long t
   const int4 sh = __ldcg(&d.tile_shift[ti]);
   const unsigned int row = __ldcg(&d.masks[ti * 32 + l]);
   const unsigned int cols = __reduce_or_sync(0xffffffffu, row);
-  if (sh.w) return true;  // warp-uniform: one tile per warp
+  if (tile_per_pair(sh.w)) return true;  // warp-uniform: one tile per warp
   const float inv = S.pc_inv;
   const float4 ilo = d.cb_lo[tile.x], ihi = d.cb_hi[tile.x];
   const float4 jlo = d.cb_lo[tile.y], jhi = d.cb_hi[tile.y];

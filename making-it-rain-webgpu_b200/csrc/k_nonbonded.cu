@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
         pj = d.pc[gj];
         qj = d.prm[gj];
         const int4 sh = d.tile_shift[ti];
-        per_pair = sh.w != 0;
+        per_pair = tile_per_pair(sh.w);
         if (!per_pair) {
           pj.x = int(unsigned(pj.x) + unsigned(sh.x));
           pj.y = int(unsigned(pj.y) + unsigned(sh.y));

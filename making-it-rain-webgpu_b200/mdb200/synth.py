@@ -265,7 +265,7 @@ def _perpendicular_min(box: np.ndarray) -> float:
                      v / np.linalg.norm(np.cross(a, b))))
 
 
-def ensemble_member(rng: np.random.Generator, seed: int, cutoff: float = 1.0):
+def ensemble_member(rng: np.random.Generator, seed: int, cutoff: float = 1.0, barostat=None):
     """One system of the batched ensemble: a target atom count drawn
     log-uniformly from 2,000 to 30,000, a cubic or rhombic-dodecahedral cell of
     TIP3P sized to it, and, half the time, an Ala helix of 10-40 residues when
@@ -290,20 +290,26 @@ def ensemble_member(rng: np.random.Generator, seed: int, cutoff: float = 1.0):
     if residues < 10:
         residues = 0
     if residues:
-        system, state = solvated(solute, x, width=width, shape=shape, seed=seed)
+        system, state = solvated(solute, x, width=width, shape=shape, seed=seed, barostat=barostat)
     else:
-        system, state = water_box(width=width, shape=shape, seed=seed)
+        system, state = water_box(width=width, shape=shape, seed=seed, barostat=barostat)
     return system, state, {"shape": shape, "width": width, "helix_residues": residues,
                            "atoms": system.particle_count}
 
 
-def config_ensemble_64(seed: int = 1, count: int = 64):
+def config_ensemble_64(seed: int = 1, count: int = 64, barostat=None):
     """The batched ensemble: `count` independent systems of uneven sizes."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(count):
-        out.append(ensemble_member(rng, seed=seed * 1000 + k))
+        out.append(ensemble_member(rng, seed=seed * 1000 + k, barostat=barostat))
     return out
+
+
+def config_npt_ensemble_64(seed: int = 1, count: int = 64, frequency: int = 25):
+    """The batched ensemble under NPT: the same 64 systems, each with a Monte
+    Carlo barostat at 1 bar and 300 K, a volume move every 25 steps."""
+    return config_ensemble_64(seed=seed, count=count, barostat=(1.0, 300.0, frequency))
 
 
 def config_npt_100k(seed: int = 1, width: float = 10.0, frequency: int = 25):

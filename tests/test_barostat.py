@@ -180,3 +180,32 @@ def test_screened_and_plain_barostat_sample_the_same_volume_distribution():
     assert gap < bound
     ratio = samples["screened"].std() / samples["plain"].std()
     assert 0.75 < ratio < 1.25, ratio
+
+
+def test_batched_barostat_rounds_move_each_system_as_it_moves_alone():
+    """Systems whose barostats are due together attempt in one round -- one
+    evaluation of the engine for their current energies, one for their
+    proposals -- and each draws from its own counter, so a system in a batch
+    makes exactly the moves it makes alone: positions, boxes and barostat
+    counts bit-identical."""
+    from mdb200 import steploop, synth
+
+    members = [synth.water_box(n_waters=700, width=2.8, seed=4, grid=(28, 28, 28), barostat=(1.0, 300.0, 5)),
+               synth.water_box(n_waters=900, width=3.1, seed=5, grid=(32, 32, 32), barostat=(1.0, 300.0, 5))]
+    opts = steploop.RunOptions(seed=9)
+    alone = []
+    for system, state in members:
+        loop = steploop.StepLoop.from_parsed(system, state, opts)
+        loop.run(200)
+        alone.append((loop.positions(), loop.box_vectors(), loop.barostat_statistics(), loop.verlet_flags()))
+        loop.destroy()
+    batch = steploop.StepLoop.batch([m[0] for m in members], [m[1] for m in members], opts)
+    batch.run(200)
+    for k, (p, b, st, fl) in enumerate(alone):
+        got = batch.barostat_statistics(k)
+        print("system", k, "alone", st, fl, "batch", got)
+        assert got["attempts"] == st["attempts"] == 40 and got["accepted"] == st["accepted"]
+        assert np.array_equal(batch.box_vectors(k), b)
+        assert np.array_equal(batch.positions(k), p)
+        assert st["accepted"] >= 5
+    batch.destroy()
