@@ -62,6 +62,11 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate
 # one ncu capture per workload with the configuration the autotuner picks
 # (other workloads report null)
 NB_TRAFFIC = {"octa-27k": 11175936, "peptide-12k": 5061632}
+# DRAM bytes per inner-list tile read, from one ncu capture of the ensemble's
+# pair kernel (326.44 MB read + 14.78 MB written over 9,279,094 tiles): the
+# ensemble's tile count follows its autotuned list settings, so its traffic is
+# this figure times the tiles the timed engine reads
+NB_TRAFFIC_PER_TILE = {"ensemble-64": 341.22e6 / 9279094}
 # the north star's single-system target, ns/day on the 27k-atom system
 NORTH_STAR_NS_PER_DAY = 1000.0
 
@@ -368,9 +373,12 @@ def main() -> None:
                     help="skin,sort_cell,tile_atoms,prune_tiles[,inner_skin]: skip the autotuner (profiling runs)")
     ap.add_argument("--phase-launches", action="store_true",
                     help="list build as separate kernel launches, one per phase (profiling runs)")
+    ap.add_argument("--tune", choices=("batch", "single"), default="batch",
+                    help="ensembles: the autotuner searches each size bucket on its systems batched "
+                         "together, or on its median-sized system alone")
     ap.add_argument("--no-plain", action="store_true",
                     help="ensemble: skip the plain per-system engines (profiling runs)")
-    ap.add_argument("--ensemble-surrogate-attempts", type=int, default=1280,
+    ap.add_argument("--ensemble-surrogate-attempts", type=int, default=2560,
                     help="npt-ensemble-64: exact attempts, pooled over the 64 systems, the network learns from")
     ap.add_argument("--surrogate-attempts", type=int, default=2000,
                     help="npt-100k: exact attempts the screening network learns from (2,000 = 50,000 steps)")
@@ -419,6 +427,15 @@ def main() -> None:
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     stride = min(args.stride, args.steps)
     strides = [stride] * (args.steps // stride) + ([args.steps % stride] if args.steps % stride else [])
+
+    def tune_buckets(systems, states):
+        """The list settings per size bucket (untimed): searched on each
+        bucket's systems batched together (`--tune batch`, how the timed engine
+        runs them) or on its median-sized system alone (`--tune single`)."""
+        if args.tune == "batch":
+            return steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=100,
+                                           batched=True)
+        return steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=400)
 
     def timed(loop, on_stride=None) -> tuple[float, dict]:
         """Warm-up, then exactly args.steps steps as timed strides; device seconds.
@@ -493,8 +510,11 @@ def main() -> None:
             "gather_GBs": gather_bytes / (prof["ms_pme_gather"] / 1000) / 1e9,
             "integrate_GBs": integ_bytes / (prof["ms_integrate"] / 1000) / 1e9,
         }
+        traffic = NB_TRAFFIC.get(config)
+        if config in NB_TRAFFIC_PER_TILE:
+            traffic = round(NB_TRAFFIC_PER_TILE[config] * prof["inner_tiles"])
         return {"bound": "fp32", "kernel": "k_nonbonded", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
-                "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": NB_TRAFFIC.get(config),
+                "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": traffic,
                 "peak_source": "nominal FP32 issue rate, 148 SM x 128 lanes x 2 flop x 1.965 GHz",
                 "algorithmic": f"{FLOP_PER_PAIR:.0f} flop x {pairs} in-cutoff pairs per launch",
                 "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0), "hbm_peak_source":
@@ -541,7 +561,7 @@ def main() -> None:
             fixed = (fixed[0], fixed[1], int(fixed[2]), int(fixed[3])) + fixed[4:]
             tuning, buckets = [fixed] * len(systems), {"all": {"source": "--tuning " + args.tuning}}
         else:
-            tuning, buckets = steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=400)
+            tuning, buckets = tune_buckets(systems, states)
         # the plain engines again with the batch's tuning, to separate the gain of
         # batching from the autotuner's
         plain_tuned_ms = None if args.no_plain else plain_engines(tuning)
@@ -601,8 +621,7 @@ def main() -> None:
             tuning, buckets = [fixed] * len(systems), {"all": {"source": "--tuning " + args.tuning}}
         else:
             nvt = synth.config_ensemble_64(seed=1)
-            tuning, buckets = steploop.tune_by_bucket([nvt[i][0] for i in share], [nvt[i][1] for i in share],
-                                                      steploop.RunOptions(device=local), steps=400)
+            tuning, buckets = tune_buckets([nvt[i][0] for i in share], [nvt[i][1] for i in share])
         plain_steps = max(4, min(args.steps, 200) // frequency) * frequency
         plain_ms = None
         if not args.no_plain:

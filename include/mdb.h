@@ -447,6 +447,17 @@ int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, con
                  int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried);
 
 /*
+ * The same search on a batch: every candidate is applied to all `n` systems
+ * of one batched engine (as mdb_batch_create), and the time is that engine's
+ * step.  A batch keeps the device busy where one small system leaves it
+ * waiting on launches, so the candidate that wins for a batch of a size
+ * bucket's systems can differ from the one that wins for any one of them.
+ */
+int mdb_autotune_batch(int32_t n, const mdb_system_desc* systems, const mdb_state_desc* states,
+                       const mdb_run_options* options, int32_t steps, mdb_tuning* best, double* best_ms_per_step,
+                       int32_t* tried);
+
+/*
  * The barostat screening network's kernels on their own (no reference
  * counterpart), for checking them against a CPU restatement.  Layout of
  * `params` (kMlpParams = 5313 floats): W1[64][16], b1[64], W2[64][64], b2[64],

@@ -27,6 +27,9 @@ struct Dev {
   int prune;          // rebuilds drop tiles with no pair inside cutoff + skin
   int inner;          // the pair kernel reads the inner list (see in_tiles)
   int any_triclinic;  // some system's box is triclinic: the pair kernel takes the general minimum image
+  // nullptr, or per system 1 if the force kernels should compute it: an
+  // evaluation of some of the systems (a barostat round's proposals) skips the others
+  const unsigned char* active;
 
   // atoms, original order
   long long *px, *py, *pz;
@@ -44,6 +47,10 @@ struct Dev {
 
   // slots, sorted order
   int* order;     // global atom or -1
+  // the order as the last integrator step saw it, kept only when the PME
+  // spread goes by slot (spread_sorted): the spread reads this copy
+  int* spread_atom;
+  int spread_sorted;
   int* tmp_order;
   int4* pc;
   float4* prm;
@@ -150,6 +157,8 @@ struct Dev {
   int* shake_failures;
 };
 
+__device__ __forceinline__ bool sys_active(const Dev& d, int s) { return d.active == nullptr || d.active[s] != 0; }
+
 // ---- launchers (one per kernel file) ----
 int prepare_list_kernel(int device);                      // 0: no cooperative launch
 bool launch_list(const Dev& d, cudaStream_t s);            // sort + wrap + tiles, one launch
@@ -160,6 +169,7 @@ void launch_inner_prune(const Dev& d, cudaStream_t s);      // the inner list, w
 void launch_nonbonded(const Dev& d, bool energy, cudaStream_t s);
 void launch_listed(const Dev& d, bool energy, cudaStream_t s);
 void launch_pme(const Dev& d, bool energy, cudaStream_t s);
+bool spread_by_slot(int n_slots);  // whether an engine of n_slots slots spreads PME charges by slot
 void launch_pme_spread(const Dev& d, cudaStream_t s);
 void launch_pme_fft(const Dev& d, bool energy, cudaStream_t s);
 void launch_pme_gather(const Dev& d, cudaStream_t s);

@@ -120,6 +120,7 @@ struct mdb_engine {
   std::vector<double> sort_cell;   // per system, nm
   std::vector<double> inner_skin;  // per system, nm; <= 0: that system's inner list is its outer list
   int64_t list_grown = 0;          // times an overflowing list was grown and rebuilt
+  unsigned char* active = nullptr;  // device: per system, whether an evaluation computes it
   std::vector<std::array<double, 9>> box_at_rebuild;  // per system: the box when a box change last asked for a rebuild
 };
 
@@ -320,9 +321,11 @@ void list_kernels(mdb_engine* e, cudaStream_t st) {
   launch_inner_prune(e->d, st);
 }
 
-// One step on three streams: the PME spread and transforms depend only on the
-// positions, so they start at once and overlap the list kernels; the gather
-// and the listed terms write forces by slot and wait for the list.
+// One step on three streams: the PME spread and transforms fork off at the
+// start and run on a high-priority stream beside the list kernels (which
+// return at once unless a rebuild or a prune is due); the gather and the
+// listed terms, which write forces by slot, wait for the list; the pair kernel
+// follows the list; all join before the integrator.
 void launch_step(mdb_engine* e) {
   const Dev& d = e->d;
   cudaEventRecord(e->fork, e->s0);
@@ -761,6 +764,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(upload(e, "pair parameters by atom", prm_atom_dev, prm_atom));
   d.prm_atom = prm_atom_dev;
   TRY(alloc(e, "order", d.order, slots));
+  d.spread_sorted = spread_by_slot(int(slots)) ? 1 : 0;
+  TRY(alloc(e, "spread order", d.spread_atom, d.spread_sorted ? slots : 1));
   TRY(alloc(e, "scatter order", d.tmp_order, slots));
   TRY(alloc(e, "pair coordinates", d.pc, slots));
   TRY(alloc(e, "pair parameters", d.prm, slots));
@@ -812,6 +817,8 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   TRY(alloc(e, "tile count", d.tile_count, n));
   TRY(alloc(e, "tile need", d.tile_need, n));
   TRY(alloc(e, "list halt", d.halt, 1));
+  TRY(alloc(e, "evaluated systems", e->active, n));
+  d.active = nullptr;
   TRY(alloc(e, "tile prefix", d.tile_prefix, n + 1));
   TRY(alloc(e, "rebuild flag", d.rebuild_flag, n));
   TRY(alloc(e, "rebuild now", d.rebuild_now, n));
@@ -948,6 +955,10 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     if (!halted || attempt == 4) break;
     if (const int st = grow_tile_list(e)) return st;
   }
+  // the slot-ordered spread's copy of the order, until the first step writes it
+  if (e->d.spread_sorted)
+    CUDA_TRY(e, cudaMemcpyAsync(e->d.spread_atom, e->d.order, sizeof(int) * size_t(e->d.n_slots),
+                                cudaMemcpyDeviceToDevice, e->s0));
   launch_momentum(e->d, e->s0);
   CUDA_TRY(e, cudaGetLastError());
   int status = check_device_status(e);
@@ -989,9 +1000,18 @@ int evaluate_many(mdb_engine* e, const std::vector<int>& systems, double* forces
     if (!halted || attempt == 4) break;
     if (const int st = grow_tile_list(e)) return st;
   }
-  launch_pme(d, true, e->s0);
-  launch_listed(d, true, e->s0);
-  launch_nonbonded(d, true, e->s0);
+  // the force kernels skip the systems not asked for
+  Dev dv = d;
+  if (int(systems.size()) < d.S) {
+    std::vector<unsigned char> on(d.S, 0);
+    for (int s : systems) on[s] = 1;
+    CUDA_TRY(e, cudaMemcpyAsync(e->active, on.data(), d.S, cudaMemcpyHostToDevice, e->s0));
+    CUDA_TRY(e, cudaStreamSynchronize(e->s0));  // `on` is pageable host memory
+    dv.active = e->active;
+  }
+  launch_pme(dv, true, e->s0);
+  launch_listed(dv, true, e->s0);
+  launch_nonbonded(dv, true, e->s0);
   CUDA_TRY(e, cudaGetLastError());
   int st = check_device_status(e);
   if (st) return st;
@@ -1019,6 +1039,8 @@ int evaluate_many(mdb_engine* e, const std::vector<int>& systems, double* forces
     }
   }
   if (out) {
+    std::vector<double> mol_all(size_t(e->mol_part_off.back() + molecular_offset_blocks(e->mol_count.back())) * 9);
+    CUDA_TRY(e, cudaMemcpy(mol_all.data(), e->mol_partials, sizeof(double) * mol_all.size(), cudaMemcpyDeviceToHost));
     std::vector<unsigned long long> en(size_t(d.S) * kECount);
     CUDA_TRY(e, cudaMemcpy(en.data(), d.energy, sizeof(long long) * en.size(), cudaMemcpyDeviceToHost));
     std::vector<double> mesh(e->n_mesh_items), mesh_vir(size_t(e->n_mesh_items) * 6);
@@ -1030,9 +1052,9 @@ int evaluate_many(mdb_engine* e, const std::vector<int>& systems, double* forces
       const SysDev& S = e->sd[s];
       mdb_energies& o = out[i];
       std::memset(&o, 0, sizeof(o));
-      std::vector<double> mol_part(size_t(molecular_offset_blocks(e->mol_count[s])) * 9);
-      CUDA_TRY(e, cudaMemcpy(mol_part.data(), e->mol_partials + size_t(e->mol_part_off[s]) * 9,
-                             sizeof(double) * mol_part.size(), cudaMemcpyDeviceToHost));
+      const std::vector<double> mol_part(mol_all.begin() + size_t(e->mol_part_off[s]) * 9,
+                                         mol_all.begin() + size_t(e->mol_part_off[s] +
+                                                                  molecular_offset_blocks(e->mol_count[s])) * 9);
       auto val = [&](int k) { return double((long long)en[size_t(S.energy_base) + k]) / 4294967296.0; };
       double em = 0, wm[6] = {0, 0, 0, 0, 0, 0};
       for (int k = 0; k < e->n_mesh_items; ++k)
@@ -1155,7 +1177,7 @@ int set_box(mdb_engine* e, int s, const double* box) {
   return request_rebuild(e, s);
 }
 
-// A volume move's box change (or its undo) that keeps the tile list: the
+// Volume moves' box changes (or their undo) that keep the tile list: the
 // tiles' shifts follow the new box from their lattice counts, the pair
 // coordinates follow the scaled positions, and a device displacement test asks
 // for a rebuild only if some atom has gone half the skin from the list's
@@ -1163,29 +1185,46 @@ int set_box(mdb_engine* e, int s, const double* box) {
 // pair-coordinate scale changes or the box has drifted by more than 1% per
 // axis since the engine last asked for one on a box change: the tiles'
 // per-pair flags were set for the box the list was built in.
-int move_box(mdb_engine* e, int s, const double* box) {
-  HostSystem& h = e->hs[s];
-  double reduced[9];
-  if (!reduce_box(box, reduced)) return fail(e, MDB_ERR_INVALID_ARGUMENT, "degenerate box");
-  double widths[3];
-  perpendicular_widths(reduced, widths);
-  if (h.cutoff > 0.5 * std::min({widths[0], widths[1], widths[2]}))
-    return fail(e, MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX, "the cutoff does not fit the new box");
-  std::copy(reduced, reduced + 9, h.box.begin());
-  update_box_constants(h);
-  const int shift = e->sd[s].pc_shift;
-  fill_box(h, e->sd[s], true);
-  bool rebuild = e->sd[s].pc_shift != shift;
-  for (int k = 0; k < 3; ++k)
-    rebuild |= std::fabs(reduced[4 * k] / e->box_at_rebuild[s][4 * k] - 1.0) > 0.01;
-  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
-  CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys) + s, &e->sd[s], sizeof(SysDev), cudaMemcpyHostToDevice));
-  if (rebuild) {
-    std::copy(reduced, reduced + 9, e->box_at_rebuild[s].begin());
-    return request_rebuild(e, s);
+int move_boxes(mdb_engine* e, const std::vector<int>& sys, const std::vector<std::array<double, 9>>& boxes) {
+  if (sys.empty()) return MDB_OK;
+  std::vector<int> rebuild;
+  for (size_t i = 0; i < sys.size(); ++i) {
+    const int s = sys[i];
+    HostSystem& h = e->hs[s];
+    double reduced[9];
+    if (!reduce_box(boxes[i].data(), reduced)) return fail(e, MDB_ERR_INVALID_ARGUMENT, "degenerate box");
+    double widths[3];
+    perpendicular_widths(reduced, widths);
+    if (h.cutoff > 0.5 * std::min({widths[0], widths[1], widths[2]}))
+      return fail(e, MDB_ERR_CUTOFF_TOO_LARGE_FOR_BOX, "the cutoff does not fit the new box");
+    std::copy(reduced, reduced + 9, h.box.begin());
+    update_box_constants(h);
+    const int shift = e->sd[s].pc_shift;
+    fill_box(h, e->sd[s], true);
+    bool again = e->sd[s].pc_shift != shift;
+    for (int k = 0; k < 3; ++k) again |= std::fabs(reduced[4 * k] / e->box_at_rebuild[s][4 * k] - 1.0) > 0.01;
+    if (again) {
+      std::copy(reduced, reduced + 9, e->box_at_rebuild[s].begin());
+      rebuild.push_back(s);
+    }
   }
-  launch_after_box_change(e->d, s, e->sd[s].n_slots, e->sd[s].tile_cap, e->s0);
+  // every system's constants in one copy, after the work already queued
+  CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+  CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys), e->sd.data(), sizeof(SysDev) * e->d.S,
+                         cudaMemcpyHostToDevice));
+  for (int s : sys)
+    if (std::find(rebuild.begin(), rebuild.end(), s) == rebuild.end())
+      launch_after_box_change(e->d, s, e->sd[s].n_slots, e->sd[s].tile_cap, e->s0);
   CUDA_TRY(e, cudaGetLastError());
+  if (!rebuild.empty()) {
+    std::vector<int> now(e->d.S, 0);
+    CUDA_TRY(e, cudaStreamSynchronize(e->s0));
+    CUDA_TRY(e, cudaMemcpy(now.data(), e->d.rebuild_now, sizeof(int) * e->d.S, cudaMemcpyDeviceToHost));
+    for (int s : rebuild) now[s] = 1;
+    const int one = 1;
+    CUDA_TRY(e, cudaMemcpy(e->d.rebuild_now, now.data(), sizeof(int) * e->d.S, cudaMemcpyHostToDevice));
+    CUDA_TRY(e, cudaMemcpy(e->d.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+  }
   return MDB_OK;
 }
 
@@ -1346,20 +1385,23 @@ double barostat_uniform(BarostatState& b, uint32_t seed) {
   return (double(x0 >> 9) + 0.5) * std::ldexp(1.0, -23);
 }
 
-// Box and positions of a volume move, on the device: back up, scale every
-// molecule's centre, move the box (the list is kept unless an atom went too far).
-int apply_volume_move(mdb_engine* e, int s, double scale) {
-  launch_scale_molecules(e->d, e->mol_first[s], e->mol_count[s], scale, e->s0);
+// Boxes and positions of volume moves, on the device: back up, scale every
+// molecule's centre, move the boxes (the list is kept unless an atom went too far).
+int apply_volume_moves(mdb_engine* e, const std::vector<int>& sys, const std::vector<double>& scale) {
+  std::vector<std::array<double, 9>> boxes(sys.size());
+  for (size_t i = 0; i < sys.size(); ++i) {
+    const int s = sys[i];
+    launch_scale_molecules(e->d, e->mol_first[s], e->mol_count[s], scale[i], e->s0);
+    for (int k = 0; k < 9; ++k) boxes[i][k] = e->hs[s].box[k] * scale[i];
+  }
   CUDA_TRY(e, cudaGetLastError());
-  double nb[9];
-  for (int i = 0; i < 9; ++i) nb[i] = e->hs[s].box[i] * scale;
-  return move_box(e, s, nb);
+  return move_boxes(e, sys, boxes);
 }
 
-int undo_volume_move(mdb_engine* e, int s, const std::array<double, 9>& old_box) {
-  launch_restore_positions(e->d, e->sd[s].atom_off, e->sd[s].n_atoms, e->s0);
+int undo_volume_moves(mdb_engine* e, const std::vector<int>& sys, const std::vector<std::array<double, 9>>& old_box) {
+  for (int s : sys) launch_restore_positions(e->d, e->sd[s].atom_off, e->sd[s].n_atoms, e->s0);
   CUDA_TRY(e, cudaGetLastError());
-  return move_box(e, s, old_box.data());
+  return move_boxes(e, sys, old_box);
 }
 
 // One Monte Carlo volume move for each system in `due` (src/gpu/loop.ts:602-641,
@@ -1424,10 +1466,14 @@ int barostat_round(mdb_engine* e, const std::vector<int>& due) {
       if (!m.exact) b.screened++;  // rejected by the network alone: no exact evaluation
     }
     if (m.exact) {
-      if ((st = apply_volume_move(e, due[i], m.scale))) return st;
       exact_sys.push_back(due[i]);
       exact_idx.push_back(i);
     }
+  }
+  {
+    std::vector<double> scales;
+    for (int i : exact_idx) scales.push_back(mv[i].scale);
+    if ((st = apply_volume_moves(e, exact_sys, scales))) return st;
   }
   std::vector<mdb_energies> e1(exact_sys.size());
   if (!exact_sys.empty() && (st = evaluate_many(e, exact_sys, nullptr, e1.data(), false))) return st;
@@ -1442,6 +1488,8 @@ int barostat_round(mdb_engine* e, const std::vector<int>& due) {
     if ((st = surrogate_predict(e, net, exact_sys, e1.data(), boxes, dl, du_rev))) return st;
   }
   bool train = false;
+  std::vector<int> undo_sys;
+  std::vector<std::array<double, 9>> undo_box;
   for (size_t k = 0; k < exact_sys.size(); ++k) {
     const int s = exact_sys[k], i = exact_idx[k];
     HostSystem& h = e->hs[s];
@@ -1474,10 +1522,12 @@ int barostat_round(mdb_engine* e, const std::vector<int>& due) {
     if (accepted) {
       b.accepted++;
       b.window_accepted++;
-    } else if ((st = undo_volume_move(e, s, m.old_box))) {
-      return st;
+    } else {
+      undo_sys.push_back(s);
+      undo_box.push_back(m.old_box);
     }
   }
+  if ((st = undo_volume_moves(e, undo_sys, undo_box))) return st;
   if (train && (st = surrogate_train(e, net, e->opt.seed, 300))) return st;
   for (int i = 0; i < n; ++i) {
     BarostatState& b = e->baro[due[i]];
@@ -1635,7 +1685,13 @@ int mdb_system_count(const mdb_engine* e, int32_t* out) {
 // (which lets a long skin keep a short pair list).
 int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, const mdb_run_options* options,
                  int32_t steps, mdb_tuning* best, double* best_ms_per_step, int32_t* tried) {
-  if (!system || !state || !options || !best || steps <= 0) return MDB_ERR_INVALID_ARGUMENT;
+  return mdb_autotune_batch(1, system, state, options, steps, best, best_ms_per_step, tried);
+}
+
+int mdb_autotune_batch(int32_t n, const mdb_system_desc* systems, const mdb_state_desc* states,
+                       const mdb_run_options* options, int32_t steps, mdb_tuning* best, double* best_ms_per_step,
+                       int32_t* tried) {
+  if (n <= 0 || !systems || !states || !options || !best || steps <= 0) return MDB_ERR_INVALID_ARGUMENT;
   struct Lists { double skin, inner; };
   static const Lists kLists8[] = {{0.15, -1.0}, {0.20, -1.0}, {0.30, 0.08}, {0.40, 0.08}, {0.50, 0.10}};
   static const Lists kLists32[] = {{0.15, -1.0}, {0.20, -1.0}};
@@ -1653,9 +1709,10 @@ int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, con
   int count = 0, last = MDB_OK;
   for (const mdb_tuning& t : grid) {
     mdb_run_options o = *options;
-    o.tuning = &t;
+    const std::vector<mdb_tuning> every(size_t(n), t);
+    o.tuning = every.data();
     mdb_engine* e = nullptr;
-    int st = mdb_batch_create(1, system, state, &o, &e);
+    int st = mdb_batch_create(n, systems, states, &o, &e);
     double ms = 0;
     if (st == MDB_OK) st = mdb_run(e, steps);  // warm-up: lists, graph capture
     if (st == MDB_OK) st = mdb_run_timed(e, steps, &ms);
@@ -1864,8 +1921,11 @@ int mdb_profile_step(mdb_engine* e, int32_t repeats, mdb_profile* out) {
     return double(ms) / repeats;
   };
   // pairs and tiles at this configuration
-  mdb_energies en{};
-  int status = evaluate(e, 0, nullptr, &en);
+  // every system (the pair counts below are the whole launch's)
+  std::vector<int> all(d.S);
+  std::iota(all.begin(), all.end(), 0);
+  std::vector<mdb_energies> en(d.S);
+  int status = evaluate_many(e, all, nullptr, en.data(), false);
   if (status) return status;
   // pairs of every system of the engine: the pair kernel's launch covers them all
   {

@@ -668,6 +668,7 @@ __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
       long long na, nb, nc;
       unpack_fold(d.fold[gs], na, nb, nc);
       d.pc[gs] = pair_coordinate(S, px, py, pz, na, nb, nc);
+      if (d.spread_sorted) d.spread_atom[gs] = a;  // the next step's spread reads this, not the order a rebuild rewrites
     }
     const float ex = from_fixed(px - d.refx[a]), ey = from_fixed(py - d.refy[a]),
                 ez = from_fixed(pz - d.refz[a]);

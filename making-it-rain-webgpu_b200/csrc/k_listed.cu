@@ -229,11 +229,17 @@ __global__ void __launch_bounds__(kThreads) k_listed(Dev d) {
   const int n0 = d.n_bonds, n1 = n0 + d.n_angles, n2 = n1 + d.n_torsions, n3 = n2 + d.n_exceptions,
             n4 = n3 + d.n_restraints;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
-    if (i < n0) bond<ENERGY>(d, d.bonds[i]);
-    else if (i < n1) angle<ENERGY>(d, d.angles[i - n0]);
-    else if (i < n2) torsion<ENERGY>(d, d.torsions[i - n1]);
-    else if (i < n3) exception<ENERGY>(d, d.exceptions[i - n2]);
-    else restraint<ENERGY>(d, d.restraints[i - n3]);
+    if (i < n0) {
+      if (sys_active(d, d.bonds[i].sys)) bond<ENERGY>(d, d.bonds[i]);
+    } else if (i < n1) {
+      if (sys_active(d, d.angles[i - n0].sys)) angle<ENERGY>(d, d.angles[i - n0]);
+    } else if (i < n2) {
+      if (sys_active(d, d.torsions[i - n1].sys)) torsion<ENERGY>(d, d.torsions[i - n1]);
+    } else if (i < n3) {
+      if (sys_active(d, d.exceptions[i - n2].sys)) exception<ENERGY>(d, d.exceptions[i - n2]);
+    } else if (sys_active(d, d.restraints[i - n3].sys)) {
+      restraint<ENERGY>(d, d.restraints[i - n3]);
+    }
   }
 }
 

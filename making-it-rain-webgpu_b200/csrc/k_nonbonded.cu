@@ -175,6 +175,14 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   for (int t0 = warp * kTilesPerWarp; t0 < total; t0 += nwarps * kTilesPerWarp) {
     const int tend = min(total, t0 + kTilesPerWarp);
     int s = find_system(d.tile_prefix, d.S, min(t0 + g, tend - 1));
+    if (ENERGY && d.active) {
+      // an evaluation of some systems only (energy evaluations; a step's
+      // force launches compute every system): a chunk that lies inside one
+      // skipped system is skipped by the whole warp; in a mixed chunk the
+      // skipped system's tiles run with an empty mask
+      const int first = find_system(d.tile_prefix, d.S, t0), last = find_system(d.tile_prefix, d.S, tend - 1);
+      if (first == last && !d.active[first]) continue;
+    }
 
     long long aix = 0, aiy = 0, aiz = 0;
     int cur_row = -1;
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
         }
         const SysDev& S = d.sys[s];
         const long long ti = S.tile_off + (t - d.tile_prefix[s]);
-        mask = row_bits<C>(d.masks, ti, l);
+        mask = !ENERGY || sys_active(d, s) ? row_bits<C>(d.masks, ti, l) : 0u;
         const int2 tile = d.tiles[ti];
         if (tile.x != cur_row) {
           flush_row();

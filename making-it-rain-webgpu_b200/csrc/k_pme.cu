@@ -214,8 +214,10 @@ __device__ __forceinline__ void spline_for(const SysDev& S, long long x, long lo
 }
 
 // ---------------------------------------------------------------- spread --
-// By atom, not by slot: the spread reads nothing the list kernels write, so it
-// runs on its own stream while they sort and rebuild.  A block takes up to
+// Both spreads read nothing the list kernels write, so they run on their own
+// stream while the list kernels sort and rebuild.
+//
+// By atom (engines up to a few waves of blocks): a block takes up to
 // kSplineAtoms atoms: their splines are computed once each into shared memory,
 // then all its threads share the 25 (ix, iy) rows of 5 z points per atom, so
 // no thread makes more than a few atomics in a row (one thread per atom making
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kThreads) k_spread(Dev d, int per) {
     if (threadIdx.x < per) {
       const int k = threadIdx.x, a = first + k * nblocks;
       float q = 0.f;
-      if (a < d.n_atoms) q = d.prm_atom[a].w;
+      if (a < d.n_atoms && sys_active(d, d.atom_sys[a])) q = d.prm_atom[a].w;
       t.q[k] = q;
       if (q != 0.f) {
         const int s = d.atom_sys[a];
@@ -280,11 +282,166 @@ __global__ void __launch_bounds__(kThreads) k_spread(Dev d, int per) {
   }
 }
 
+// By slot (larger engines): the slots of a snapshot of the list's sorted
+// order that the integrator writes at the end of every step (`spread_atom`),
+// so the order the list kernels are rewriting is never read.  A block takes
+// 128 consecutive slots -- four super-clusters along the space-filling curve,
+// a compact piece of space -- adds their charges into a patch of the mesh in
+// shared memory, and adds the patch's nonzero points to the grid: about a
+// fifth of the global atomics of spreading each atom's 125 points directly.
+// The patch holds the block's spline bases (unwrapped around its first atom)
+// plus the 5-point stencil; a block whose patch would not fit (a cluster torn
+// across a jump of the curve) or whose slots reach into the next system
+// spreads directly.  Every contribution is the same fixed-point value as in
+// the by-atom spread, so the grid is the same to the bit.  The shared-memory
+// phases make a block's chain longer: below a few waves of blocks (the 12k
+// and 27k single systems) the by-atom kernel finishes first, above it (a
+// 64-system ensemble of 627k atoms) this one takes 30% less time.
+constexpr int kPatchSlots = 128;
+constexpr int kPatchPoints = 4096;  // 32 KB of int64
+
+__global__ void __launch_bounds__(kThreads) k_spread_sorted(Dev d) {
+  __shared__ unsigned long long patch[kPatchPoints];
+  __shared__ int base[kPatchSlots][3];
+  __shared__ float th[kPatchSlots][3][5];
+  __shared__ float qs[kPatchSlots];
+  __shared__ int sysk[kPatchSlots];
+  __shared__ int lo_part[kPatchSlots / 32][3], hi_part[kPatchSlots / 32][3];
+  __shared__ int lo[3], ext[3], use_patch;
+  const int first = blockIdx.x * kPatchSlots;
+  if (first >= d.n_slots) return;
+  const int last = min(d.n_slots, first + kPatchSlots) - 1;
+  // a block may hold the end of one system and the start of the next: then
+  // every atom spreads directly into its own system's grid
+  const int s = d.slot_sys[first];
+  const bool one_system = d.slot_sys[last] == s;
+  const int a0 = d.spread_atom[first];
+  if (one_system && (a0 < 0 || !sys_active(d, s))) return;  // padding only, or a skipped system
+  const SysDev& S = d.sys[s];
+  const int K[3] = {S.grid[0], S.grid[1], S.grid[2]};
+  // splines; in a one-system block the bases unwrapped around the first slot's atom
+  const int t = threadIdx.x;
+  int ub[3] = {0, 0, 0};
+  bool live = false;
+  if (t < kPatchSlots) {
+    const int gs = first + t;
+    float q = 0.f;
+    int st = s;
+    if (gs <= last) {
+      st = d.slot_sys[gs];
+      const int a = d.spread_atom[gs];
+      if (a >= 0 && sys_active(d, st)) q = d.prm_atom[a].w;
+      if (q != 0.f) {
+        const SysDev& Sa = d.sys[st];
+        Spline sp;
+        spline_for(Sa, d.px[a], d.py[a], d.pz[a], sp, false);
+        Spline sp0;
+        if (one_system) spline_for(S, d.px[a0], d.py[a0], d.pz[a0], sp0, false);
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          int b = sp.base[ax];
+          if (one_system) {
+            const int r = sp0.base[ax];
+            if (b - r > K[ax] / 2) b -= K[ax];
+            if (r - b > K[ax] / 2) b += K[ax];
+          }
+          ub[ax] = b;
+          base[t][ax] = b;
+          for (int i = 0; i < kPmeOrder; ++i) th[t][ax][i] = sp.th[ax][i];
+        }
+        live = true;
+      }
+    }
+    qs[t] = q;
+    sysk[t] = st;
+  }
+  // the bases' range: warp reductions, then the block's
+  if (t < kPatchSlots) {
+    const int big = 1 << 30;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const int mn = __reduce_min_sync(0xffffffffu, live ? ub[ax] : big);
+      const int mx = __reduce_max_sync(0xffffffffu, live ? ub[ax] : -big);
+      if ((t & 31) == 0) {
+        lo_part[t >> 5][ax] = mn;
+        hi_part[t >> 5][ax] = mx;
+      }
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    int points = 1;
+    bool fits = one_system;
+    for (int ax = 0; ax < 3; ++ax) {
+      int mn = lo_part[0][ax], mx = hi_part[0][ax];
+      for (int w = 1; w < kPatchSlots / 32; ++w) {
+        mn = min(mn, lo_part[w][ax]);
+        mx = max(mx, hi_part[w][ax]);
+      }
+      lo[ax] = mn;
+      ext[ax] = mx - mn + kPmeOrder;
+      fits = fits && mx >= mn && ext[ax] <= K[ax];
+      points *= max(ext[ax], 1);
+    }
+    use_patch = fits && points <= kPatchPoints;
+  }
+  __syncthreads();
+  if (use_patch) {
+    const int ex = ext[0], ey = ext[1], ez = ext[2], np = ex * ey * ez;
+    for (int i = t; i < np; i += blockDim.x) patch[i] = 0ull;
+    __syncthreads();
+    for (int w = t; w < kPatchSlots * kPmeOrder * kPmeOrder; w += blockDim.x) {
+      const int k = w / (kPmeOrder * kPmeOrder), r = w - k * kPmeOrder * kPmeOrder;
+      const float q = qs[k];
+      if (q == 0.f) continue;
+      const int ix = r / kPmeOrder, iy = r - ix * kPmeOrder;
+      const float wxy = q * th[k][0][ix] * th[k][1][iy];
+      unsigned long long* row =
+          patch + ((base[k][0] - lo[0] + ix) * ey + (base[k][1] - lo[1] + iy)) * ez + (base[k][2] - lo[2]);
+#pragma unroll
+      for (int iz = 0; iz < kPmeOrder; ++iz) atomicAdd(&row[iz], static_cast<unsigned long long>(to_fixed(wxy * th[k][2][iz])));
+    }
+    __syncthreads();
+    for (int i = t; i < np; i += blockDim.x) {
+      const unsigned long long v = patch[i];
+      if (!v) continue;
+      const int px = i / (ey * ez), rem = i - px * ey * ez, py = rem / ez, pz = rem - py * ez;
+      int gx = (lo[0] + px) % K[0], gy = (lo[1] + py) % K[1], gz = (lo[2] + pz) % K[2];
+      if (gx < 0) gx += K[0];
+      if (gy < 0) gy += K[1];
+      if (gz < 0) gz += K[2];
+      atomicAdd(d.qgrid + S.grid_off + (static_cast<long long>(gx) * K[1] + gy) * K[2] + gz, v);
+    }
+  } else {
+    // the direct spread of each atom's 125 points, into its own system's grid
+    for (int w = t; w < kPatchSlots * kPmeOrder * kPmeOrder; w += blockDim.x) {
+      const int k = w / (kPmeOrder * kPmeOrder), r = w - k * kPmeOrder * kPmeOrder;
+      const float q = qs[k];
+      if (q == 0.f) continue;
+      const SysDev& Sk = d.sys[sysk[k]];
+      const int Kx = Sk.grid[0], Ky = Sk.grid[1], Kz = Sk.grid[2];
+      const int ix = r / kPmeOrder, iy = r - ix * kPmeOrder;
+      int gx = (base[k][0] + ix) % Kx, gy = (base[k][1] + iy) % Ky;
+      if (gx < 0) gx += Kx;
+      if (gy < 0) gy += Ky;
+      const float wxy = q * th[k][0][ix] * th[k][1][iy];
+      unsigned long long* row = d.qgrid + Sk.grid_off + (static_cast<long long>(gx) * Ky + gy) * Kz;
+#pragma unroll
+      for (int iz = 0; iz < kPmeOrder; ++iz) {
+        int gz = (base[k][2] + iz) % Kz;
+        if (gz < 0) gz += Kz;
+        add_fixed(&row[gz], wxy * th[k][2][iz]);
+      }
+    }
+  }
+}
+
 // --------------------------------------------------------------- z pass ---
 // int64 charge grid -> complex half spectrum along z, clearing the grid.
 __global__ void __launch_bounds__(kThreads) k_fft_z_forward(Dev d) {
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_z[blockIdx.x];
+  if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
   const SysDev& S = d.sys[w.sys];
   const int Kz = S.grid[2], kzh = S.kzh;
   float2* A = smem;
@@ -308,6 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_forward(Dev d) {
 __global__ void __launch_bounds__(kThreads) k_fft_y(Dev d, int sign) {
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_y[blockIdx.x];
+  if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
   const SysDev& S = d.sys[w.sys];
   const int Ky = S.grid[1], kzh = S.kzh;
   float2* A = smem;
@@ -331,6 +489,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   extern __shared__ float2 smem[];
   __shared__ double partial[7][kThreads / 32];
   const FftWork w = d.fft_x[blockIdx.x];
+  if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
   const SysDev& S = d.sys[w.sys];
   const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
   float2* A = smem;
@@ -433,6 +592,7 @@ constexpr int kPlaneThreads = 512;
 __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_p[blockIdx.x];
+  if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
   const SysDev& S = d.sys[w.sys];
   const int Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
   const unsigned ky_magic = magic_for(unsigned(Ky)), kzh_magic = magic_for(unsigned(kzh)),
@@ -477,6 +637,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
 __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_p[blockIdx.x];
+  if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
   const SysDev& S = d.sys[w.sys];
   const int Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
   const unsigned ky_magic = magic_for(unsigned(Ky)), kzh_magic = magic_for(unsigned(kzh)),
@@ -525,6 +686,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
 __global__ void __launch_bounds__(kThreads) k_fft_z_inverse(Dev d) {
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_z[blockIdx.x];
+  if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
   const SysDev& S = d.sys[w.sys];
   const int Kz = S.grid[2], kzh = S.kzh;
   float2* A = smem;
@@ -552,7 +714,7 @@ __global__ void __launch_bounds__(kThreads) k_gather(Dev d) {
     const int a = d.order[gs];
     if (a < 0) continue;
     const float q = d.prm[gs].w;
-    if (q == 0.f) continue;
+    if (q == 0.f || !sys_active(d, d.slot_sys[gs])) continue;
     const SysDev& S = d.sys[d.slot_sys[gs]];
     Spline sp;
     spline_for(S, d.px[a], d.py[a], d.pz[a], sp, true);
@@ -615,8 +777,15 @@ void set_pme_smem(int z, int y, int x, int plane) {
   cudaFuncSetAttribute(k_fft_x_convolve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
 }
 
+// Engines with at least four blocks of 128 slots per SM spread by slot.
+bool spread_by_slot(int n_slots) { return (n_slots + kPatchSlots - 1) / kPatchSlots >= 148 * 4; }
+
 void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
+  if (d.spread_sorted) {
+    k_spread_sorted<<<(d.n_slots + kPatchSlots - 1) / kPatchSlots, kThreads, 0, st>>>(d);
+    return;
+  }
   // about one block per two SMs, up to kSplineAtoms atoms each: small systems
   // get short blocks (latency), large ones full ones (fewer SMs taken from the
   // pair kernel running beside)

@@ -272,6 +272,8 @@ EXPORTS = {
     "mdb_mlp_predict": (C.c_int, [C.POINTER(C.c_float)] * 2 + [C.c_int32, C.POINTER(C.c_float)]),
     "mdb_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunOptions), C.c_int32, C.POINTER(Tuning),
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "mdb_autotune_batch": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(RunOptions), C.c_int32,
+                                     C.POINTER(Tuning), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mdb_reciprocal_noalloc": (
         C.c_int,
         [C.c_int32, C.c_void_p, C.c_void_p, _dp, C.c_double, _ip, C.c_void_p, C.c_void_p, C.c_void_p],

@@ -388,22 +388,34 @@ __all__ = ["StepLoop", "RunOptions", "Report", "EngineError", "CutoffTooLargeFor
 
 # ---- autotuner (no reference counterpart) -------------------------------------
 def autotune(system: System, state: State, options: RunOptions | None = None, steps: int = 200) -> dict:
-    """Time the library's candidate grid of (verlet_skin, sort_cell) for one
-    system on the device (`mdb_autotune`) and return the fastest."""
+    """Time the library's candidate grid of list settings for one system on
+    the device (`mdb_autotune`) and return the fastest."""
+    return autotune_batch([system], [state], options, steps)
+
+
+def autotune_batch(systems: Sequence[System], states: Sequence[State], options: RunOptions | None = None,
+                   steps: int = 200) -> dict:
+    """The same search with every candidate applied to all the systems of one
+    batched engine (`mdb_autotune_batch`): the fastest for the batch's step."""
     options = options or RunOptions()
     lib = abi.load()
-    sh, th = system.desc(), state.desc()
+    if len(systems) != len(states) or not systems:
+        raise ValueError("one state per system, and at least one system")
+    sys_handles = [s.desc() for s in systems]
+    st_handles = [s.desc() for s in states]
+    sys_array = (abi.SystemDesc * len(systems))(*[h.desc for h in sys_handles])
+    st_array = (abi.StateDesc * len(states))(*[h.desc for h in st_handles])
     opts = dataclasses.replace(options, tuning=None).to_c()
     best = abi.Tuning()
     ms = C.c_double()
     tried = C.c_int32()
-    status = lib.mdb_autotune(C.byref(sh.desc), C.byref(th.desc), C.byref(opts), int(steps), C.byref(best),
-                              C.byref(ms), C.byref(tried))
+    status = lib.mdb_autotune_batch(len(systems), sys_array, st_array, C.byref(opts), int(steps), C.byref(best),
+                                    C.byref(ms), C.byref(tried))
     if status != abi.OK:
         raise _ERRORS.get(status, EngineError)(status, lib.mdb_status_string(status).decode())
     return {"verlet_skin": best.verlet_skin, "sort_cell": best.sort_cell, "tile_atoms": best.tile_atoms,
             "prune_tiles": best.prune_tiles, "inner_skin": best.inner_skin, "ms_per_step": ms.value,
-            "candidates": tried.value}
+            "candidates": tried.value, "systems": len(systems)}
 
 
 def size_bucket(atoms: int) -> int:
@@ -412,11 +424,14 @@ def size_bucket(atoms: int) -> int:
 
 
 def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: RunOptions | None = None,
-                   steps: int = 200, cache: dict | None = None) -> tuple[list, dict]:
-    """One `autotune` per size bucket, on the bucket's median-sized system;
-    every system of the bucket takes its result.  Returns the per-system
-    (verlet_skin, sort_cell) list for `RunOptions.tuning` and the per-bucket
-    results.  `cache` (bucket -> result) skips buckets already tuned."""
+                   steps: int = 200, cache: dict | None = None, batched: bool = False) -> tuple[list, dict]:
+    """One search per size bucket; every system of the bucket takes its
+    result.  Without `batched`, `autotune` on the bucket's median-sized
+    system; with it, `autotune_batch` on the bucket's own systems together
+    (from the smallest up, at most 2^18 atoms in all), which is how a batched
+    engine runs them.  Returns the per-system tuning list for
+    `RunOptions.tuning` and the per-bucket results.  `cache` (bucket ->
+    result) skips buckets already tuned."""
     cache = {} if cache is None else cache
     buckets: dict[int, list[int]] = {}
     for k, s in enumerate(systems):
@@ -425,8 +440,17 @@ def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: 
         if b in cache:
             continue
         members = sorted(members, key=lambda k: systems[k].particle_count)
-        rep = members[len(members) // 2]
-        cache[b] = autotune(systems[rep], states[rep], options, steps)
+        if batched:
+            take, atoms = [], 0
+            for k in members:
+                if take and atoms + systems[k].particle_count > (1 << 18):
+                    break
+                take.append(k)
+                atoms += systems[k].particle_count
+            cache[b] = autotune_batch([systems[k] for k in take], [states[k] for k in take], options, steps)
+        else:
+            rep = members[len(members) // 2]
+            cache[b] = autotune(systems[rep], states[rep], options, steps)
     tuning = [tuple(cache[size_bucket(s.particle_count)][k]
                     for k in ("verlet_skin", "sort_cell", "tile_atoms", "prune_tiles", "inner_skin"))
               for s in systems]

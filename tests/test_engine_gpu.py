@@ -131,6 +131,31 @@ def test_batch_equals_single(mdb, water):
     batch.destroy()
 
 
+def test_slot_ordered_spread_equals_atom_ordered_spread(mdb):
+    """An engine of 80k atoms spreads PME charges by slot through shared-memory
+    mesh patches, a single 10k-atom system by atom straight into the grid: the
+    same fixed-point sums, so eight systems batched advance exactly as each
+    does alone -- through steps that rebuild the list, whose snapshot of the
+    slot order the spread reads."""
+    from mdb200 import synth
+
+    members = [synth.water_box(width=4.6, seed=20 + k) for k in range(8)]
+    assert sum(m[0].particle_count for m in members) >= 148 * 4 * 128  # the slot-ordered spread's threshold
+    single = []
+    for system, state in members:
+        loop = make_loop(mdb, system, state, seed=6)
+        loop.run(30)
+        single.append(loop.positions())
+        loop.destroy()
+    batch = mdb.StepLoop.batch([m[0] for m in members], [m[1] for m in members], mdb.RunOptions(seed=6))
+    batch.run(30)
+    rebuilds = [batch.verlet_flags(k)["rebuilds"] for k in range(len(members))]
+    print("rebuilds per system", rebuilds)
+    for k in range(len(members)):
+        assert np.array_equal(batch.positions(k), single[k]), k
+    batch.destroy()
+
+
 def test_potential_leaves_state_and_matches_evaluate(mdb, water):
     system, state = water
     loop = make_loop(mdb, system, state)
@@ -404,3 +429,4 @@ def test_cell_geometry_and_passes_per_step(mdb, water):
     assert 8 <= passes <= 30
     assert loop.profile_step(repeats=2)["launches_per_step"] == passes
     loop.destroy()
+
