@@ -437,6 +437,13 @@ def main() -> None:
                                            batched=True)
         return steploop.tune_by_bucket(systems, states, steploop.RunOptions(device=local), steps=400)
 
+    timed_events = {}
+
+    def list_events(loop) -> dict:
+        """Rebuilds and prunes so far, summed over the engine's systems."""
+        flags = [loop.verlet_flags(k) for k in range(loop.system_count)]
+        return {"rebuilds": sum(f["rebuilds"] for f in flags), "prunes": sum(f["prunes"] for f in flags)}
+
     def timed(loop, on_stride=None) -> tuple[float, dict]:
         """Warm-up, then exactly args.steps steps as timed strides; device seconds.
         `on_stride(loop)` runs after each stride, outside its timed interval."""
@@ -448,6 +455,7 @@ def main() -> None:
             loop.run(s)
         barrier()
         device_ms = 0.0
+        events0 = list_events(loop)
         t0 = time.perf_counter()
         for s in strides:
             flush_l2(flush)
@@ -457,6 +465,8 @@ def main() -> None:
                 on_stride(loop)
         barrier()
         t1 = time.perf_counter()
+        events1 = list_events(loop)
+        timed_events[id(loop)] = {k: events1[k] - events0[k] for k in events0}
         time.sleep(0.7)  # let the sampler record a line after the region
         clocks.__exit__(None, None, None)
         return max_over_ranks(device_ms / 1000.0), clocks.summary(t0, t1)
@@ -786,6 +796,9 @@ def main() -> None:
         result_loop = loop
 
     roof = roofline(result_loop)
+    if id(result_loop) in timed_events:
+        # list work inside the timed steps: system rebuilds and inner-list prunes
+        roof["list_events"] = dict(timed_events[id(result_loop)], steps=args.steps)
     result = {
         "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_s * 1000.0 / args.steps, "higher_is_better": True,

@@ -49,7 +49,6 @@ constexpr double kDefaultInnerSkin = -1.0;  // nm; <= 0: no inner list unless a 
 // twice that at a 0.2 nm skin (~90 for 32).  A list that needs more stops the
 // integrator and is grown and rebuilt by the host (grow_tile_list).
 int row_cap_for(int cluster) { return cluster == 8 ? 384 : 192; }
-constexpr int kFftTile = 8;  // kz columns per y- and x-pass CTA
 // the exact stage switches the screening network off once its running RMS
 // error exceeds this many kT (the plain barostat takes over)
 constexpr double kSurrogateMaxRmsKT = 1.5;
@@ -581,9 +580,9 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
         wx.push_back({s, y, k, std::min(kFftTile, S.kzh - k)});
         e->fft_x_sys.push_back(s);
       }
-    smem_x = std::max(smem_x, 2 * kFftTile * Kx * int(sizeof(float2)));
+    smem_x = std::max(smem_x, (2 * kFftTile + 1) * Kx * int(sizeof(float2)));  // two tiles of lines, twiddles
     for (int x = 0; x < Kx; ++x) wp.push_back({s, x, 0, 1});
-    smem_p = std::max(smem_p, 2 * Ky * Kz * int(sizeof(float2)));
+    smem_p = std::max(smem_p, (2 * Ky * Kz + Ky + Kz) * int(sizeof(float2)));  // two planes, twiddles
 
     // atoms
     const double* pos = states[s].positions;
@@ -867,6 +866,10 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   d.fft_y = w_dev; d.n_fft_y = int(wy.size());
   TRY(upload(e, "fft x work", w_dev, wx));
   d.fft_x = w_dev; d.n_fft_x = int(wx.size());
+  int max_kx = 1;
+  for (const SysDev& S : e->sd) max_kx = std::max(max_kx, S.grid[0]);
+  d.influence_stride = kFftTile * max_kx;
+  TRY(alloc(e, "pme influence function", d.influence, wx.size() * size_t(d.influence_stride)));
   TRY(upload(e, "fft plane work", w_dev, wp));
   d.fft_p = w_dev; d.n_fft_p = int(wp.size());
   // a whole x-plane in shared memory, twice, when every system's fits
@@ -941,6 +944,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   CUDA_TRY(e, cudaEventCreate(&e->t1));
   CUDA_TRY(e, cudaDeviceSynchronize());
 
+  launch_influence(e->d, -1, e->s0);
   // first list and the first COM velocity, by the phase kernels (a list that
   // overflows its starting capacity is grown and built again)
   if (const int st = request_rebuild(e, -1)) return st;
@@ -1174,6 +1178,8 @@ int set_box(mdb_engine* e, int s, const double* box) {
   fill_box(h, e->sd[s], true);
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys) + s, &e->sd[s], sizeof(SysDev), cudaMemcpyHostToDevice));
+  launch_influence(e->d, s, e->s0);
+  CUDA_TRY(e, cudaGetLastError());
   return request_rebuild(e, s);
 }
 
@@ -1212,6 +1218,7 @@ int move_boxes(mdb_engine* e, const std::vector<int>& sys, const std::vector<std
   CUDA_TRY(e, cudaStreamSynchronize(e->s0));
   CUDA_TRY(e, cudaMemcpy(const_cast<SysDev*>(e->d.sys), e->sd.data(), sizeof(SysDev) * e->d.S,
                          cudaMemcpyHostToDevice));
+  launch_influence(e->d, sys.size() == 1 ? sys[0] : -1, e->s0);
   for (int s : sys)
     if (std::find(rebuild.begin(), rebuild.end(), s) == rebuild.end())
       launch_after_box_change(e->d, s, e->sd[s].n_slots, e->sd[s].tile_cap, e->s0);

@@ -967,6 +967,8 @@ __global__ void __launch_bounds__(kThreads) k_wrap(Dev d) {
 // each reads them before taking its ticket.
 template <int C>
 __global__ void __launch_bounds__(kThreads) k_inner_prune(Dev d) {
+  wait_for_predecessor();
+  release_successor();
   if (!*d.any_rebuild && !*d.any_prune) return;
   phase_inner<C>(d);
   __shared__ int last;
@@ -1071,8 +1073,8 @@ void rebuild_tiles(const Dev& d, cudaStream_t st) {
 
 void launch_inner_prune(const Dev& d, cudaStream_t st) {
   if (!d.inner) return;
-  if (d.cluster == 8) k_inner_prune<8><<<148 * 4, kThreads, 0, st>>>(d);
-  else k_inner_prune<32><<<148 * 4, kThreads, 0, st>>>(d);
+  if (d.cluster == 8) launch_chained(k_inner_prune<8>, 148 * 4, kThreads, 0, st, d);
+  else launch_chained(k_inner_prune<32>, 148 * 4, kThreads, 0, st, d);
 }
 
 void launch_rebuild_tiles(const Dev& d, cudaStream_t st) {

@@ -519,6 +519,7 @@ __device__ void unit_positions(Stage& sh, const UnitDev& u, float tol, bool& bad
 __global__ void __launch_bounds__(kThreads) k_integrate(Dev d) {
   __shared__ Stage sh;
   __shared__ double red[3][kThreads / 32];
+  wait_for_predecessor();
   const int b = blockIdx.x;
   const int s = d.iblk_sys[b];
   const SysDev& S = d.sys[s];
@@ -712,7 +713,7 @@ __global__ void __launch_bounds__(kThreads) k_momentum(Dev d) {
 }  // namespace
 
 void launch_integrate(const Dev& d, cudaStream_t st) {
-  k_integrate<<<d.n_iblk, kThreads, 0, st>>>(d);
+  launch_chained(k_integrate, d.n_iblk, kThreads, 0, st, d);
 }
 
 void launch_momentum(const Dev& d, cudaStream_t st) {

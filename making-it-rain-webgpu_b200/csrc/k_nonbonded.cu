@@ -108,13 +108,27 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
 // all slots first and evaluating only the pairs inside, 32 at a time through
 // shared memory, gave the same bits but 5-15% more time (7% fewer
 // instructions, longer shared-memory dependency chains).
+// The system's constants arrive in registers (`SysConst`): read from global
+// memory in every tile, they cost the loop a load each.
+struct SysConst {
+  float alpha, a2sp, cut2, inv;
+  long long tile_base;  // the system's first tile in the list, minus its first tile index
+  int next;             // the next system's first tile index
+};
+
+__device__ __forceinline__ SysConst sys_const(const Dev& d, int s) {
+  const SysDev& S = d.sys[s];
+  const int first = d.tile_prefix[s];
+  return SysConst{S.alpha, S.alpha_2_sqrtpi, S.cut2, S.pc_inv, S.tile_off - static_cast<long long>(first),
+                  d.tile_prefix[s + 1]};
+}
+
 template <int C, bool ENERGY, bool TRICLINIC>
-__device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, int4 pj, float4 qj,
-                                           unsigned int mask, bool per_pair, int l, float& fix, float& fiy,
-                                           float& fiz,
-                                           float& fjx, float& fjy, float& fjz, float& ecoul, float& elj,
-                                           int& pairs, float* vir) {
-  const float alpha = S.alpha, a2sp = S.alpha_2_sqrtpi, cut2 = S.cut2, inv = S.pc_inv;
+__device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, int4 pi, float4 qi, int4 pj,
+                                           float4 qj, unsigned int mask, bool per_pair, int l, float& fix,
+                                           float& fiy, float& fiz, float& fjx, float& fjy, float& fjz, float& ecoul,
+                                           float& elj, int& pairs, float* vir) {
+  const float alpha = K.alpha, a2sp = K.a2sp, cut2 = K.cut2, inv = K.inv;
   const int src = (l + 1) & (C - 1);
   constexpr int kUnroll = C == 8 ? 8 : 4;
 #pragma unroll kUnroll
@@ -165,6 +179,7 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, int4 pi, float4 qi, 
 // typical list, so most warps take one chunk and then retire.
 template <int C, bool ENERGY, bool TRICLINIC>
 __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
+  wait_for_predecessor();  // no early release: later waves would share their SMs with the next kernel
   constexpr int G = 32 / C;
   const int lane = threadIdx.x & 31;
   const int g = lane / C, l = lane & (C - 1);
@@ -229,6 +244,9 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
       }
     };
 
+    SysConst K = sys_const(d, s);
+    int4 pi_row = make_int4(0, 0, 0, 0);
+    float4 qi_row = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int base = t0; base < tend; base += G) {
       const int t = base + g;
       const bool active = t < tend;  // the same for every lane of a group
@@ -238,22 +256,26 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
       int gj = -1;
       bool per_pair = false;
       if (active) {
-        while (t >= d.tile_prefix[s + 1]) {
-          flush_energy(s);
-          ++s;
+        if (t >= K.next) {
+          while (t >= d.tile_prefix[s + 1]) {
+            flush_energy(s);
+            ++s;
+          }
+          K = sys_const(d, s);
         }
-        const SysDev& S = d.sys[s];
-        const long long ti = S.tile_off + (t - d.tile_prefix[s]);
+        const long long ti = K.tile_base + t;
         mask = !ENERGY || sys_active(d, s) ? row_bits<C>(d.masks, ti, l) : 0u;
         const int2 tile = d.tiles[ti];
         if (tile.x != cur_row) {
           flush_row();
           cur_row = tile.x;
+          // the row's atom stays in registers across the row's tiles
+          pi_row = d.pc[tile.x * C + l];
+          qi_row = d.prm[tile.x * C + l];
         }
-        const int gi = tile.x * C + l;
         gj = tile.y * C + l;
-        pi = d.pc[gi];
-        qi = d.prm[gi];
+        pi = pi_row;
+        qi = qi_row;
         pj = d.pc[gj];
         qj = d.prm[gj];
         const int4 sh = d.tile_shift[ti];
@@ -268,8 +290,8 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
       float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       int np = 0;
       mask = C == 32 ? __funnelshift_r(mask, mask, l) : ((mask >> l) | (mask << ((C - l) & (C - 1)))) & 0xFFu;
-      tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy, fjz, ec,
-                                       el, np, vir);
+      tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], K, pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy,
+                                       fjz, ec, el, np, vir);
       if (!active) continue;
       aix += to_fixed(fix);
       aiy += to_fixed(fiy);
@@ -303,11 +325,11 @@ void launch_shape(const Dev& d, bool energy, bool triclinic, cudaStream_t st) {
                              (d.tile_cap_total + kTilesPerWarp * warps_per_block - 1) /
                                  (kTilesPerWarp * warps_per_block))));
   if (energy) {
-    if (triclinic) k_nonbonded<C, true, true><<<blocks, kThreads, 0, st>>>(d);
-    else k_nonbonded<C, true, false><<<blocks, kThreads, 0, st>>>(d);
+    if (triclinic) launch_chained(k_nonbonded<C, true, true>, blocks, kThreads, 0, st, d);
+    else launch_chained(k_nonbonded<C, true, false>, blocks, kThreads, 0, st, d);
   } else {
-    if (triclinic) k_nonbonded<C, false, true><<<blocks, kThreads, 0, st>>>(d);
-    else k_nonbonded<C, false, false><<<blocks, kThreads, 0, st>>>(d);
+    if (triclinic) launch_chained(k_nonbonded<C, false, true>, blocks, kThreads, 0, st, d);
+    else launch_chained(k_nonbonded<C, false, false>, blocks, kThreads, 0, st, d);
   }
 }
 

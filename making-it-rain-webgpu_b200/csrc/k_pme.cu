@@ -129,6 +129,12 @@ __device__ __forceinline__ void stage_butterfly(const float2* src, float2* dst, 
   for (int q = 0; q < R; ++q) dst[dest + q * ns] = v[q];
 }
 
+// A transform's twiddle table (n entries) into shared memory, where the
+// butterflies read it: a global read in every butterfly stage otherwise.
+__device__ __forceinline__ void stage_twiddles(float2* dst, const float2* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(&src[i]);
+}
+
 // Stockham autosort over `nl` lines of length n in shared memory
 // (src/reference/fft.ts:128 is the f64 restatement of the same recursion).
 // Returns the buffer holding the result.
@@ -237,6 +243,7 @@ struct SplineTable {
 };
 
 __global__ void __launch_bounds__(kThreads) k_spread(Dev d, int per) {
+  wait_for_predecessor();
   __shared__ SplineTable t;
   const int nblocks = gridDim.x;
   for (int first = blockIdx.x; first < d.n_atoms; first += nblocks * per) {
@@ -301,7 +308,12 @@ constexpr int kPatchSlots = 128;
 constexpr int kPatchPoints = 4096;  // 32 KB of int64
 
 __global__ void __launch_bounds__(kThreads) k_spread_sorted(Dev d) {
-  __shared__ unsigned long long patch[kPatchPoints];
+  wait_for_predecessor();
+  // the patch's fixed-point sums in two 32-bit halves (hi = v >> 20 signed,
+  // lo = the low 20 bits), so the adds are 32-bit shared atomics: at most 128
+  // atoms add to a point, which keeps both halves far from overflow
+  __shared__ int patch_hi[kPatchPoints];
+  __shared__ unsigned int patch_lo[kPatchPoints];
   __shared__ int base[kPatchSlots][3];
   __shared__ float th[kPatchSlots][3][5];
   __shared__ float qs[kPatchSlots];
@@ -388,7 +400,10 @@ __global__ void __launch_bounds__(kThreads) k_spread_sorted(Dev d) {
   __syncthreads();
   if (use_patch) {
     const int ex = ext[0], ey = ext[1], ez = ext[2], np = ex * ey * ez;
-    for (int i = t; i < np; i += blockDim.x) patch[i] = 0ull;
+    for (int i = t; i < np; i += blockDim.x) {
+      patch_hi[i] = 0;
+      patch_lo[i] = 0u;
+    }
     __syncthreads();
     for (int w = t; w < kPatchSlots * kPmeOrder * kPmeOrder; w += blockDim.x) {
       const int k = w / (kPmeOrder * kPmeOrder), r = w - k * kPmeOrder * kPmeOrder;
@@ -396,14 +411,18 @@ __global__ void __launch_bounds__(kThreads) k_spread_sorted(Dev d) {
       if (q == 0.f) continue;
       const int ix = r / kPmeOrder, iy = r - ix * kPmeOrder;
       const float wxy = q * th[k][0][ix] * th[k][1][iy];
-      unsigned long long* row =
-          patch + ((base[k][0] - lo[0] + ix) * ey + (base[k][1] - lo[1] + iy)) * ez + (base[k][2] - lo[2]);
+      const int row = ((base[k][0] - lo[0] + ix) * ey + (base[k][1] - lo[1] + iy)) * ez + (base[k][2] - lo[2]);
 #pragma unroll
-      for (int iz = 0; iz < kPmeOrder; ++iz) atomicAdd(&row[iz], static_cast<unsigned long long>(to_fixed(wxy * th[k][2][iz])));
+      for (int iz = 0; iz < kPmeOrder; ++iz) {
+        const long long v = to_fixed(wxy * th[k][2][iz]);
+        atomicAdd(&patch_hi[row + iz], static_cast<int>(v >> 20));
+        atomicAdd(&patch_lo[row + iz], static_cast<unsigned int>(v & 0xFFFFF));
+      }
     }
     __syncthreads();
     for (int i = t; i < np; i += blockDim.x) {
-      const unsigned long long v = patch[i];
+      const unsigned long long v = static_cast<unsigned long long>(
+          (static_cast<long long>(patch_hi[i]) << 20) + static_cast<long long>(patch_lo[i]));
       if (!v) continue;
       const int px = i / (ey * ez), rem = i - px * ey * ez, py = rem / ez, pz = rem - py * ez;
       int gx = (lo[0] + px) % K[0], gy = (lo[1] + py) % K[1], gz = (lo[2] + pz) % K[2];
@@ -439,6 +458,7 @@ __global__ void __launch_bounds__(kThreads) k_spread_sorted(Dev d) {
 // --------------------------------------------------------------- z pass ---
 // int64 charge grid -> complex half spectrum along z, clearing the grid.
 __global__ void __launch_bounds__(kThreads) k_fft_z_forward(Dev d) {
+  wait_for_predecessor();
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_z[blockIdx.x];
   if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
@@ -463,6 +483,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_forward(Dev d) {
 
 // --------------------------------------------------------------- y pass ---
 __global__ void __launch_bounds__(kThreads) k_fft_y(Dev d, int sign) {
+  wait_for_predecessor();
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_y[blockIdx.x];
   if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
@@ -484,8 +505,50 @@ __global__ void __launch_bounds__(kThreads) k_fft_y(Dev d, int sign) {
 }
 
 // ------------------------------------------- x pass with the convolution ---
+// The Ewald influence function (pme-convolve.wgsl:34; pme.ts:160-209) at
+// mesh index (mx, my, kz) of the half spectrum, mb the signed y index; the
+// wave vector and its square come back for the virial.  0 at the origin.
+// Written with explicit roundings so the table and the energy variant agree
+// to the bit.
+__device__ __forceinline__ float influence(const SysDev& S, const float* modx, const float* mody, const float* modz,
+                                           int Kx, int mx, int mb, int my, int kz, float& kx, float& ky, float& kzv,
+                                           float& k2) {
+  if (mx == 0 && my == 0 && kz == 0) return 0.f;
+  const float two_pi = 6.283185307179586f;
+  const float* M = S.inv_f;
+  const float ma = static_cast<float>(mx <= Kx / 2 ? mx : mx - Kx), fb = static_cast<float>(mb),
+              mc = static_cast<float>(kz);  // kz <= Kz/2 on the half spectrum
+  kx = __fmul_rn(two_pi, __fmul_rn(ma, M[0]));
+  ky = __fmul_rn(two_pi, fmaf(fb, M[4], __fmul_rn(ma, M[3])));
+  kzv = __fmul_rn(two_pi, fmaf(mc, M[8], fmaf(fb, M[7], __fmul_rn(ma, M[6]))));
+  k2 = fmaf(kzv, kzv, fmaf(ky, ky, __fmul_rn(kx, kx)));
+  const float den = __fmul_rn(__fmul_rn(__fmul_rn(k2, modx[mx]), mody[my]), modz[kz]);
+  return __fdiv_rn(__fmul_rn(S.pme_pref, expf(__fmul_rn(k2, S.exp_scale))), den);
+}
+
+// The influence function of every x-pass work item of system `s` (all
+// systems: s < 0), in the order the x pass visits its elements.  Run after
+// every change of a box.
+__global__ void __launch_bounds__(kThreads) k_influence(Dev d, int s) {
+  const FftWork w = d.fft_x[blockIdx.x];
+  if (s >= 0 && w.sys != s) return;
+  const SysDev& S = d.sys[w.sys];
+  const int Kx = S.grid[0], Ky = S.grid[1];
+  const float* modx = d.moduli + S.mod_off;
+  const float* mody = modx + Kx;
+  const float* modz = mody + Ky;
+  const int my = w.a, mb = my <= Ky / 2 ? my : my - Ky;
+  float* table = d.influence + static_cast<long long>(blockIdx.x) * d.influence_stride;
+  for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
+    const int l = i / Kx, mx = i - l * Kx;
+    float kx, ky, kzv, k2;
+    table[i] = influence(S, modx, mody, modz, Kx, mx, mb, my, w.b + l, kx, ky, kzv, k2);
+  }
+}
+
 template <bool ENERGY>
 __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
+  wait_for_predecessor();
   extern __shared__ float2 smem[];
   __shared__ double partial[7][kThreads / 32];
   const FftWork w = d.fft_x[blockIdx.x];
@@ -494,6 +557,8 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   const int Kx = S.grid[0], Ky = S.grid[1], Kz = S.grid[2], kzh = S.kzh;
   float2* A = smem;
   float2* B = smem + w.n * Kx;
+  float2* twx = smem + 2 * kFftTile * Kx;  // the twiddles, after the two tiles of lines
+  stage_twiddles(twx, d.twiddles + S.tw_off[0], Kx);
   const long long stride = static_cast<long long>(Ky) * kzh;
   float2* base = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * kzh + w.b;
   const unsigned n_magic = magic_for(unsigned(w.n)), kx_magic = magic_for(unsigned(Kx));
@@ -512,7 +577,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
       if (i0 + u * int(blockDim.x) < w.n * Kx) A[l[u] * Kx + x[u]] = v[u];
   }
   __syncthreads();
-  float2* R = fft_lines(A, B, Kx, w.n, S.radices[0], S.nradix[0], d.twiddles + S.tw_off[0], -1);
+  float2* R = fft_lines(A, B, Kx, w.n, S.radices[0], S.nradix[0], twx, -1);
   float2* other = R == A ? B : A;
   // Convolution (pme-convolve.wgsl:34; pme.ts:160-209) on the half spectrum.
   double energy = 0.0;
@@ -522,22 +587,17 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
   const float* modx = d.moduli + S.mod_off;
   const float* mody = modx + Kx;
   const float* modz = mody + Ky;
-  const float two_pi = 6.283185307179586f;
+  // the force variant (every MD step) reads the influence function from the
+  // table k_influence fills at every box change; the energy variant needs the
+  // wave vectors for the virial and evaluates it here, the same function
+  const float* table = d.influence + static_cast<long long>(blockIdx.x) * d.influence_stride;
   for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
     const int l = int(quotient(unsigned(i), kx_magic)), mx = i - l * Kx;
     const int kz = w.b + l;
-    const int ma = mx <= Kx / 2 ? mx : mx - Kx;
-    const int mc = kz;  // kz <= Kz/2 on the half spectrum
     float2 v = R[i];
-    float factor = 0.f, kx = 0.f, ky = 0.f, kzv = 0.f, k2 = 1.f;
-    if (mx != 0 || my != 0 || kz != 0) {
-      const float* M = S.inv_f;
-      kx = two_pi * ma * M[0];
-      ky = two_pi * (ma * M[3] + mb * M[4]);
-      kzv = two_pi * (ma * M[6] + mb * M[7] + mc * M[8]);
-      k2 = kx * kx + ky * ky + kzv * kzv;
-      factor = S.pme_pref * expf(k2 * S.exp_scale) / (k2 * modx[mx] * mody[my] * modz[kz]);
-    }
+    float factor, kx = 0.f, ky = 0.f, kzv = 0.f, k2 = 1.f;
+    if (ENERGY) factor = influence(S, modx, mody, modz, Kx, mx, mb, my, kz, kx, ky, kzv, k2);
+    else factor = __ldg(&table[i]);
     if (ENERGY) {
       const double weight = (kz == 0 || (2 * kz == Kz)) ? 1.0 : 2.0;
       const double ek =
@@ -558,7 +618,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
     R[i] = v;
   }
   __syncthreads();
-  const float2* Q = fft_lines(R, other, Kx, w.n, S.radices[0], S.nradix[0], d.twiddles + S.tw_off[0], +1);
+  const float2* Q = fft_lines(R, other, Kx, w.n, S.radices[0], S.nradix[0], twx, +1);
   for (int i = threadIdx.x; i < w.n * Kx; i += blockDim.x) {
     const int x = int(quotient(unsigned(i), n_magic)), l = i - x * w.n;
     base[x * stride + l] = Q[l * Kx + x];
@@ -590,6 +650,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_convolve(Dev d) {
 constexpr int kPlaneThreads = 512;
 
 __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
+  wait_for_predecessor();
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_p[blockIdx.x];
   if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
@@ -599,6 +660,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
                  rest_magic = magic_for(unsigned(Kz - kzh));
   float2* A = smem;
   float2* B = smem + Ky * Kz;
+  float2* twz = smem + 2 * Ky * Kz;  // the twiddles, after the two planes
+  float2* twy = twz + Kz;
+  stage_twiddles(twz, d.twiddles + S.tw_off[2], Kz);
+  stage_twiddles(twy, d.twiddles + S.tw_off[1], Ky);
   unsigned long long* grid = d.qgrid + S.grid_off + static_cast<long long>(w.a) * Ky * Kz;
   // four loads in flight per thread before any is used
   for (int i0 = threadIdx.x; i0 < Ky * Kz; i0 += 4 * blockDim.x) {
@@ -618,7 +683,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
     }
   }
   __syncthreads();
-  float2* R = fft_lines(A, B, Kz, Ky, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], -1);
+  float2* R = fft_lines(A, B, Kz, Ky, S.radices[2], S.nradix[2], twz, -1);
   float2* T = R == A ? B : A;
   // the half spectrum's kz columns become y-lines
   for (int i = threadIdx.x; i < kzh * Ky; i += blockDim.x) {
@@ -626,7 +691,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
     T[k * Ky + y] = R[y * Kz + k];
   }
   __syncthreads();
-  const float2* Y = fft_lines(T, R, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], -1);
+  const float2* Y = fft_lines(T, R, Ky, kzh, S.radices[1], S.nradix[1], twy, -1);
   float2* out = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
   for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
     const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
@@ -635,6 +700,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_zy_forward(Dev d) {
 }
 
 __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
+  wait_for_predecessor();
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_p[blockIdx.x];
   if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
@@ -644,6 +710,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
                  rest_magic = magic_for(unsigned(Kz - kzh));
   float2* A = smem;
   float2* B = smem + Ky * Kz;
+  float2* twz = smem + 2 * Ky * Kz;  // the twiddles, after the two planes
+  float2* twy = twz + Kz;
+  stage_twiddles(twz, d.twiddles + S.tw_off[2], Kz);
+  stage_twiddles(twy, d.twiddles + S.tw_off[1], Ky);
   const float2* in = d.cgrid + S.cgrid_off + static_cast<long long>(w.a) * Ky * kzh;
   for (int i0 = threadIdx.x; i0 < Ky * kzh; i0 += 4 * blockDim.x) {
     float2 v[4];
@@ -662,7 +732,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
     }
   }
   __syncthreads();
-  float2* Y = fft_lines(A, B, Ky, kzh, S.radices[1], S.nradix[1], d.twiddles + S.tw_off[1], +1);
+  float2* Y = fft_lines(A, B, Ky, kzh, S.radices[1], S.nradix[1], twy, +1);
   float2* Z = Y == A ? B : A;
   for (int i = threadIdx.x; i < Ky * kzh; i += blockDim.x) {
     const int y = int(quotient(unsigned(i), kzh_magic)), k = i - y * kzh;
@@ -676,7 +746,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
     Z[y * Kz + k] = make_float2(c.x, -c.y);
   }
   __syncthreads();
-  const float2* R = fft_lines(Z, Y, Kz, Ky, S.radices[2], S.nradix[2], d.twiddles + S.tw_off[2], +1);
+  const float2* R = fft_lines(Z, Y, Kz, Ky, S.radices[2], S.nradix[2], twz, +1);
   float* out = d.phi + S.grid_off + static_cast<long long>(w.a) * Ky * Kz;
   for (int i = threadIdx.x; i < Ky * Kz; i += blockDim.x) out[i] = R[i].x;
 }
@@ -684,6 +754,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yz_inverse(Dev d) {
 // ---------------------------------------------------------- z inverse ----
 // complex half spectrum -> real potential grid along z.
 __global__ void __launch_bounds__(kThreads) k_fft_z_inverse(Dev d) {
+  wait_for_predecessor();
   extern __shared__ float2 smem[];
   const FftWork w = d.fft_z[blockIdx.x];
   if (!sys_active(d, w.sys)) return;  // the whole block: before any barrier
@@ -710,6 +781,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_inverse(Dev d) {
 
 // ---------------------------------------------------------------- gather --
 __global__ void __launch_bounds__(kThreads) k_gather(Dev d) {
+  wait_for_predecessor();
   for (int gs = blockIdx.x * blockDim.x + threadIdx.x; gs < d.n_slots; gs += gridDim.x * blockDim.x) {
     const int a = d.order[gs];
     if (a < 0) continue;
@@ -783,36 +855,41 @@ bool spread_by_slot(int n_slots) { return (n_slots + kPatchSlots - 1) / kPatchSl
 void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
   if (d.spread_sorted) {
-    k_spread_sorted<<<(d.n_slots + kPatchSlots - 1) / kPatchSlots, kThreads, 0, st>>>(d);
+    launch_chained(k_spread_sorted, (d.n_slots + kPatchSlots - 1) / kPatchSlots, kThreads, 0, st, d);
     return;
   }
   // about one block per two SMs, up to kSplineAtoms atoms each: small systems
   // get short blocks (latency), large ones full ones (fewer SMs taken from the
   // pair kernel running beside)
   const int per = std::max(16, std::min(kSplineAtoms, (d.n_atoms + 73) / 74));
-  k_spread<<<std::max(1, std::min((d.n_atoms + per - 1) / per, 148 * 8)), kThreads, 0, st>>>(d, per);
+  launch_chained(k_spread, std::max(1, std::min((d.n_atoms + per - 1) / per, 148 * 8)), kThreads, 0, st, d, per);
 }
 
 void launch_pme_fft(const Dev& d, bool energy, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
-  if (d.fft_planes) k_fft_zy_forward<<<d.n_fft_p, kPlaneThreads, g_smem.p, st>>>(d);
+  if (d.fft_planes) launch_chained(k_fft_zy_forward, d.n_fft_p, kPlaneThreads, g_smem.p, st, d);
   else {
-    k_fft_z_forward<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
-    k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, -1);
+    launch_chained(k_fft_z_forward, d.n_fft_z, kThreads, g_smem.z, st, d);
+    launch_chained(k_fft_y, d.n_fft_y, kThreads, g_smem.y, st, d, -1);
   }
-  if (energy) k_fft_x_convolve<true><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
-  else k_fft_x_convolve<false><<<d.n_fft_x, kThreads, g_smem.x, st>>>(d);
-  if (d.fft_planes) k_fft_yz_inverse<<<d.n_fft_p, kPlaneThreads, g_smem.p, st>>>(d);
+  if (energy) launch_chained(k_fft_x_convolve<true>, d.n_fft_x, kThreads, g_smem.x, st, d);
+  else launch_chained(k_fft_x_convolve<false>, d.n_fft_x, kThreads, g_smem.x, st, d);
+  if (d.fft_planes) launch_chained(k_fft_yz_inverse, d.n_fft_p, kPlaneThreads, g_smem.p, st, d);
   else {
-    k_fft_y<<<d.n_fft_y, kThreads, g_smem.y, st>>>(d, +1);
-    k_fft_z_inverse<<<d.n_fft_z, kThreads, g_smem.z, st>>>(d);
+    launch_chained(k_fft_y, d.n_fft_y, kThreads, g_smem.y, st, d, +1);
+    launch_chained(k_fft_z_inverse, d.n_fft_z, kThreads, g_smem.z, st, d);
   }
+}
+
+void launch_influence(const Dev& d, int s, cudaStream_t st) {
+  if (d.n_fft_x == 0) return;
+  k_influence<<<d.n_fft_x, kThreads, 0, st>>>(d, s);
 }
 
 void launch_pme_gather(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
   // a thread per slot; blocks of 64 so that even 10k atoms spread over every SM
-  k_gather<<<std::max(1, std::min((d.n_slots + 63) / 64, 148 * 16)), 64, 0, st>>>(d);
+  launch_chained(k_gather, std::max(1, std::min((d.n_slots + 63) / 64, 148 * 16)), 64, 0, st, d);
 }
 
 void launch_pme(const Dev& d, bool energy, cudaStream_t st) {
@@ -1002,18 +1079,9 @@ __global__ void k_na_x_convolve(SysDev S, NaPtrs p) {
   for (int i = threadIdx.x; i < nk * Kx; i += blockDim.x) {
     const int l = i / Kx, mx = i - l * Kx;
     const int kz = kz0 + l;
-    const int ma = mx <= Kx / 2 ? mx : mx - Kx;
     float2 v = R[i];
-    float factor = 0.f;
-    if (mx != 0 || my != 0 || kz != 0) {
-      const float* M = S.inv_f;
-      const float two_pi = 6.283185307179586f;
-      const float kx = two_pi * ma * M[0];
-      const float ky = two_pi * (ma * M[3] + mb * M[4]);
-      const float kzv = two_pi * (ma * M[6] + mb * M[7] + kz * M[8]);
-      const float k2 = kx * kx + ky * ky + kzv * kzv;
-      factor = S.pme_pref * expf(k2 * S.exp_scale) / (k2 * modx[mx] * mody[my] * modz[kz]);
-    }
+    float kx, ky, kzv, k2;
+    const float factor = influence(S, modx, mody, modz, Kx, mx, mb, my, kz, kx, ky, kzv, k2);
     const double weight = (kz == 0 || (2 * kz == Kz)) ? 1.0 : 2.0;
     energy += weight * double(factor) * (double(v.x) * v.x + double(v.y) * v.y);
     v.x *= 2.f * factor;

@@ -169,6 +169,11 @@ class StepLoop:
             raise _ERRORS.get(status, EngineError)(status, message)
         return cls(handle, lib, list(systems), list(states), options)
 
+    @property
+    def system_count(self) -> int:
+        """Systems in the engine."""
+        return len(self._systems)
+
     # ---- internals -------------------------------------------------------
     def _check(self, status: int) -> None:
         if status != abi.OK:

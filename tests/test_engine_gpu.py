@@ -156,6 +156,29 @@ def test_slot_ordered_spread_equals_atom_ordered_spread(mdb):
     batch.destroy()
 
 
+def test_set_box_equals_an_engine_created_at_that_box(mdb):
+    """A box set on an engine -- its PME influence table, which the force
+    steps read, is refilled; the list is rebuilt -- gives the trajectory of an
+    engine created at that box and those positions, to the bit."""
+    from mdb200 import synth
+    from mdb200.system import State
+
+    system, state = synth.water_box(n_waters=900, width=3.1, seed=8, grid=(32, 32, 32))
+    scale = 1.004
+    box2 = np.asarray(state.box, dtype=np.float64) * scale
+    pos2 = np.asarray(state.positions, dtype=np.float64) * scale
+    moved = make_loop(mdb, system, state, seed=9)
+    moved.set_box(box2)
+    moved.set_positions(pos2)
+    moved.run(20)
+    fresh = make_loop(mdb, system, State(positions=pos2, box=box2, velocities=state.velocities, step=state.step),
+                      seed=9)
+    fresh.run(20)
+    assert np.array_equal(moved.positions(), fresh.positions())
+    moved.destroy()
+    fresh.destroy()
+
+
 def test_potential_leaves_state_and_matches_evaluate(mdb, water):
     system, state = water
     loop = make_loop(mdb, system, state)
@@ -310,6 +333,25 @@ def test_autotune_picks_a_candidate_and_tuned_batch_equals_tuned_single(mdb):
     assert np.array_equal(batch.positions(0), single[0])
     assert np.array_equal(batch.positions(1), single[1])
     batch.destroy()
+
+
+def test_batched_autotune_searches_the_bucket_together(mdb):
+    """`autotune_batch` times every candidate on one batched engine of all the
+    systems given; `tune_by_bucket(batched=True)` runs it per size bucket on
+    the bucket's own systems and hands each system its bucket's choice."""
+    from mdb200 import synth
+
+    members = [synth.water_box(n_waters=n, width=w, seed=k, grid=(30, 30, 30))
+               for k, (n, w) in enumerate([(700, 2.8), (760, 2.9), (1500, 3.6)])]
+    best = mdb.autotune_batch([m[0] for m in members[:2]], [m[1] for m in members[:2]], steps=30)
+    print("autotune_batch", best)
+    assert best["candidates"] == 32 and best["systems"] == 2
+    assert best["verlet_skin"] in (0.15, 0.20, 0.30, 0.40, 0.50) and best["tile_atoms"] in (8, 32)
+    assert best["ms_per_step"] > 0
+    tuning, buckets = mdb.tune_by_bucket([m[0] for m in members], [m[1] for m in members], steps=30, batched=True)
+    assert len(tuning) == 3 and len(buckets) == 2  # 2,100 and 2,280 atoms share a bucket; 4,500 is the next
+    assert tuning[0] == tuning[1]
+    assert buckets[mdb.size_bucket(members[0][0].particle_count)]["systems"] == 2
 
 
 @pytest.mark.parametrize("shape,prune", [(8, 1), (8, 2), (32, 1), (32, 2)])
