@@ -691,6 +691,7 @@ def main() -> None:
             "autotuner": {str(b): {k: round(v, 4) if isinstance(v, float) else v for k, v in r.items()}
                           for b, r in buckets.items()},
             "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
+                          "fit_ms": round(after["trainingMs"], 1),
                           "active": after["surrogateActive"], "disabled": after["surrogateDisabled"],
                           "rms_kj_mol": after["surrogateRms"], "attempts_timed": attempts,
                           "exact_per_attempt": (after["exactEvaluations"] - before["exactEvaluations"])
@@ -747,6 +748,7 @@ def main() -> None:
             "steps_per_s": steps_per_s,
             "autotuner": {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()},
             "surrogate": {"training_attempts": after["trainingSamples"], "training_seconds": round(t_train, 1),
+                          "fit_ms": round(after["trainingMs"], 1),
                           "active": after["surrogateActive"], "rms_kj_mol": after["surrogateRms"],
                           "attempts_timed": attempts,
                           "exact_per_attempt": (after["exactEvaluations"] - before["exactEvaluations"])

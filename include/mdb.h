@@ -244,6 +244,7 @@ typedef struct mdb_barostat_stats {
   int32_t surrogate_disabled;/* 1 when the exact stage found the network too inaccurate */
   double surrogate_rms;      /* running RMS of (predicted - exact) potential change, kJ/mol */
   double training_loss;      /* final mean squared training loss (standardised units) */
+  double training_ms;        /* device time of the network's fits so far */
 } mdb_barostat_stats;
 
 /*

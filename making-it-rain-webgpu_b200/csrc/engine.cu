@@ -79,6 +79,7 @@ struct Surrogate {
   float* xi = nullptr;            // device: inference inputs, two rows per system
   float* yi = nullptr;            // device: inference outputs
   double final_loss = 0;
+  double fit_ms = 0;              // device time of the fits so far (one CTA: the epochs run in sequence)
 };
 
 struct BarostatState {
@@ -1341,7 +1342,19 @@ int surrogate_train(mdb_engine* e, Surrogate& net, uint32_t seed, int epochs) {
   net.dev.beta2 = 0.999f;
   net.dev.eps = 1e-8f;
   std::vector<double> losses;
-  CUDA_TRY(e, mlp_train(net.dev, net.x, net.t, n, epochs, seed, net.loss, &losses, e->s0));
+  // its own events: a timed run (mdb_run_timed) may be holding the engine's
+  cudaEvent_t fit0 = nullptr, fit1 = nullptr;
+  CUDA_TRY(e, cudaEventCreate(&fit0));
+  CUDA_TRY(e, cudaEventCreate(&fit1));
+  cudaEventRecord(fit0, e->s0);
+  const cudaError_t fit = mlp_train(net.dev, net.x, net.t, n, epochs, seed, net.loss, &losses, e->s0);
+  cudaEventRecord(fit1, e->s0);
+  float fit_ms = 0;
+  if (fit == cudaSuccess && cudaEventSynchronize(fit1) == cudaSuccess) cudaEventElapsedTime(&fit_ms, fit0, fit1);
+  cudaEventDestroy(fit0);
+  cudaEventDestroy(fit1);
+  CUDA_TRY(e, fit);
+  net.fit_ms += fit_ms;
   net.final_loss = losses.empty() ? 0.0 : losses.back();
   net.active = true;
   return MDB_OK;
@@ -1864,6 +1877,7 @@ int mdb_get_barostat_stats(const mdb_engine* e, int32_t s, mdb_barostat_stats* o
   out->training_samples = int64_t(net.delta_u.size());
   out->surrogate_rms = std::sqrt(net.err2);
   out->training_loss = net.final_loss;
+  out->training_ms = net.fit_ms;
   return MDB_OK;
 }
 

@@ -185,6 +185,7 @@ class BarostatStats(C.Structure):
         ("surrogate_disabled", C.c_int32),
         ("surrogate_rms", C.c_double),
         ("training_loss", C.c_double),
+        ("training_ms", C.c_double),
     ]
 
 

@@ -326,7 +326,7 @@ class StepLoop:
                 "screened": s.screened, "exactEvaluations": s.exact_evaluations,
                 "trainingSamples": s.training_samples, "surrogateActive": bool(s.surrogate_active),
                 "surrogateDisabled": bool(s.surrogate_disabled), "surrogateRms": s.surrogate_rms,
-                "trainingLoss": s.training_loss}
+                "trainingLoss": s.training_loss, "trainingMs": s.training_ms}
 
     def verlet_flags(self, system: int = 0) -> dict:
         """`StepLoop.verletFlags`, loop.ts:941."""
