@@ -720,30 +720,37 @@ __device__ bool tile_within_reach<8>(const Dev& d, const SysDev& S, long long ti
     if (gx * gx + gy * gy + gz * gz >= reach2 * (1.0f + 4e-5f)) return false;
   }
   const unsigned int w0 = __ldcg(&d.masks[ti * 2]), w1 = __ldcg(&d.masks[ti * 2 + 1]);
-  const int4 r0 = d.pc[tile.x * 8];
+  // both clusters' sixteen atoms in one round of loads, then the 64 tests
+  // (loading each i atom inside the loop made a chain of eight round trips)
+  int4 qi[8], qj[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    qi[k] = d.pc[tile.x * 8 + k];
+    qj[k] = d.pc[tile.y * 8 + k];
+  }
+  const int4 r0 = qi[0];
   const unsigned ox = unsigned(r0.x) - unsigned(sh.x), oy = unsigned(r0.y) - unsigned(sh.y),
                  oz = unsigned(r0.z) - unsigned(sh.z);
   float jx[8], jy[8], jz[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    const int4 q = d.pc[tile.y * 8 + j];
-    jx[j] = int(unsigned(q.x) - ox) * inv;
-    jy[j] = int(unsigned(q.y) - oy) * inv;
-    jz[j] = int(unsigned(q.z) - oz) * inv;
+    jx[j] = int(unsigned(qj[j].x) - ox) * inv;
+    jy[j] = int(unsigned(qj[j].y) - oy) * inv;
+    jz[j] = int(unsigned(qj[j].z) - oz) * inv;
   }
+#pragma unroll
   for (int i = 0; i < 8; ++i) {
     const unsigned int row = ((i < 4 ? w0 : w1) >> ((i & 3) * 8)) & 0xFFu;
-    if (!row) continue;
-    const int4 q = d.pc[tile.x * 8 + i];
-    const float ix = int(unsigned(q.x) - unsigned(r0.x)) * inv, iy = int(unsigned(q.y) - unsigned(r0.y)) * inv,
-                iz = int(unsigned(q.z) - unsigned(r0.z)) * inv;
+    const float ix = int(unsigned(qi[i].x) - unsigned(r0.x)) * inv,
+                iy = int(unsigned(qi[i].y) - unsigned(r0.y)) * inv,
+                iz = int(unsigned(qi[i].z) - unsigned(r0.z)) * inv;
     bool hit = false;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const float dx = jx[j] - ix, dy = jy[j] - iy, dz = jz[j] - iz;
       hit |= ((row >> j) & 1u) && dx * dx + dy * dy + dz * dz < reach2;
     }
-    if (hit) return true;
+    if (hit) return true;  // most kept tiles stop at their first rows
   }
   return false;
 }

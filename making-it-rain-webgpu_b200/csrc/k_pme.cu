@@ -223,7 +223,7 @@ __device__ __forceinline__ void spline_for(const SysDev& S, long long x, long lo
 // Both spreads read nothing the list kernels write, so they run on their own
 // stream while the list kernels sort and rebuild.
 //
-// By atom (engines up to a few waves of blocks): a block takes up to
+// By atom (engines under one block of slots per SM): a block takes up to
 // kSplineAtoms atoms: their splines are computed once each into shared memory,
 // then all its threads share the 25 (ix, iy) rows of 5 z points per atom, so
 // no thread makes more than a few atomics in a row (one thread per atom making
@@ -301,9 +301,10 @@ __global__ void __launch_bounds__(kThreads) k_spread(Dev d, int per) {
 // across a jump of the curve) or whose slots reach into the next system
 // spreads directly.  Every contribution is the same fixed-point value as in
 // the by-atom spread, so the grid is the same to the bit.  The shared-memory
-// phases make a block's chain longer: below a few waves of blocks (the 12k
-// and 27k single systems) the by-atom kernel finishes first, above it (a
-// 64-system ensemble of 627k atoms) this one takes 30% less time.
+// phases make a block's chain longer: below one block per SM (the 12k-atom
+// peptide) the by-atom kernel finishes first; above it this one takes less
+// time (the 27k-atom octahedron 7% less, a 64-system ensemble of 627k atoms
+// 45% less).
 constexpr int kPatchSlots = 128;
 constexpr int kPatchPoints = 4096;  // 32 KB of int64
 
@@ -849,8 +850,10 @@ void set_pme_smem(int z, int y, int x, int plane) {
   cudaFuncSetAttribute(k_fft_x_convolve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
 }
 
-// Engines with at least four blocks of 128 slots per SM spread by slot.
-bool spread_by_slot(int n_slots) { return (n_slots + kPatchSlots - 1) / kPatchSlots >= 148 * 4; }
+// Engines with at least one block of 128 slots per SM spread by slot: the
+// 27k-atom octahedron (205 blocks) spreads in 25.5 us by slot against 27.5 us
+// by atom, the 12k-atom peptide (96 blocks) in 15.5 us against 13.7 us.
+bool spread_by_slot(int n_slots) { return (n_slots + kPatchSlots - 1) / kPatchSlots >= 148; }
 
 void launch_pme_spread(const Dev& d, cudaStream_t st) {
   if (d.n_fft_z == 0) return;
