@@ -986,6 +986,12 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     e->coop_list = true;
   }
   if (e->opt.flags & MDB_FLAG_PHASE_LAUNCHES) e->coop_list = false;
+  // A large batch rebuilds some system's list nearly every step; its search
+  // phases then want the full grids of separate launches more than the
+  // cooperative kernel's two blocks per SM (64-system ensemble, 627k atoms:
+  // 3.51 against 3.56 ms per step), and a step of milliseconds hides the
+  // thirteen launches.  Single systems and small batches keep the one launch.
+  if (d.S > 1 && d.n_slots >= (1 << 18)) e->coop_list = false;
   return MDB_OK;
 }
 
