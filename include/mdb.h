@@ -453,6 +453,8 @@ int mdb_autotune(const mdb_system_desc* system, const mdb_state_desc* state, con
  * step.  A batch keeps the device busy where one small system leaves it
  * waiting on launches, so the candidate that wins for a batch of a size
  * bucket's systems can differ from the one that wins for any one of them.
+ * With n > 1 the grid is 8-atom tiles only, over ten (skin, inner skin)
+ * pairs from (0.15 nm, none) to (0.5, 0.1) and two sort cells: 20 candidates.
  */
 int mdb_autotune_batch(int32_t n, const mdb_system_desc* systems, const mdb_state_desc* states,
                        const mdb_run_options* options, int32_t steps, mdb_tuning* best, double* best_ms_per_step,

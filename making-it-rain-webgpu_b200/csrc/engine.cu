@@ -1724,12 +1724,22 @@ int mdb_autotune_batch(int32_t n, const mdb_system_desc* systems, const mdb_stat
   static const double kCells8[] = {0.20, 0.25};
   static const double kCells32[] = {0.20, 0.25, 0.35};
   static const int kPrune[] = {1, 2};
+  // A batch keeps the device busy, so only the slots read and the list work
+  // count: 8x8 tiles (32x32 ones never won a batch) over a finer ladder of
+  // skins and inner skins, and no pruning at rebuild (the inner list prunes).
+  static const Lists kListsBatch[] = {{0.15, -1.0}, {0.20, -1.0}, {0.25, -1.0}, {0.25, 0.06}, {0.30, 0.06},
+                                      {0.30, 0.08}, {0.35, 0.08}, {0.40, 0.08}, {0.40, 0.10}, {0.50, 0.10}};
   std::vector<mdb_tuning> grid;
-  for (int prune : kPrune) {
-    for (const Lists& l : kLists8)
-      for (double cell : kCells8) grid.push_back(mdb_tuning{l.skin, cell, 8, prune, l.inner});
-    for (const Lists& l : kLists32)
-      for (double cell : kCells32) grid.push_back(mdb_tuning{l.skin, cell, 32, prune, l.inner});
+  if (n > 1) {
+    for (const Lists& l : kListsBatch)
+      for (double cell : kCells8) grid.push_back(mdb_tuning{l.skin, cell, 8, 2, l.inner});
+  } else {
+    for (int prune : kPrune) {
+      for (const Lists& l : kLists8)
+        for (double cell : kCells8) grid.push_back(mdb_tuning{l.skin, cell, 8, prune, l.inner});
+      for (const Lists& l : kLists32)
+        for (double cell : kCells32) grid.push_back(mdb_tuning{l.skin, cell, 32, prune, l.inner});
+    }
   }
   double best_ms = std::numeric_limits<double>::infinity();
   int count = 0, last = MDB_OK;

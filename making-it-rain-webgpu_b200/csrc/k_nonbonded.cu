@@ -27,10 +27,17 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
-// Tiles per warp: blocks take fixed chunks of the list and retire as they
-// finish, so the PME stream's kernels can take SMs while the pair kernel runs;
-// short chunks (two passes of four 8x8 tiles) balance best.
-constexpr int kTilesPerWarp = 8;  // 16 and 32 measured slower on the peptide and octahedron workloads
+// Tiles per warp (a template argument, TPW): blocks take fixed chunks of the
+// list and retire as they finish, so the PME stream's kernels can take SMs
+// while the pair kernel runs.  Short lists balance best with short chunks;
+// long ones save the per-chunk work (the system lookup, the row and energy
+// flushes) with long ones.  Measured: the 12k and 27k single systems (lists of
+// 0.14 and 0.30 M tiles) are fastest at 8 (16: octahedron step 0.144 against
+// 0.141 ms); the 100k box (2 M tiles) at 16 (pair kernel 0.209 against 0.220
+// ms); the 64-system ensemble (9 M tiles) at 64 (pair kernel 1.81 ms; 32:
+// 1.83, 16: 1.90, 8: 2.03, 4: 2.18).
+constexpr long long kChunk16Tiles = 1ll << 20;  // a typical list at least this long takes chunks of 16
+constexpr long long kChunk64Tiles = 1ll << 22;  // and from here chunks of 64
 
 // erfc(x) = exp(-x^2) P(u): P fits erfcx on x in [0, 3.6] as a degree-7
 // polynomial in u = 3.111 t - 2.111, t = 1/(1 + x/2) (fit_erfcx.py in this
@@ -172,12 +179,12 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
   }
 }
 
-// A warp takes chunks of kTilesPerWarp consecutive tiles of the list (chunk
+// A warp takes chunks of TPW consecutive tiles of the list (chunk
 // w, then w + warps, ...) and walks each 32/C tiles at a time; group g of the
 // warp runs tile t + g.  Every lane keeps its own row and system, because the
 // groups of one warp may be at different ones.  The grid is sized for a
 // typical list, so most warps take one chunk and then retire.
-template <int C, bool ENERGY, bool TRICLINIC>
+template <int C, int TPW, bool ENERGY, bool TRICLINIC>
 __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   wait_for_predecessor();  // no early release: later waves would share their SMs with the next kernel
   constexpr int G = 32 / C;
@@ -187,8 +194,8 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int total = d.tile_prefix[d.S];
-  for (int t0 = warp * kTilesPerWarp; t0 < total; t0 += nwarps * kTilesPerWarp) {
-    const int tend = min(total, t0 + kTilesPerWarp);
+  for (int t0 = warp * TPW; t0 < total; t0 += nwarps * TPW) {
+    const int tend = min(total, t0 + TPW);
     int s = find_system(d.tile_prefix, d.S, min(t0 + g, tend - 1));
     if (ENERGY && d.active) {
       // an evaluation of some systems only (energy evaluations; a step's
@@ -314,23 +321,30 @@ __global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
   }
 }
 
-template <int C>
+template <int C, int TPW>
 void launch_shape(const Dev& d, bool energy, bool triclinic, cudaStream_t st) {
   // one chunk per warp for a list of ~160 tiles per cluster (8x8 tiles in
   // water run 90-150); a longer list makes warps take further chunks
   const int warps_per_block = kThreads / 32;
   const long long typical = static_cast<long long>(d.n_blocks) * (C == 8 ? 160 : 100);
   const int blocks = static_cast<int>(std::max<long long>(
-      1, std::min<long long>((typical + kTilesPerWarp * warps_per_block - 1) / (kTilesPerWarp * warps_per_block),
-                             (d.tile_cap_total + kTilesPerWarp * warps_per_block - 1) /
-                                 (kTilesPerWarp * warps_per_block))));
+      1, std::min<long long>((typical + TPW * warps_per_block - 1) / (TPW * warps_per_block),
+                             (d.tile_cap_total + TPW * warps_per_block - 1) / (TPW * warps_per_block))));
   if (energy) {
-    if (triclinic) launch_chained(k_nonbonded<C, true, true>, blocks, kThreads, 0, st, d);
-    else launch_chained(k_nonbonded<C, true, false>, blocks, kThreads, 0, st, d);
+    if (triclinic) launch_chained(k_nonbonded<C, TPW, true, true>, blocks, kThreads, 0, st, d);
+    else launch_chained(k_nonbonded<C, TPW, true, false>, blocks, kThreads, 0, st, d);
   } else {
-    if (triclinic) launch_chained(k_nonbonded<C, false, true>, blocks, kThreads, 0, st, d);
-    else launch_chained(k_nonbonded<C, false, false>, blocks, kThreads, 0, st, d);
+    if (triclinic) launch_chained(k_nonbonded<C, TPW, false, true>, blocks, kThreads, 0, st, d);
+    else launch_chained(k_nonbonded<C, TPW, false, false>, blocks, kThreads, 0, st, d);
   }
+}
+
+template <int C>
+void launch_size(const Dev& d, bool energy, bool triclinic, cudaStream_t st) {
+  const long long typical = static_cast<long long>(d.n_blocks) * (C == 8 ? 160 : 100);
+  if (typical >= kChunk64Tiles) launch_shape<C, 64>(d, energy, triclinic, st);
+  else if (typical >= kChunk16Tiles) launch_shape<C, 16>(d, energy, triclinic, st);
+  else launch_shape<C, 8>(d, energy, triclinic, st);
 }
 
 }  // namespace
@@ -343,8 +357,8 @@ void launch_nonbonded(const Dev& d, bool energy, cudaStream_t st) {
     list.tile_shift = d.in_shift;
     list.tile_prefix = d.in_prefix;
   }
-  if (d.cluster == 8) launch_shape<8>(list, energy, d.any_triclinic != 0, st);
-  else launch_shape<32>(list, energy, d.any_triclinic != 0, st);
+  if (d.cluster == 8) launch_size<8>(list, energy, d.any_triclinic != 0, st);
+  else launch_size<32>(list, energy, d.any_triclinic != 0, st);
 }
 
 }  // namespace mdb

@@ -346,8 +346,9 @@ def test_batched_autotune_searches_the_bucket_together(mdb):
                for k, (n, w) in enumerate([(700, 2.8), (760, 2.9), (1500, 3.6)])]
     best = mdb.autotune_batch([m[0] for m in members[:2]], [m[1] for m in members[:2]], steps=30)
     print("autotune_batch", best)
-    assert best["candidates"] == 32 and best["systems"] == 2
-    assert best["verlet_skin"] in (0.15, 0.20, 0.30, 0.40, 0.50) and best["tile_atoms"] in (8, 32)
+    assert best["candidates"] == 20 and best["systems"] == 2  # the batch grid: 8-atom tiles only
+    assert best["verlet_skin"] in (0.15, 0.20, 0.25, 0.30, 0.35, 0.40, 0.50) and best["tile_atoms"] == 8
+    assert best["inner_skin"] in (-1.0, 0.06, 0.08, 0.10) and best["prune_tiles"] == 2
     assert best["ms_per_step"] > 0
     tuning, buckets = mdb.tune_by_bucket([m[0] for m in members], [m[1] for m in members], steps=30, batched=True)
     assert len(tuning) == 3 and len(buckets) == 2  # 2,100 and 2,280 atoms share a bucket; 4,500 is the next
