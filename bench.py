@@ -619,7 +619,7 @@ def main() -> None:
                 st = lp.barostat_statistics(k)
                 for key in ("attempts", "accepted", "screened", "exactEvaluations"):
                     out[key] = out.get(key, 0) + st[key]
-                for key in ("trainingSamples", "surrogateActive", "surrogateDisabled", "surrogateRms"):
+                for key in ("trainingSamples", "surrogateActive", "surrogateDisabled", "surrogateRms", "trainingMs"):
                     out[key] = st[key]
             return out
 
