@@ -63,10 +63,10 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate
 # (other workloads report null)
 NB_TRAFFIC = {"octa-27k": 11175936, "peptide-12k": 5061632}
 # DRAM bytes per inner-list tile read, from one ncu capture of the ensemble's
-# pair kernel (326.44 MB read + 14.78 MB written over 9,279,094 tiles): the
+# pair kernel (327.23 MB read + 14.18 MB written over 9,279,093 tiles): the
 # ensemble's tile count follows its autotuned list settings, so its traffic is
 # this figure times the tiles the timed engine reads
-NB_TRAFFIC_PER_TILE = {"ensemble-64": 341.22e6 / 9279094}
+NB_TRAFFIC_PER_TILE = {"ensemble-64": 341.41e6 / 9279093}
 # the north star's single-system target, ns/day on the 27k-atom system
 NORTH_STAR_NS_PER_DAY = 1000.0
 
