@@ -931,12 +931,16 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
   set_pme_smem(smem_z, smem_y, smem_x, d.fft_planes ? smem_p : 0);
 
   // PME and the listed terms run beside the pair kernel at the highest
-  // priority: their small, latency-bound grids take SMs as pair blocks retire
+  // priority: their small, latency-bound grids take SMs as pair blocks
+  // retire.  A large batch keeps every SM busy whatever runs first, and there
+  // equal priorities measured 0.7% faster (64-system ensemble, 3.240 against
+  // 3.262 ms per step).
   int least = 0, greatest = 0;
   CUDA_TRY(e, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  const int side = d.S > 1 && d.n_slots >= (1 << 18) ? least : greatest;
   CUDA_TRY(e, cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking));
-  CUDA_TRY(e, cudaStreamCreateWithPriority(&e->s1, cudaStreamNonBlocking, greatest));
-  CUDA_TRY(e, cudaStreamCreateWithPriority(&e->s2, cudaStreamNonBlocking, greatest));
+  CUDA_TRY(e, cudaStreamCreateWithPriority(&e->s1, cudaStreamNonBlocking, side));
+  CUDA_TRY(e, cudaStreamCreateWithPriority(&e->s2, cudaStreamNonBlocking, side));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->join1, cudaEventDisableTiming));
   CUDA_TRY(e, cudaEventCreateWithFlags(&e->join2, cudaEventDisableTiming));
