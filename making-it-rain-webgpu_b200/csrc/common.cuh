@@ -98,6 +98,7 @@ struct SysDev {
   int pc_half[3];    // half of the diagonal in pair-coordinate units
   float pc_inv_diag[3];  // 1/diagonal in pair-coordinate units
   float cut2, list2, half_skin2, alpha, alpha_2_sqrtpi;
+  float gauss_scale;  // -alpha^2 log2(e): exp(-(alpha r)^2) = 2^(r^2 gauss_scale)
   // the inner list: tiles with a pair inside (cutoff + inner skin)^2, re-pruned
   // from the outer list once an atom has moved (inner skin / 2)^2 since the last prune
   float inner2, half_inner2;

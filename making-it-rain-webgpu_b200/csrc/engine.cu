@@ -544,6 +544,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
     S.half_inner2 = e->inner_skin[s] > 0 ? float(0.25 * inner * inner) : 3.0e38f;
     S.alpha = float(h.alpha);
     S.alpha_2_sqrtpi = float(h.alpha * 2.0 / std::sqrt(3.14159265358979323846));
+    S.gauss_scale = float(-h.alpha * h.alpha / std::log(2.0));
     S.exp_scale = float(-1.0 / (4 * h.alpha * h.alpha));
     S.com_freq = h.com_frequency;
     S.total_mass = h.total_mass;

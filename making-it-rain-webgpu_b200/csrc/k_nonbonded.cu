@@ -39,12 +39,36 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr long long kChunk16Tiles = 1ll << 20;  // a typical list at least this long takes chunks of 16
 constexpr long long kChunk64Tiles = 1ll << 22;  // and from here chunks of 64
 
+// The three special functions of a pair, as the flush-to-zero forms of the
+// PTX approximations.  None of their operands or results can be subnormal
+// here: r^2 is at least the square of the closest unexcluded approach (about
+// 0.01 nm^2), the reciprocal's operand lies in [1, 1 + alpha cutoff / 2], and
+// the exponent of the Gaussian is at least -(alpha cutoff)^2 log2(e) (-10 at
+// an Ewald tolerance of 5e-4; below -126 only where erfc(alpha r) is itself
+// below 1e-38), so the results are the ones the subnormal-preserving forms
+// give, without their range fix-ups.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float exp2_ftz(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // erfc(x) = exp(-x^2) P(u): P fits erfcx on x in [0, 3.6] as a degree-7
 // polynomial in u = 3.111 t - 2.111, t = 1/(1 + x/2) (fit_erfcx.py in this
 // directory derives the coefficients).  The kernel then needs one exponential
 // per pair, shared with the Gaussian term of the force.
 __device__ __forceinline__ float erfcx_poly(float x) {
-  const float t = __fdividef(1.0f, fmaf(0.5f, x, 1.0f));
+  const float t = rcp_ftz(fmaf(0.5f, x, 1.0f));
   const float u = fmaf(t, 3.1111111111111116f, -2.1111111111111116f);
   float p = 2.8532681218254e-05f;
   p = fmaf(p, u, 7.591772236827632e-05f);
@@ -66,16 +90,17 @@ __device__ __forceinline__ float pair_r2(float rx, float ry, float rz) {
 }
 
 // (dE/dr)/r of one pair at r2 < cutoff^2; with ENERGY also its Coulomb and LJ
-// energies.
+// energies.  The Gaussian exp(-(alpha r)^2) is 2^(r^2 gscale), gscale =
+// -alpha^2 log2(e): one product from r^2, not from alpha r.
 template <bool ENERGY>
-__device__ __forceinline__ float pair_force(float r2, float4 qi, float4 qj, float alpha, float a2sp, float& coul_e,
-                                            float& lj_e) {
-  const float rinv = rsqrtf(r2);
+__device__ __forceinline__ float pair_force(float r2, float4 qi, float4 qj, float alpha, float a2sp, float gscale,
+                                            float& coul_e, float& lj_e) {
+  const float rinv = rsqrt_ftz(r2);
   const float rinv2 = __fmul_rn(rinv, rinv);
   const float r = __fmul_rn(r2, rinv);
   const float qq = __fmul_rn(qi.x, qj.x);
   const float x = __fmul_rn(alpha, r);
-  const float gauss = __expf(__fmul_rn(-x, x));
+  const float gauss = exp2_ftz(__fmul_rn(r2, gscale));
   const float coul = __fmul_rn(__fmul_rn(qq, __fmul_rn(gauss, erfcx_poly(x))), rinv);
   const float eps = __fmul_rn(qi.z, qj.z);
   const float sig = __fadd_rn(qi.y, qj.y);
@@ -118,7 +143,7 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
 // The system's constants arrive in registers (`SysConst`): read from global
 // memory in every tile, they cost the loop a load each.
 struct SysConst {
-  float alpha, a2sp, cut2, inv;
+  float alpha, a2sp, gscale, cut2, inv;
   long long tile_base;  // the system's first tile in the list, minus its first tile index
   int next;             // the next system's first tile index
 };
@@ -126,7 +151,7 @@ struct SysConst {
 __device__ __forceinline__ SysConst sys_const(const Dev& d, int s) {
   const SysDev& S = d.sys[s];
   const int first = d.tile_prefix[s];
-  return SysConst{S.alpha, S.alpha_2_sqrtpi, S.cut2, S.pc_inv, S.tile_off - static_cast<long long>(first),
+  return SysConst{S.alpha, S.alpha_2_sqrtpi, S.gauss_scale, S.cut2, S.pc_inv, S.tile_off - static_cast<long long>(first),
                   d.tile_prefix[s + 1]};
 }
 
@@ -135,7 +160,7 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
                                            float4 qj, unsigned int mask, bool per_pair, int l, float& fix,
                                            float& fiy, float& fiz, float& fjx, float& fjy, float& fjz, float& ecoul,
                                            float& elj, int& pairs, float* vir) {
-  const float alpha = K.alpha, a2sp = K.a2sp, cut2 = K.cut2, inv = K.inv;
+  const float alpha = K.alpha, a2sp = K.a2sp, gscale = K.gscale, cut2 = K.cut2, inv = K.inv;
   const int src = (l + 1) & (C - 1);
   constexpr int kUnroll = C == 8 ? 8 : 4;
 #pragma unroll kUnroll
@@ -147,7 +172,7 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
     const float r2 = pair_r2(rx, ry, rz);
     if (((mask >> k) & 1u) && r2 < cut2) {
       float coul = 0.f, lj = 0.f;
-      const float fs = pair_force<ENERGY>(r2, qi, qj, alpha, a2sp, coul, lj);
+      const float fs = pair_force<ENERGY>(r2, qi, qj, alpha, a2sp, gscale, coul, lj);
       fix = fmaf(fs, rx, fix);
       fiy = fmaf(fs, ry, fiy);
       fiz = fmaf(fs, rz, fiz);
@@ -185,7 +210,7 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
 // groups of one warp may be at different ones.  The grid is sized for a
 // typical list, so most warps take one chunk and then retire.
 template <int C, int TPW, bool ENERGY, bool TRICLINIC>
-__global__ void __launch_bounds__(kThreads) k_nonbonded(Dev d) {
+__global__ void __launch_bounds__(kThreads, ENERGY ? 1 : 4) k_nonbonded(Dev d) {
   wait_for_predecessor();  // no early release: later waves would share their SMs with the next kernel
   constexpr int G = 32 / C;
   const int lane = threadIdx.x & 31;
