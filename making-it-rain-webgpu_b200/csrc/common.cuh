@@ -94,6 +94,7 @@ struct SysDev {
   // pair coordinates
   int pc_shift;
   float pc_inv;      // 2^-pc_shift
+  float cut2u;       // cut2 in pair-coordinate units, cut2 2^(2 pc_shift)
   int pc_box[9];     // lattice in pair-coordinate units
   int pc_half[3];    // half of the diagonal in pair-coordinate units
   float pc_inv_diag[3];  // 1/diagonal in pair-coordinate units

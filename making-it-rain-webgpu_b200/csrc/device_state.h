@@ -43,7 +43,7 @@ struct Dev {
   long long *bx, *by, *bz;         // positions before a Monte Carlo volume move
   const int* mol_off;              // molecule m's atoms: mol_atoms[mol_off[m] .. mol_off[m+1])
   const int* mol_atoms;            // global atom indices, molecule by molecule, system by system
-  const float4* prm_atom;  // q*sqrt(ONE_4PI_EPS0), sigma/2, sqrt(eps), q
+  const float4* prm_atom;  // q*sqrt(ONE_4PI_EPS0), sigma/2, sqrt(24 eps), q
 
   // slots, sorted order
   int* order;     // global atom or -1

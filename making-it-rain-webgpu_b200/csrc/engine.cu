@@ -272,6 +272,7 @@ void fill_box(const HostSystem& h, SysDev& S, bool keep_shift) {
   if (!keep_shift || shift < S.pc_shift) S.pc_shift = shift;
   const double sc = std::ldexp(1.0, S.pc_shift);
   S.pc_inv = float(1.0 / sc);
+  S.cut2u = float(std::ldexp(double(S.cut2), 2 * S.pc_shift));  // exact: a power-of-two scaling
   for (int i = 0; i < 9; ++i) S.pc_box[i] = int(std::llround(B[i] * sc));
   for (int k = 0; k < 3; ++k) {
     S.pc_half[k] = S.pc_box[k * 4] / 2;
@@ -599,7 +600,7 @@ int build_engine(mdb_engine* e, int n, const mdb_system_desc* systems, const mdb
       invm.push_back(h.mass[a] == 0 ? 0.f : float(1.0 / h.mass[a]));
       atom_sys.push_back(s);
       prm_atom.push_back(make_float4(float(h.charge[a]) * sq, float(0.5 * h.sigma[a]),
-                                     float(std::sqrt(h.epsilon[a])), float(h.charge[a])));
+                                     float(std::sqrt(24.0 * h.epsilon[a])), float(h.charge[a])));
     }
     for (int k = 0; k < S.n_slots; ++k) slot_sys.push_back(s);
     for (int k = 0; k < S.n_blocks; ++k) block_sys.push_back(s);

@@ -91,30 +91,31 @@ __device__ __forceinline__ float pair_r2(float rx, float ry, float rz) {
 
 // (dE/dr)/r of one pair at r2 < cutoff^2; with ENERGY also its Coulomb and LJ
 // energies.  The Gaussian exp(-(alpha r)^2) is 2^(r^2 gscale), gscale =
-// -alpha^2 log2(e): one product from r^2, not from alpha r.
+// -alpha^2 log2(e): one product from r^2, not from alpha r.  With P = erfcx(x),
+// x = alpha r, and g the Gaussian, the Coulomb part of (dE/dr)/r is
+// -qq g (P / r + a2sp) / r^2, and the parameters carry sqrt(24 eps), so the
+// pair's product is 24 eps and the LJ part is 24 eps (s6 - 2 s12) / r^2.
 template <bool ENERGY>
 __device__ __forceinline__ float pair_force(float r2, float4 qi, float4 qj, float alpha, float a2sp, float gscale,
                                             float& coul_e, float& lj_e) {
   const float rinv = rsqrt_ftz(r2);
   const float rinv2 = __fmul_rn(rinv, rinv);
-  const float r = __fmul_rn(r2, rinv);
-  const float qq = __fmul_rn(qi.x, qj.x);
-  const float x = __fmul_rn(alpha, r);
+  const float x = __fmul_rn(alpha, __fmul_rn(r2, rinv));
   const float gauss = exp2_ftz(__fmul_rn(r2, gscale));
-  const float coul = __fmul_rn(__fmul_rn(qq, __fmul_rn(gauss, erfcx_poly(x))), rinv);
-  const float eps = __fmul_rn(qi.z, qj.z);
+  const float p = erfcx_poly(x);
+  const float qg = __fmul_rn(__fmul_rn(qi.x, qj.x), gauss);
+  const float eps24 = __fmul_rn(qi.z, qj.z);
   const float sig = __fadd_rn(qi.y, qj.y);
   const float s2 = __fmul_rn(__fmul_rn(sig, sig), rinv2);
   const float s6 = __fmul_rn(__fmul_rn(s2, s2), s2);
   const float s12 = __fmul_rn(s6, s6);
   if (ENERGY) {
-    coul_e = coul;
-    lj_e = __fmul_rn(__fmul_rn(4.0f, eps), __fsub_rn(s12, s6));
+    coul_e = __fmul_rn(__fmul_rn(qg, p), rinv);
+    // 4 eps (s12 - s6)
+    lj_e = __fmul_rn(__fmul_rn(eps24, 1.0f / 6.0f), __fsub_rn(s12, s6));
   }
-  // -coul - qq a2sp gauss + eps (24 s6 - 48 s12), over r^2
-  const float lj_f = fmaf(-48.0f, s12, __fmul_rn(24.0f, s6));
-  const float c_f = fmaf(-__fmul_rn(qq, a2sp), gauss, -coul);
-  return __fmul_rn(rinv2, fmaf(eps, lj_f, c_f));
+  const float coul_f = __fmul_rn(qg, fmaf(p, rinv, a2sp));
+  return __fmul_rn(rinv2, fmaf(eps24, fmaf(-2.0f, s12, s6), -coul_f));
 }
 
 // Lanes of the group that holds `lane`, as a shuffle mask.
@@ -143,7 +144,7 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
 // The system's constants arrive in registers (`SysConst`): read from global
 // memory in every tile, they cost the loop a load each.
 struct SysConst {
-  float alpha, a2sp, gscale, cut2, inv;
+  float alpha, a2sp, gscale, cut2u, inv;  // cut2u: the cutoff squared in pair-coordinate units
   long long tile_base;  // the system's first tile in the list, minus its first tile index
   int next;             // the next system's first tile index
 };
@@ -151,7 +152,7 @@ struct SysConst {
 __device__ __forceinline__ SysConst sys_const(const Dev& d, int s) {
   const SysDev& S = d.sys[s];
   const int first = d.tile_prefix[s];
-  return SysConst{S.alpha, S.alpha_2_sqrtpi, S.gauss_scale, S.cut2, S.pc_inv, S.tile_off - static_cast<long long>(first),
+  return SysConst{S.alpha, S.alpha_2_sqrtpi, S.gauss_scale, S.cut2u, S.pc_inv, S.tile_off - static_cast<long long>(first),
                   d.tile_prefix[s + 1]};
 }
 
@@ -160,7 +161,12 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
                                            float4 qj, unsigned int mask, bool per_pair, int l, float& fix,
                                            float& fiy, float& fiz, float& fjx, float& fjy, float& fjz, float& ecoul,
                                            float& elj, int& pairs, float* vir) {
-  const float alpha = K.alpha, a2sp = K.a2sp, gscale = K.gscale, cut2 = K.cut2, inv = K.inv;
+  const float alpha = K.alpha, a2sp = K.a2sp, gscale = K.gscale, inv = K.inv;
+  // The separation stays in pair-coordinate units (u = float(d)) until it is
+  // needed in nm: inv = 2^-shift is a power of two, so every scaling below is
+  // exact and r2 = r2u inv^2, fs rx = (fs inv) ux and r2 < cut2 <=>
+  // r2u < cut2 / inv^2 hold bit for bit.
+  const float inv2 = __fmul_rn(inv, inv), cut2u = K.cut2u;
   const int src = (l + 1) & (C - 1);
   constexpr int kUnroll = C == 8 ? 8 : 4;
 #pragma unroll kUnroll
@@ -168,18 +174,21 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
     int dx = int(unsigned(pj.x) - unsigned(pi.x)), dy = int(unsigned(pj.y) - unsigned(pi.y)),
         dz = int(unsigned(pj.z) - unsigned(pi.z));
     if (per_pair) min_image<TRICLINIC>(S, dx, dy, dz);
-    const float rx = dx * inv, ry = dy * inv, rz = dz * inv;
-    const float r2 = pair_r2(rx, ry, rz);
-    if (((mask >> k) & 1u) && r2 < cut2) {
+    const float ux = float(dx), uy = float(dy), uz = float(dz);
+    const float r2u = pair_r2(ux, uy, uz);
+    if (((mask >> k) & 1u) && r2u < cut2u) {
       float coul = 0.f, lj = 0.f;
+      const float r2 = __fmul_rn(r2u, inv2);
       const float fs = pair_force<ENERGY>(r2, qi, qj, alpha, a2sp, gscale, coul, lj);
-      fix = fmaf(fs, rx, fix);
-      fiy = fmaf(fs, ry, fiy);
-      fiz = fmaf(fs, rz, fiz);
-      fjx = fmaf(-fs, rx, fjx);
-      fjy = fmaf(-fs, ry, fjy);
-      fjz = fmaf(-fs, rz, fjz);
+      const float fsu = __fmul_rn(fs, inv);
+      fix = fmaf(fsu, ux, fix);
+      fiy = fmaf(fsu, uy, fiy);
+      fiz = fmaf(fsu, uz, fiz);
+      fjx = fmaf(-fsu, ux, fjx);
+      fjy = fmaf(-fsu, uy, fjy);
+      fjz = fmaf(-fsu, uz, fjz);
       if (ENERGY) {
+        const float rx = __fmul_rn(ux, inv), ry = __fmul_rn(uy, inv), rz = __fmul_rn(uz, inv);
         ecoul += coul;
         elj += lj;
         pairs += 1;
