@@ -156,9 +156,9 @@ __device__ __forceinline__ SysConst sys_const(const Dev& d, int s) {
                   d.tile_prefix[s + 1]};
 }
 
-template <int C, bool ENERGY, bool TRICLINIC>
+template <int C, bool ENERGY, bool TRICLINIC, bool IMAGE>
 __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, int4 pi, float4 qi, int4 pj,
-                                           float4 qj, unsigned int mask, bool per_pair, int l, float& fix,
+                                           float4 qj, unsigned int mask, int l, float& fix,
                                            float& fiy, float& fiz, float& fjx, float& fjy, float& fjz, float& ecoul,
                                            float& elj, int& pairs, float* vir) {
   const float alpha = K.alpha, a2sp = K.a2sp, gscale = K.gscale, inv = K.inv;
@@ -173,7 +173,7 @@ __device__ __forceinline__ void tile_pairs(const SysDev& S, const SysConst& K, i
   for (int k = 0; k < C; ++k) {
     int dx = int(unsigned(pj.x) - unsigned(pi.x)), dy = int(unsigned(pj.y) - unsigned(pi.y)),
         dz = int(unsigned(pj.z) - unsigned(pi.z));
-    if (per_pair) min_image<TRICLINIC>(S, dx, dy, dz);
+    if (IMAGE) min_image<TRICLINIC>(S, dx, dy, dz);
     const float ux = float(dx), uy = float(dy), uz = float(dz);
     const float r2u = pair_r2(ux, uy, uz);
     if (((mask >> k) & 1u) && r2u < cut2u) {
@@ -331,8 +331,18 @@ __global__ void __launch_bounds__(kThreads, ENERGY ? 1 : 4) k_nonbonded(Dev d) {
       float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       int np = 0;
       mask = C == 32 ? __funnelshift_r(mask, mask, l) : ((mask >> l) | (mask << ((C - l) & (C - 1)))) & 0xFFu;
-      tile_pairs<C, ENERGY, TRICLINIC>(d.sys[s], K, pi, qi, pj, qj, mask, per_pair, l, fix, fiy, fiz, fjx, fjy,
-                                       fjz, ec, el, np, vir);
+      // The minimum image, for every lane of the warp when any of its tiles
+      // needs it: one warp-wide decision instead of a divergent branch per
+      // slot.  A tile that does not need it holds every pair under its
+      // nearest image already, and the reduction leaves such a separation
+      // unchanged when it is inside the cutoff and longer than the cutoff
+      // when it is not, so both loops give the same pairs and the same bits.
+      if (__any_sync(kFull, per_pair))
+        tile_pairs<C, ENERGY, TRICLINIC, true>(d.sys[s], K, pi, qi, pj, qj, mask, l, fix, fiy, fiz, fjx, fjy, fjz, ec,
+                                               el, np, vir);
+      else
+        tile_pairs<C, ENERGY, TRICLINIC, false>(d.sys[s], K, pi, qi, pj, qj, mask, l, fix, fiy, fiz, fjx, fjy, fjz,
+                                                ec, el, np, vir);
       if (!active) continue;
       aix += to_fixed(fix);
       aiy += to_fixed(fiy);
