@@ -61,7 +61,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA issue rate
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_nonbonded launch, from
 # one ncu capture per workload with the configuration the autotuner picks
 # (other workloads report null)
-NB_TRAFFIC = {"octa-27k": 11175936, "peptide-12k": 5061632}
+NB_TRAFFIC = {"octa-27k": 11183616, "peptide-12k": 5061632}
 # DRAM bytes per inner-list tile read, from one ncu capture of the ensemble's
 # pair kernel (327.23 MB read + 14.18 MB written over 9,279,093 tiles): the
 # ensemble's tile count follows its autotuned list settings, so its traffic is

@@ -131,8 +131,8 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
   return v;
 }
 
-// `per_pair`: take the minimum image of every pair; otherwise pj already
-// carries the tile's lattice shift and the plain difference is the separation.
+// IMAGE: take the minimum image of every pair; otherwise pj already carries
+// the tile's lattice shift and the plain difference is the separation.
 // `mask` arrives rotated: bit k is the pair of step k (j = l + k mod C).  Every
 // tile runs this same code whatever its neighbours in the warp, so a tile's
 // result does not depend on where in the list it sits.  Measured and not
