@@ -48,22 +48,63 @@ __device__ __forceinline__ void add_force(const Dev& d, const SysDev& S, int ato
   add_fixed(&d.fz[gs], z);
 }
 
+// Energy launches: a thread's energy and virial words in registers (2^32
+// fixed point, every slot up to the virial's last), summed over the warp
+// before they reach the system's words in global memory.  A thread per term
+// adding straight into the same dozen words serialises on them (100k waters:
+// about 1.1 M same-address atomics per evaluation); integer sums make the
+// totals the same whatever the grouping.
+struct EnergySums {
+  long long v[kEPairs];
+};
+
 template <bool ENERGY>
-__device__ __forceinline__ void add_energy(const Dev& d, const SysDev& S, int slot, float e) {
-  if (ENERGY) add_fixed(&d.energy[S.energy_base + slot], e);
+__device__ __forceinline__ void add_energy(EnergySums& acc, int slot, float e) {
+  if (ENERGY) acc.v[slot] += to_fixed(e);
 }
 
 // Virial contribution r (x) F of one atom of a term, r measured from the
 // term's first atom (energy evaluations only; a 3x3 row-major tensor).
 template <bool ENERGY>
-__device__ __forceinline__ void add_virial(const Dev& d, const SysDev& S, float3 r, float fx, float fy, float fz) {
+__device__ __forceinline__ void add_virial(EnergySums& acc, float3 r, float fx, float fy, float fz) {
   if (!ENERGY) return;
-  unsigned long long* w = &d.energy[S.energy_base + kEVirial0];
   const float rr[3] = {r.x, r.y, r.z}, ff[3] = {fx, fy, fz};
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int b = 0; b < 3; ++b) add_fixed(&w[3 * a + b], rr[a] * ff[b]);
+    for (int b = 0; b < 3; ++b) acc.v[kEVirial0 + 3 * a + b] += to_fixed(rr[a] * ff[b]);
+}
+
+// One thread's sums into system s's words, and cleared.
+__device__ __forceinline__ void flush_sums(const Dev& d, EnergySums& acc, int s) {
+  unsigned long long* e = &d.energy[d.sys[s].energy_base];
+#pragma unroll
+  for (int k = 0; k < kEPairs; ++k) {
+    if (acc.v[k]) add_fixed64(&e[k], acc.v[k]);
+    acc.v[k] = 0;
+  }
+}
+
+// The warp's sums at the end of the kernel (every lane present): one add per
+// word when every lane that has sums has them for the same system, else one
+// per lane.
+__device__ __forceinline__ void flush_warp(const Dev& d, EnergySums& acc, int s) {
+  const unsigned full = 0xffffffffu;
+  const int lead = __reduce_max_sync(full, s);
+  if (lead < 0) return;
+  if (__all_sync(full, s == lead || s < 0)) {
+    unsigned long long* e = &d.energy[d.sys[lead].energy_base];
+#pragma unroll
+    for (int k = 0; k < kEPairs; ++k) {
+      long long v = acc.v[k];
+      if (!__any_sync(full, v != 0)) continue;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
+      if ((threadIdx.x & 31) == 0 && v) add_fixed64(&e[k], v);
+    }
+  } else if (s >= 0) {
+    flush_sums(d, acc, s);
+  }
 }
 
 // Error-free transformations on f32 (Knuth's TwoSum; the fma product error).
@@ -104,20 +145,20 @@ __device__ __forceinline__ float bond_stretch(const Dev& d, const BondDev& t, fl
 }
 
 template <bool ENERGY>
-__device__ void bond(const Dev& d, const BondDev& t) {
+__device__ void bond(const Dev& d, const BondDev& t, EnergySums& acc) {
   const SysDev& S = d.sys[t.sys];
   float3 v;
   float r;
   const float dr = bond_stretch(d, t, v, r);
-  add_energy<ENERGY>(d, S, kEBond, 0.5f * t.k * dr * dr);
+  add_energy<ENERGY>(acc, kEBond, 0.5f * t.k * dr * dr);
   const float sc = t.k * dr / r;
   add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);
   add_force(d, S, t.b, -sc * v.x, -sc * v.y, -sc * v.z);
-  add_virial<ENERGY>(d, S, v, -sc * v.x, -sc * v.y, -sc * v.z);
+  add_virial<ENERGY>(acc, v, -sc * v.x, -sc * v.y, -sc * v.z);
 }
 
 template <bool ENERGY>
-__device__ void angle(const Dev& d, const AngleDev& t) {
+__device__ void angle(const Dev& d, const AngleDev& t, EnergySums& acc) {
   const SysDev& S = d.sys[t.sys];
   const float3 v1 = diff(d, t.b, t.a), v2 = diff(d, t.b, t.c);
   const float r1 = v1.x * v1.x + v1.y * v1.y + v1.z * v1.z;
@@ -130,7 +171,7 @@ __device__ void angle(const Dev& d, const AngleDev& t) {
   const float theta = atan2f(sqrtf(nx * nx + ny * ny + nz * nz), dot);
   (void)cs;
   const float dth = theta - t.theta0;
-  add_energy<ENERGY>(d, S, kEAngle, 0.5f * t.k * dth * dth);
+  add_energy<ENERGY>(acc, kEAngle, 0.5f * t.k * dth * dth);
   const float dE = t.k * dth;
   const float tA = dE / (r1 * nn), tC = -dE / (r2 * nn);
   const float f1x = -tA * (v1.y * nz - v1.z * ny), f1y = -tA * (v1.z * nx - v1.x * nz),
@@ -140,12 +181,12 @@ __device__ void angle(const Dev& d, const AngleDev& t) {
   add_force(d, S, t.a, f1x, f1y, f1z);
   add_force(d, S, t.c, f3x, f3y, f3z);
   add_force(d, S, t.b, -f1x - f3x, -f1y - f3y, -f1z - f3z);
-  add_virial<ENERGY>(d, S, v1, f1x, f1y, f1z);
-  add_virial<ENERGY>(d, S, v2, f3x, f3y, f3z);
+  add_virial<ENERGY>(acc, v1, f1x, f1y, f1z);
+  add_virial<ENERGY>(acc, v2, f3x, f3y, f3z);
 }
 
 template <bool ENERGY>
-__device__ void torsion(const Dev& d, const TorsionDev& t) {
+__device__ void torsion(const Dev& d, const TorsionDev& t, EnergySums& acc) {
   const SysDev& S = d.sys[t.sys];
   const float3 b1 = diff(d, t.a, t.b), b2 = diff(d, t.b, t.c), b3 = diff(d, t.c, t.d);
   const float n1x = b1.y * b2.z - b1.z * b2.y, n1y = b1.z * b2.x - b1.x * b2.z, n1z = b1.x * b2.y - b1.y * b2.x;
@@ -158,7 +199,7 @@ __device__ void torsion(const Dev& d, const TorsionDev& t) {
   const float arg = t.periodicity * phi - t.phase;
   float sn, cn;
   sincosf(arg, &sn, &cn);
-  add_energy<ENERGY>(d, S, kETorsion, t.k * (1.f + cn));
+  add_energy<ENERGY>(acc, kETorsion, t.k * (1.f + cn));
   if (n1 == 0.f || n2 == 0.f) return;
   const float dEdPhi = -t.k * t.periodicity * sn;
   const float s1 = dEdPhi * b2n / n1, s4 = -dEdPhi * b2n / n2;
@@ -174,16 +215,16 @@ __device__ void torsion(const Dev& d, const TorsionDev& t) {
   if (ENERGY) {
     const float3 rc = make_float3(b1.x + b2.x, b1.y + b2.y, b1.z + b2.z);
     const float3 rd = make_float3(rc.x + b3.x, rc.y + b3.y, rc.z + b3.z);
-    add_virial<ENERGY>(d, S, b1, -(1.f + ss) * f1x + tt * f4x, -(1.f + ss) * f1y + tt * f4y,
+    add_virial<ENERGY>(acc, b1, -(1.f + ss) * f1x + tt * f4x, -(1.f + ss) * f1y + tt * f4y,
                        -(1.f + ss) * f1z + tt * f4z);
-    add_virial<ENERGY>(d, S, rc, ss * f1x - (1.f + tt) * f4x, ss * f1y - (1.f + tt) * f4y,
+    add_virial<ENERGY>(acc, rc, ss * f1x - (1.f + tt) * f4x, ss * f1y - (1.f + tt) * f4y,
                        ss * f1z - (1.f + tt) * f4z);
-    add_virial<ENERGY>(d, S, rd, f4x, f4y, f4z);
+    add_virial<ENERGY>(acc, rd, f4x, f4y, f4z);
   }
 }
 
 template <bool ENERGY>
-__device__ void exception(const Dev& d, const ExceptionDev& t) {
+__device__ void exception(const Dev& d, const ExceptionDev& t, EnergySums& acc) {
   const SysDev& S = d.sys[t.sys];
   const float3 v = min_image_fixed(S, d.px[t.b] - d.px[t.a], d.py[t.b] - d.py[t.a], d.pz[t.b] - d.pz[t.a]);
   const float r2 = v.x * v.x + v.y * v.y + v.z * v.z;
@@ -206,21 +247,21 @@ __device__ void exception(const Dev& d, const ExceptionDev& t) {
     own += t.eps4 * (s12 - s6);
     dEdR += t.eps4 * rinv * (6.f * s6 - 12.f * s12);
   }
-  add_energy<ENERGY>(d, S, kEExclusion, correction);
-  add_energy<ENERGY>(d, S, kEException, own);
+  add_energy<ENERGY>(acc, kEExclusion, correction);
+  add_energy<ENERGY>(acc, kEException, own);
   if (dEdR != 0.f) {
     const float sc = dEdR * rinv;
     add_force(d, S, t.a, sc * v.x, sc * v.y, sc * v.z);
     add_force(d, S, t.b, -sc * v.x, -sc * v.y, -sc * v.z);
-    add_virial<ENERGY>(d, S, v, -sc * v.x, -sc * v.y, -sc * v.z);
+    add_virial<ENERGY>(acc, v, -sc * v.x, -sc * v.y, -sc * v.z);
   }
 }
 
 template <bool ENERGY>
-__device__ void restraint(const Dev& d, const RestraintDev& t) {
+__device__ void restraint(const Dev& d, const RestraintDev& t, EnergySums& acc) {
   const SysDev& S = d.sys[t.sys];
   const float3 v = min_image_fixed(S, d.px[t.p] - t.x0, d.py[t.p] - t.y0, d.pz[t.p] - t.z0);
-  add_energy<ENERGY>(d, S, kERestraint, t.k * (v.x * v.x + v.y * v.y + v.z * v.z));
+  add_energy<ENERGY>(acc, kERestraint, t.k * (v.x * v.x + v.y * v.y + v.z * v.z));
   add_force(d, S, t.p, -2.f * t.k * v.x, -2.f * t.k * v.y, -2.f * t.k * v.z);
 }
 
@@ -228,19 +269,30 @@ template <bool ENERGY>
 __global__ void __launch_bounds__(kThreads) k_listed(Dev d) {
   const int n0 = d.n_bonds, n1 = n0 + d.n_angles, n2 = n1 + d.n_torsions, n3 = n2 + d.n_exceptions,
             n4 = n3 + d.n_restraints;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
-    if (i < n0) {
-      if (sys_active(d, d.bonds[i].sys)) bond<ENERGY>(d, d.bonds[i]);
-    } else if (i < n1) {
-      if (sys_active(d, d.angles[i - n0].sys)) angle<ENERGY>(d, d.angles[i - n0]);
-    } else if (i < n2) {
-      if (sys_active(d, d.torsions[i - n1].sys)) torsion<ENERGY>(d, d.torsions[i - n1]);
-    } else if (i < n3) {
-      if (sys_active(d, d.exceptions[i - n2].sys)) exception<ENERGY>(d, d.exceptions[i - n2]);
-    } else if (sys_active(d, d.restraints[i - n3].sys)) {
-      restraint<ENERGY>(d, d.restraints[i - n3]);
-    }
+  EnergySums acc;
+  int acc_sys = -1;  // the system acc holds sums for
+  if (ENERGY) {
+#pragma unroll
+    for (int k = 0; k < kEPairs; ++k) acc.v[k] = 0;
   }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
+    const int sys = i < n0   ? d.bonds[i].sys
+                    : i < n1 ? d.angles[i - n0].sys
+                    : i < n2 ? d.torsions[i - n1].sys
+                    : i < n3 ? d.exceptions[i - n2].sys
+                             : d.restraints[i - n3].sys;
+    if (!sys_active(d, sys)) continue;
+    if (ENERGY && sys != acc_sys) {
+      if (acc_sys >= 0) flush_sums(d, acc, acc_sys);
+      acc_sys = sys;
+    }
+    if (i < n0) bond<ENERGY>(d, d.bonds[i], acc);
+    else if (i < n1) angle<ENERGY>(d, d.angles[i - n0], acc);
+    else if (i < n2) torsion<ENERGY>(d, d.torsions[i - n1], acc);
+    else if (i < n3) exception<ENERGY>(d, d.exceptions[i - n2], acc);
+    else restraint<ENERGY>(d, d.restraints[i - n3], acc);
+  }
+  if (ENERGY) flush_warp(d, acc, acc_sys);
 }
 
 }  // namespace

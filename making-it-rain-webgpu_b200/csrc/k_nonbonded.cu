@@ -118,6 +118,23 @@ __device__ __forceinline__ float pair_force(float r2, float4 qi, float4 qj, floa
   return __fmul_rn(rinv2, fmaf(eps24, fmaf(-2.0f, s12, s6), -coul_f));
 }
 
+// A system's pair energies, pair count and pair virial (xx yy zz xy xz yz)
+// into its energy words; the virial slots are row-major 3x3, the symmetric
+// tensor written to both halves.
+__device__ __forceinline__ void add_pair_energies(unsigned long long* e, long long c, long long lj, long long p,
+                                                  const long long* v) {
+  if (c) add_fixed64(&e[kECoulomb], c);
+  if (lj) add_fixed64(&e[kELj], lj);
+  if (p) add_fixed64(&e[kEPairs], p);
+  const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    if (!v[k]) continue;
+    add_fixed64(&e[kEVirial0 + slot[k]], v[k]);
+    if (mirror[k] >= 0) add_fixed64(&e[kEVirial0 + mirror[k]], v[k]);
+  }
+}
+
 // Lanes of the group that holds `lane`, as a shuffle mask.
 template <int C>
 __device__ __forceinline__ unsigned group_mask(int lane) {
@@ -228,6 +245,21 @@ __global__ void __launch_bounds__(kThreads, ENERGY ? 1 : 4) k_nonbonded(Dev d) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int total = d.tile_prefix[d.S];
+  // Energy launches: the groups' sums for the system of the block's first
+  // chunk meet in shared memory and reach the system's energy words once per
+  // block.  Every group adding into the same dozen words of global memory
+  // serialises on them (a 100k-atom box: some 3 M same-address atomics per
+  // evaluation).  The sums are integers, so the totals do not change.
+  __shared__ unsigned long long blk_acc[9];  // coulomb, LJ, pairs, virial xx yy zz xy xz yz
+  __shared__ int blk_sys;
+  if (ENERGY) {
+    if (threadIdx.x < 9) blk_acc[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) {
+      const int t_first = blockIdx.x * (blockDim.x >> 5) * TPW;
+      blk_sys = t_first < total ? find_system(d.tile_prefix, d.S, t_first) : -1;
+    }
+    __syncthreads();
+  }
   for (int t0 = warp * TPW; t0 < total; t0 += nwarps * TPW) {
     const int tend = min(total, t0 + TPW);
     int s = find_system(d.tile_prefix, d.S, min(t0 + g, tend - 1));
@@ -265,19 +297,15 @@ __global__ void __launch_bounds__(kThreads, ENERGY ? 1 : 4) k_nonbonded(Dev d) {
         long long v[6];
   #pragma unroll
         for (int k = 0; k < 6; ++k) v[k] = group_sum64<C>(vir64[k], gmask);
-        if (l == 0) {
-          unsigned long long* e = &d.energy[d.sys[sys].energy_base];
-          if (c) add_fixed64(&e[kECoulomb], c);
-          if (lj) add_fixed64(&e[kELj], lj);
-          if (p) add_fixed64(&e[kEPairs], p);
-          // slots: row-major 3x3, the symmetric pair tensor written to both halves
-          const int slot[6] = {0, 4, 8, 1, 2, 5}, mirror[6] = {-1, -1, -1, 3, 6, 7};
+        if (l == 0 && sys == blk_sys) {
+          if (c) atomicAdd(&blk_acc[0], static_cast<unsigned long long>(c));
+          if (lj) atomicAdd(&blk_acc[1], static_cast<unsigned long long>(lj));
+          if (p) atomicAdd(&blk_acc[2], static_cast<unsigned long long>(p));
   #pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            if (!v[k]) continue;
-            add_fixed64(&e[kEVirial0 + slot[k]], v[k]);
-            if (mirror[k] >= 0) add_fixed64(&e[kEVirial0 + mirror[k]], v[k]);
-          }
+          for (int k = 0; k < 6; ++k)
+            if (v[k]) atomicAdd(&blk_acc[3 + k], static_cast<unsigned long long>(v[k]));
+        } else if (l == 0) {
+          add_pair_energies(&d.energy[d.sys[sys].energy_base], c, lj, p, v);
         }
         ecoul64 = elj64 = pairs64 = 0;
   #pragma unroll
@@ -362,6 +390,16 @@ __global__ void __launch_bounds__(kThreads, ENERGY ? 1 : 4) k_nonbonded(Dev d) {
     }
     flush_row();
     flush_energy(s);
+  }
+  if (ENERGY) {
+    __syncthreads();
+    if (threadIdx.x == 0 && blk_sys >= 0) {
+      long long v[6];
+  #pragma unroll
+      for (int k = 0; k < 6; ++k) v[k] = static_cast<long long>(blk_acc[3 + k]);
+      add_pair_energies(&d.energy[d.sys[blk_sys].energy_base], static_cast<long long>(blk_acc[0]),
+                        static_cast<long long>(blk_acc[1]), static_cast<long long>(blk_acc[2]), v);
+    }
   }
 }
 
