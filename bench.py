@@ -67,8 +67,8 @@ NB_TRAFFIC = {"octa-27k": 11183616, "peptide-12k": 5061632}
 # ensemble's tile count follows its autotuned list settings, so its traffic is
 # this figure times the tiles the timed engine reads
 NB_TRAFFIC_PER_TILE = {"ensemble-64": 341.41e6 / 9279093}
-# the north star's single-system target, ns/day on the 27k-atom system
-NORTH_STAR_NS_PER_DAY = 1000.0
+# the single-system target: 1 microsecond a day on the 27k-atom octahedron
+TARGET_27K_NS_PER_DAY = 1000.0
 
 
 def workload(name: str, seed: int):
@@ -792,9 +792,9 @@ def main() -> None:
                             "autotuner": {k: round(v, 4) if isinstance(v, float) else v for k, v in best.items()}}
         if config == "octa-27k":
             per_replica = value / world
-            extra["north_star"] = {"target_ns_per_day": NORTH_STAR_NS_PER_DAY, "ns_per_day": per_replica,
-                                   "met": per_replica >= NORTH_STAR_NS_PER_DAY,
-                                   "what": "one 27k-atom system on one B200 (replicas count once)"}
+            extra["target"] = {"target_ns_per_day": TARGET_27K_NS_PER_DAY, "ns_per_day": per_replica,
+                               "met": per_replica >= TARGET_27K_NS_PER_DAY,
+                               "what": "one 27k-atom system on one B200 (replicas count once)"}
         result_loop = loop
 
     roof = roofline(result_loop)
