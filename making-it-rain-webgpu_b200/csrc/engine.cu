@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "../../include/mdb.h"
+#include "barostat_rules.h"
 #include "device_state.h"
 #include "mlp.h"
 #include "prep.h"
@@ -1493,7 +1494,7 @@ int barostat_round(mdb_engine* e, const std::vector<int>& due) {
     b.attempts++;
     b.window_attempts++;
     if (screen) {
-      m.a1 = std::min(1.0, std::exp(-(du_pred[i] + m.volume_term) / m.kT));
+      m.a1 = screen_probability(du_pred[i], m.volume_term, m.kT);
       m.exact = barostat_uniform(b, e->opt.seed) < m.a1;
       if (!m.exact) b.screened++;  // rejected by the network alone: no exact evaluation
     }
@@ -1532,15 +1533,14 @@ int barostat_round(mdb_engine* e, const std::vector<int>& due) {
     const double w = du + m.volume_term;
     bool accepted = false;
     if (screen) {
-      const double a1_rev = std::min(1.0, std::exp(-(du_rev[k] - m.volume_term) / m.kT));
-      const double a2 = std::min(1.0, std::exp(-w / m.kT) * a1_rev / m.a1);
+      const double a2 = exact_stage_probability(w, du_rev[k], m.volume_term, m.kT, m.a1);
       accepted = barostat_uniform(b, e->opt.seed) < a2;
       // the exact stage checks the network's prediction
       const double err = du_pred[i] - du;
       net.err2 = net.checked == 0 ? err * err : 0.98 * net.err2 + 0.02 * err * err;
       if (++net.checked >= 50 && std::sqrt(net.err2) > kSurrogateMaxRmsKT * m.kT) net.disabled = true;
     } else {
-      accepted = !(w > 0 && barostat_uniform(b, e->opt.seed) > std::exp(-w / m.kT));
+      accepted = plain_accept(w, m.kT, [&] { return barostat_uniform(b, e->opt.seed); });
       if (net.target > 0 && !net.active) {
         double f[kMlpIn];
         surrogate_features(e0[i], h, m.old_box.data(), m.dlnv, f);
