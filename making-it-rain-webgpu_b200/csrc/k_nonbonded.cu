@@ -150,9 +150,10 @@ __device__ __forceinline__ long long group_sum64(long long v, unsigned mask) {
 
 // IMAGE: take the minimum image of every pair; otherwise pj already carries
 // the tile's lattice shift and the plain difference is the separation.
-// `mask` arrives rotated: bit k is the pair of step k (j = l + k mod C).  Every
-// tile runs this same code whatever its neighbours in the warp, so a tile's
-// result does not depend on where in the list it sits.  Measured and not
+// `mask` arrives rotated: bit k is the pair of step k (j = l + k mod C).  A
+// tile's pairs get the same separations and arithmetic in either image loop,
+// whatever its neighbours in the warp, so a tile's result does not depend on
+// where in the list it sits.  Measured and not
 // kept: evaluating every slot and selecting zeros (no branch) costs 28% more
 // on 32x32 tiles, whose warps often have no pair inside at a step; screening
 // all slots first and evaluating only the pairs inside, 32 at a time through
