@@ -17,7 +17,10 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import json
 import math
+import os
+from pathlib import Path
 from typing import Optional, Sequence
 
 import numpy as np
@@ -429,15 +432,29 @@ def size_bucket(atoms: int) -> int:
 
 
 def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: RunOptions | None = None,
-                   steps: int = 200, cache: dict | None = None, batched: bool = False) -> tuple[list, dict]:
+                   steps: int = 200, cache: dict | None = None, batched: bool = False,
+                   cache_file: os.PathLike | str | None = None, gpu: str | None = None) -> tuple[list, dict]:
     """One search per size bucket; every system of the bucket takes its
     result.  Without `batched`, `autotune` on the bucket's median-sized
     system; with it, `autotune_batch` on the bucket's own systems together
     (from the smallest up, at most 2^18 atoms in all), which is how a batched
     engine runs them.  Returns the per-system tuning list for
     `RunOptions.tuning` and the per-bucket results.  `cache` (bucket ->
-    result) skips buckets already tuned."""
+    result) skips buckets already tuned.
+
+    `cache_file` keeps the results between runs: a JSON file of tuned buckets
+    under a key made of the GPU model (`gpu`, else NVML's name for
+    `options.device`), the library's ABI version and the search (batched or
+    not, steps per candidate).  Buckets found there are not searched again;
+    the file is rewritten with every bucket known afterwards.  One file suits
+    one kind of workload: the buckets are by atom count alone."""
     cache = {} if cache is None else cache
+    key = None
+    if cache_file is not None:
+        model = gpu if gpu is not None else gpu_model((options or RunOptions()).device)
+        key = tuning_cache_key(model, batched, steps)
+        for b, result in load_tuning_cache(cache_file, key).items():
+            cache.setdefault(b, result)
     buckets: dict[int, list[int]] = {}
     for k, s in enumerate(systems):
         buckets.setdefault(size_bucket(s.particle_count), []).append(k)
@@ -456,10 +473,57 @@ def tune_by_bucket(systems: Sequence[System], states: Sequence[State], options: 
         else:
             rep = members[len(members) // 2]
             cache[b] = autotune(systems[rep], states[rep], options, steps)
+    if cache_file is not None:
+        save_tuning_cache(cache_file, key, cache)
     tuning = [tuple(cache[size_bucket(s.particle_count)][k]
                     for k in ("verlet_skin", "sort_cell", "tile_atoms", "prune_tiles", "inner_skin"))
               for s in systems]
     return tuning, cache
+
+
+def gpu_model(device: int = 0) -> str:
+    """The model name NVML gives for device index `device` ("unknown" when
+    NVML is not there): list settings tuned on one model hold for every GPU
+    of that model.  NVML counts devices as the driver does, which is CUDA's
+    order unless CUDA_VISIBLE_DEVICES reorders them."""
+    try:
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            name = pynvml.nvmlDeviceGetName(pynvml.nvmlDeviceGetHandleByIndex(int(device)))
+        finally:
+            pynvml.nvmlShutdown()
+    except Exception:  # no driver, no NVML, no such device
+        return "unknown"
+    return name.decode() if isinstance(name, bytes) else str(name)
+
+
+def tuning_cache_key(model: str, batched: bool, steps: int) -> str:
+    """The key of a tuning-cache entry: GPU model, library ABI, search."""
+    return f"{model} | abi {abi.ABI_VERSION} | {'batched' if batched else 'median system'} | {int(steps)} steps"
+
+
+def load_tuning_cache(path: os.PathLike | str, key: str) -> dict:
+    """The buckets saved under `key` in the JSON file at `path` ({} when the
+    file or the key is absent)."""
+    target = Path(path)
+    if not target.exists():
+        return {}
+    data = json.loads(target.read_text())
+    return {int(b): dict(r) for b, r in data.get(key, {}).items()}
+
+
+def save_tuning_cache(path: os.PathLike | str, key: str, cache: dict) -> None:
+    """Write `cache` (bucket -> result) under `key`, keeping the file's other
+    keys; the file is replaced in one rename, so a reader never sees half of
+    it."""
+    target = Path(path)
+    data = json.loads(target.read_text()) if target.exists() else {}
+    data[key] = {str(b): cache[b] for b in sorted(cache)}
+    partial = target.with_name(target.name + ".partial")
+    partial.write_text(json.dumps(data, indent=1, sort_keys=True))
+    os.replace(partial, target)
 
 
 # ---- the barostat screening network's kernels on their own ---------------------
